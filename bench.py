@@ -1,0 +1,297 @@
+"""Benchmark: Brownian-dynamics particle-steps/s on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config 4] [--precision f32c|f64]
+
+A "step" is one Brownian-dynamics step of the whole workload (all systems of
+the batch): pair forces over 27-cell neighbourhoods, external forces, the
+Euler-Maruyama update with Philox noise and the re-binning, i.e. one launch
+of the fused step kernel.  The default workload is the batched ensemble
+(512 periodic systems, N log-uniform in [500, 20000], 2.45 M particles), the
+configuration the FP32-batched-vs-FP64 metric is quoted on.
+
+value: particle-steps/s with the state resident in HBM, device-timed with CUDA
+       events on the engine's stream (max over ranks).  The per-step state
+       (2.45 M x 64 B = 157 MB read+written) exceeds the 126 MB L2.
+e2e:   the same metric through the C ABI with host buffers: every frame of
+       100 steps uploads the particles from pinned host memory
+       (rdgpu_set_particles), steps, and downloads them (rdgpu_get_particles),
+       the per-frame traffic of the reference's JNI frame loop.
+--impl reference: the CPU path of the reference semantics (the C oracle port,
+       all host threads, the reference's Java core cannot run here) on a
+       bounded sample of the same workload.
+Multi-GPU: replicas only (independent replicate ensembles, one per rank, no
+data-path collective); value sums all ranks' particle-steps over the slowest
+rank's time.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ALG_BYTES = {"f32c": 64, "f64": 64}   # state read + written per particle-step
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=1000)
+    p.add_argument("--warmup", type=int, default=200)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--config", type=int, default=4)
+    p.add_argument("--precision", default="f32c", choices=["f32c", "f64"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_particle(prec, config):
+    """DRAM bytes per particle-step of the step kernel from the committed ncu
+    summary (profiles/step_kernel_traffic.json), scaled to this launch."""
+    path = os.path.join(ROOT, "profiles", "step_kernel_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d[f"{prec}_config{config}"]["bytes_per_particle_step"]
+    except Exception:
+        return None
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([v.strip() for v in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm = sorted(float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit())
+        mx = max((float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()), default=None)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = [names[k] for k in range(4) if any(s[2 + k].lower() == "active" for s in self.samples)]
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def workload(config, rank):
+    from readdygpu_b200 import configs
+    if config == 4:
+        return configs.config4()
+    return configs.CONFIGS[config]()
+
+
+def cpu_baseline(w, budget_s=12.0, threads=None):
+    """The oracle (C port of the reference CPU semantics) on a bounded sample:
+    the first systems of the batch (or the whole single system), OpenMP over
+    all host threads, Philox noise, particle-steps/s."""
+    import numpy as np
+    from oracle import oracle as O
+    threads = threads or O.max_threads()
+    d0 = w.system.to_desc()
+    if w.boxes is None:
+        systems = [(d0, w.xyz, w.types)]
+    else:
+        systems = []
+        for k, (lo, hi, per, sd) in enumerate(w.boxes):
+            d = w.system.to_desc()
+            for a in range(3):
+                d.lo[a], d.hi[a], d.periodic[a] = lo[a], hi[a], per[a]
+            a_, b_ = w.offsets[k], w.offsets[k + 1]
+            systems.append((d, w.xyz[a_:b_], w.types[a_:b_]))
+    done = 0
+    used = []
+    t0 = time.perf_counter()
+    steps = 2
+    for (d, xyz, ty) in systems:
+        x = O.to_rel_f64(d, xyz)
+        O.run_steps(d, x, ty, 7, 0, steps, threads)
+        done += len(ty) * steps
+        used.append(len(ty))
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{len(used)} systems ({sum(used)} particles) x {steps} steps of the workload, "
+                      f"C oracle, {threads} OpenMP threads, {dt:.1f} s"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    w = workload(args.config, 0)
+    cb = cpu_baseline(w, budget_s=20.0)
+    line = {"impl": "reference", "metric": "particle-steps/s", "value": cb["value"], "unit": "particle-steps/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w.name, "particles": w.n, "systems": len(w.boxes) if w.boxes else 1},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "note": "reference CPU semantics via the C oracle port; the reference's own Java core needs a JVM, "
+                    "which this image lacks"}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    import readdygpu_b200 as R
+
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    w = workload(args.config, rank)
+    kw = {}
+    if w.boxes is not None:
+        # each rank owns its own replicate ensemble: shift the seeds
+        kw["boxes"] = [(lo, hi, per, sd + 7919 * rank) for (lo, hi, per, sd) in w.boxes]
+    eng = R.Engine(w.system, precision=args.precision, device=local, seed=11 + rank, **kw)
+    eng.set_particles(w.xyz, w.types, offsets=w.offsets)
+    stream = torch.cuda.ExternalStream(eng.stream, device=local)
+    eng.step(args.warmup)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if ws > 1:
+            torch.distributed.barrier()
+
+    # ---- device-timed, state resident in HBM ----------------------------
+    l0 = eng.launch_count()
+    barrier()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        ev0.record(stream)
+        eng.step(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+    barrier()
+    launches = eng.launch_count() - l0
+    ms = ev0.elapsed_time(ev1)
+    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+    if ws > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(t.item())
+    n_all = w.n * ws
+    value = n_all * args.steps / (ms_max / 1e3)
+    ms_step = ms_max / args.steps
+    per_launch_s = (ms / 1e3) / args.steps
+    alg = ALG_BYTES[args.precision] * w.n
+    peak, peak_kind = measured_peak_hbm()
+    achieved = alg / per_launch_s / 1e9
+    tpp = traffic_per_particle(args.precision, args.config)
+
+    # ---- end to end through the C ABI with host buffers ------------------
+    e2e = None
+    if not args.no_e2e:
+        frame = 100
+        frames = max(1, min(20, args.steps // frame))
+        xh, th = eng.get_particles()
+        xh = np.ascontiguousarray(xh)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(frames):
+            eng.set_particles(xh, th, offsets=w.offsets)
+            eng.step(frame)
+            xh, th = eng.get_particles()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        tt = torch.tensor([dt], dtype=torch.float64, device=f"cuda:{local}")
+        if ws > 1:
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        dt = float(tt.item())
+        h2d = w.n * (3 * 8 + 4) + (len(w.offsets) * 8 if w.offsets is not None else 0)
+        d2h = w.n * (3 * 8 + 4)
+        e2e = {"value": n_all * frame * frames / dt, "unit": "particle-steps/s",
+               "h2d_bytes_per_step": h2d / frame, "d2h_bytes_per_step": d2h / frame,
+               "frame_steps": frame, "frames": frames,
+               "note": "per frame: pinned-host upload + re-binning, 100 steps, download"}
+
+    cb = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(w)
+    if rank == 0:
+        line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "f32c" else "f64",
+                "data": "synthetic",
+                "config": {"workload": w.name, "particles": w.n,
+                           "systems": len(w.boxes) if w.boxes else 1, "precision": args.precision,
+                           "parallelism": f"replicas{ws}",
+                           "l2": "inputs larger than L2 (state read+written per step exceeds 126 MB)"
+                           if alg > 126e6 else "state fits in L2"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "peak_kind": peak_kind,
+                             "traffic": (tpp * w.n if tpp else None),
+                             "kernel": "step_kernel", "alg_bytes_per_particle_step": ALG_BYTES[args.precision]},
+                "e2e": e2e, "cpu_baseline": cb, "gpu_launches": launches, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

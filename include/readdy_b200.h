@@ -1,0 +1,245 @@
+/*
+ * readdy_b200.h -- C ABI of the B200-native ReaDDy Brownian-dynamics engine.
+ *
+ * This is the boundary that replaces the reference's native GPU core
+ * (lib/ReaDDyGPU_Cpp/CudaKernels/CudaSimulation.cuh:39-116, class CudaSimulation,
+ * driven by lib/ReaDDyGPU.cpp:31 through JNI).  The JNI entry point itself
+ * (Java_readdy_impl_sim_top_TopGPU_cCreateSimulation, lib/simulationGPU.h:15-16)
+ * is declared in readdy_b200_jni.h and is built on top of these functions.
+ *
+ * Conventions
+ *   - Plain C types only; every pointer argument is a HOST pointer unless its
+ *     name ends in _dev.  The library owns all device memory of a handle.
+ *   - Every function returns an int status: RDGPU_OK (0) or a negative
+ *     RDGPU_ERR_* code (the reference's CudaSimulation methods return 0 = ok,
+ *     1 = error, CudaSimulation.cu:138-455).  rdgpu_last_error() gives the text.
+ *   - Units follow ReaDDy: nm, s, kJ/mol, K; D in nm^2/s.
+ *   - Particles are addressed by their index in the arrays handed to
+ *     rdgpu_set_particles (the reference's "gpuIndex", ReaDDyGPU.cpp:288).
+ *     All per-particle outputs come back in that order.
+ *   - There is no CPU fallback: without a usable CUDA device every compute
+ *     call fails with RDGPU_ERR_CUDA.
+ */
+#ifndef READDY_B200_H
+#define READDY_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RDGPU_ABI_VERSION 1
+
+#define RDGPU_MAX_TYPES          16
+#define RDGPU_MAX_PAIR_POTS      32
+#define RDGPU_MAX_EXT_POTS       16
+#define RDGPU_MAX_POTS_PER_PAIR  4
+
+/* status codes */
+#define RDGPU_OK              0
+#define RDGPU_ERR_ARG        -1   /* invalid argument / description          */
+#define RDGPU_ERR_CUDA       -2   /* CUDA runtime error or no device          */
+#define RDGPU_ERR_OVERFLOW   -3   /* cell occupancy cap could not be grown    */
+#define RDGPU_ERR_NONFINITE  -4   /* a particle position became NaN/Inf       */
+#define RDGPU_ERR_STATE      -5   /* call out of order (e.g. no particles)    */
+#define RDGPU_ERR_NOMEM      -6   /* device allocation failed                 */
+#define RDGPU_ERR_JUMP       -7   /* a particle moved more than a box length  */
+
+/* precision of a handle */
+#define RDGPU_PREC_F64   0   /* plain FP64 positions and forces (the drop-in)      */
+#define RDGPU_PREC_F32C  1   /* FP32 forces, Kahan-compensated FP32 positions      */
+
+/* pair (order-two) potential kinds */
+#define RDGPU_P2_HARMONIC        1  /* P2_Harmonic.java:144-234                          */
+#define RDGPU_P2_WEAK_PIECEWISE  2  /* P2_WeakInteractionPiecewiseHarmonic.java:114-206 */
+
+/* external (order-one) potential kinds */
+#define RDGPU_P1_DISK      1   /* P1_Disk.java:112-320      */
+#define RDGPU_P1_CYLINDER  2   /* P1_Cylinder.java:109-340  */
+#define RDGPU_P1_SPHERE    3   /* P1_Sphere.java:119-340    */
+#define RDGPU_P1_CUBE      4   /* P1_Cube.java (box wall)   */
+
+/* subtypes (the reference's subtype ids, Simulation.cpp:102-205) */
+#define RDGPU_SUB_ATTRACTIVE  1
+#define RDGPU_SUB_REPULSIVE   2
+#define RDGPU_SUB_SPRING      3   /* harmonic only  */
+#define RDGPU_SUB_MEMBRANE    4   /* sphere only    */
+
+typedef struct {
+    int32_t kind;                 /* RDGPU_P2_*                                       */
+    int32_t subtype;              /* RDGPU_SUB_* (ignored for WEAK_PIECEWISE)          */
+    double  k;                    /* forceConst [kJ/mol/nm^2]                          */
+    double  r0;                   /* < 0: use the pair's collision radius sum
+                                     (P2_Harmonic.java:124-128); >= 0: explicit r0   */
+    double  length;               /* WEAK_PIECEWISE: well width l                      */
+    double  depth;                /* WEAK_PIECEWISE: well depth d [kJ/mol]             */
+    uint8_t pairs[RDGPU_MAX_TYPES * RDGPU_MAX_TYPES]; /* 1: acts on (t1,t2); symmetric */
+} rdgpu_pair_pot;
+
+typedef struct {
+    int32_t kind;                 /* RDGPU_P1_*                                       */
+    int32_t subtype;              /* RDGPU_SUB_*                                      */
+    double  k;                    /* forceConst                                        */
+    double  center[3];            /* DISK, CYLINDER, SPHERE                            */
+    double  normal[3];            /* DISK, CYLINDER (normalised by the library)        */
+    double  radius;               /* DISK, CYLINDER, SPHERE                            */
+    double  height;               /* CYLINDER                                          */
+    double  origin[3];            /* CUBE                                              */
+    double  extension[3];         /* CUBE                                              */
+    int32_t consider_radius;      /* SPHERE/CUBE: use the particle radius (default 1)  */
+    uint8_t types[RDGPU_MAX_TYPES]; /* 1: acts on particles of that type               */
+} rdgpu_ext_pot;
+
+typedef struct {
+    int32_t n_types;
+    double  D[RDGPU_MAX_TYPES];                 /* diffusion constant [nm^2/s]      */
+    /* coll_radius[i*RDGPU_MAX_TYPES+j]: radius of type i when in contact with j.
+       Pair r0 = coll_radius[i][j] + coll_radius[j][i]
+       (ParticleParametersFactory.java:167-170).                                     */
+    double  coll_radius[RDGPU_MAX_TYPES * RDGPU_MAX_TYPES];
+    /* default collision radius of a type, the pRadius handed to external
+       potentials (DiffusionEngine.java:105, defaultCollRadiusMap).                  */
+    double  p_radius[RDGPU_MAX_TYPES];
+    int32_t n_pair;
+    rdgpu_pair_pot pair[RDGPU_MAX_PAIR_POTS];
+    int32_t n_ext;
+    rdgpu_ext_pot ext[RDGPU_MAX_EXT_POTS];
+    double  kB;                                 /* kJ/(mol K)                       */
+    double  T;                                  /* K                                */
+    double  dt;                                 /* BD time step [s]                 */
+    double  lo[3], hi[3];                       /* lattice bounds [nm]              */
+    int32_t periodic[3];                        /* 1: periodic along that axis      */
+    /* cutoff used for harmonic attractive/spring pairs, which have no natural
+       cutoff (the reference uses maxCutoff, ReaDDyGPU.cpp:101).  0: none allowed. */
+    double  max_cutoff;
+    /* cell edge; 0 = the largest pair cutoff.  Must be >= that cutoff.             */
+    double  cell_size;
+} rdgpu_system_desc;
+
+/* one system of a batch: its own box and Philox seed */
+typedef struct {
+    double   lo[3], hi[3];
+    int32_t  periodic[3];
+    uint64_t seed;
+} rdgpu_box;
+
+typedef struct {
+    int32_t  precision;           /* RDGPU_PREC_*                                      */
+    int32_t  device;              /* CUDA device ordinal                               */
+    int32_t  cell_cap;            /* slots per cell, power of two; 0 = automatic       */
+    int32_t  lanes_per_particle;  /* 1,2,4,8; 0 = automatic (autotuner table)          */
+    int32_t  cells_per_lane;      /* cells summed by one lane in a work item; 0 = auto */
+    int32_t  block_size;          /* threads per block of the step kernel; 0 = auto    */
+    int32_t  graph_steps;         /* steps captured per CUDA graph; 0 = 100, <0 = off  */
+    int32_t  reserved;
+    uint64_t seed;                /* Philox seed of a single-system handle             */
+} rdgpu_options;
+
+typedef struct {
+    double   energy;                    /* total potential energy [kJ/mol], FP64     */
+    double   msd[RDGPU_MAX_TYPES];      /* mean squared displacement per type [nm^2] */
+    int64_t  count[RDGPU_MAX_TYPES];    /* particles per type                        */
+    int64_t  step;                      /* steps done since rdgpu_set_particles      */
+    int32_t  cell_cap;                  /* current slots per cell                    */
+    int32_t  overflow_regrows;          /* times the cap was grown and a step redone */
+} rdgpu_metrics;
+
+typedef struct rdgpu_engine* rdgpu_handle;
+
+/* ---- lifetime ---------------------------------------------------------- */
+
+/* Single system; box from desc->lo/hi/periodic.  Replaces
+   CudaSimulation::CudaSimulation + initialize (CudaSimulation.cu:138-455).       */
+int rdgpu_create(const rdgpu_system_desc* desc, const rdgpu_options* opt,
+                 rdgpu_handle* out);
+
+/* A batch of independent replicate systems that share the particle types and
+   potentials of desc but each have their own box and seed.  All systems step
+   together in one persistent launch per step.  No reference counterpart (the
+   reference runs one system per process).                                     */
+int rdgpu_create_batch(const rdgpu_system_desc* desc, int32_t n_systems,
+                       const rdgpu_box* boxes, const rdgpu_options* opt,
+                       rdgpu_handle* out);
+
+int rdgpu_destroy(rdgpu_handle h);
+
+/* Text of the last error on this handle (or of the last failed create when
+   h is NULL).  Valid until the next call on the handle.                       */
+const char* rdgpu_last_error(rdgpu_handle h);
+
+/* ---- state ------------------------------------------------------------- */
+
+/* Upload particles (absolute coordinates, xyz interleaved) and bin them.
+   offsets: n_systems+1 prefix offsets into the arrays (NULL for a single
+   system).  Resets the step counter, the MSD origin and the RDF accumulator.
+   Replaces copyPosToDevice + copyTypesToDevice + createNeighborList +
+   copyNeighborListToDevice (CudaSimulation.cu:562-626, ReaDDyGPU.cpp:421-442). */
+int rdgpu_set_particles(rdgpu_handle h, const int64_t* offsets, int64_t n_total,
+                        const double* xyz, const int32_t* types);
+
+/* Download positions (absolute, xyz interleaved) and types in particle-index
+   order.  Replaces copyPosFromDevice (CudaSimulation.cu:2309 ff).             */
+int rdgpu_get_particles(rdgpu_handle h, double* xyz, int32_t* types);
+
+int rdgpu_num_particles(rdgpu_handle h, int64_t* n_total);
+
+/* ---- dynamics ---------------------------------------------------------- */
+
+/* Advance every system by nsteps Brownian-dynamics steps (Philox noise keyed
+   by (seed, step, particle index)).  Replaces the per-step launch sequence
+   orderOne/warpOrderTwo/groups/update (CudaSimulation.cu:2309-2476).          */
+int rdgpu_step(rdgpu_handle h, int64_t nsteps);
+
+/* One step that takes its Gaussian noise from the host array noise
+   (3 per particle, particle-index order) instead of Philox.  For parity
+   testing against the CPU path with identical noise.                         */
+int rdgpu_step_with_noise(rdgpu_handle h, const double* noise);
+
+/* Philox seed of system `sys` (single system: 0). */
+int rdgpu_set_seed(rdgpu_handle h, int32_t sys, uint64_t seed);
+
+/* ---- diagnostics and observables -------------------------------------- */
+
+/* Forces F = -grad V (pair + external) at the current positions, particle-index
+   order, 3 per particle, and the total energy.  Uses the same device code as
+   the step kernel.                                                            */
+int rdgpu_forces(rdgpu_handle h, double* forces, double* energy);
+
+/* Per particle: number of neighbours j != i with r_ij^2 < rc(ti,tj)^2 and the
+   wrapping sum of splitmix64(index_j) over them (order independent).          */
+int rdgpu_neighbor_digest(rdgpu_handle h, int32_t* counts, uint64_t* hashes);
+
+/* The Gaussian noise rdgpu_step would draw at step `step` (3 per particle). */
+int rdgpu_debug_noise(rdgpu_handle h, int64_t step, double* noise);
+
+/* RDF pair counts: for every ordered pair (i,j), i != j, in the same system
+   with r < rmax, counts[(ti*n_types+tj)*nbins + bin] += 1 where bin is the k
+   with (k*w)^2 <= r^2 < ((k+1)*w)^2, w = rmax/nbins (FP64 predicate on the
+   stored positions).  Equivalent to the reference's per-unordered-pair
+   increment of [ti][tj] and [tj][ti] (CudaSimulation.cu:1815-1818).
+   accumulate != 0 adds to the device accumulator (one "frame"); the host
+   array then receives the accumulated counts; accumulate == 0 returns only
+   this frame's counts and leaves the accumulator alone.                      */
+int rdgpu_rdf(rdgpu_handle h, int32_t nbins, double rmax, int32_t accumulate,
+              uint64_t* counts, int64_t* frames);
+
+/* g(r) of the accumulator, normalised in FP64:
+   g[ti][tj][k] = counts / (frames * N_ti * (N_tj - [ti==tj]) / V * shell_k),
+   shell_k = 4/3 pi ((k+1)^3 - k^3) w^3, V the box volume (single system).     */
+int rdgpu_rdf_normalized(rdgpu_handle h, double* g);
+
+int rdgpu_metrics_get(rdgpu_handle h, rdgpu_metrics* m);
+
+/* ---- device-resident access for benchmarks ----------------------------- */
+
+/* The cudaStream_t the handle launches on (as void*). */
+void* rdgpu_stream(rdgpu_handle h);
+
+/* Kernels launched by the last rdgpu_step (for launch accounting). */
+int64_t rdgpu_launch_count(rdgpu_handle h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* READDY_B200_H */

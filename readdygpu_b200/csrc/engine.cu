@@ -1,0 +1,1154 @@
+// engine.cu -- host side of the B200 Brownian-dynamics engine and the C ABI
+// declared in include/readdy_b200.h.
+//
+// Replaces the reference's CudaSimulation host wrapper
+// (lib/ReaDDyGPU_Cpp/CudaKernels/CudaSimulation.cu:138-626, 2309-2476):
+// device state, cell binning, per-step launches.  One stream per handle; the
+// steps of rdgpu_step are replayed from a captured CUDA graph.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/readdy_b200.h"
+#include "engine_kernels.cuh"
+
+using namespace rdgpu;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+constexpr int kBlock = 256;
+
+}  // namespace
+
+// the opaque handle type of the C ABI
+struct rdgpu_engine {
+    int prec = RDGPU_PREC_F64;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    rdgpu_system_desc desc{};
+    rdgpu_options opt{};
+    int nsys = 0;
+    std::vector<rdgpu_box> boxes;
+    std::vector<SysDev> sys_h;
+    SysDev* sys_d = nullptr;
+    std::vector<WorkItem> items_h;
+    WorkItem* items_d = nullptr;
+    void* tab_d = nullptr;
+    void* ext_d = nullptr;
+    int n_ext = 0;
+    // state
+    void* bufA[2] = {nullptr, nullptr};   // FP32: pos, FP64: records
+    void* bufB[2] = {nullptr, nullptr};   // FP32: cmp
+    int* cnt[3] = {nullptr, nullptr, nullptr};
+    int* work_ctr = nullptr;
+    int* err = nullptr;
+    long long* err_step = nullptr;
+    long long* step_d = nullptr;
+    int* scratch_i = nullptr;
+    long long ncells_tot = 0, nslots_tot = 0, npart_tot = 0;
+    std::vector<long long> part_off;     // n_sys + 1
+    std::vector<int> types_h;            // by global index
+    // dense scratch (by global particle index)
+    void* denseA = nullptr;
+    void* denseB = nullptr;
+    double* x0_d = nullptr;              // MSD origin, box-relative unwrapped
+    double* vec_d = nullptr;             // 3N doubles scratch
+    double* val_d = nullptr;             // N doubles scratch
+    int* ityp_d = nullptr;               // N ints scratch
+    unsigned long long* u64_d = nullptr; // N scratch
+    double* red_d = nullptr;             // reduction output
+    long long* redc_d = nullptr;
+    int* pinned_err = nullptr;
+    long long* pinned_step = nullptr;
+    long long step_h = 0;
+    // RDF accumulator
+    unsigned long long* rdf_acc = nullptr;
+    unsigned long long* rdf_tmp = nullptr;
+    double* rdf_e2 = nullptr;
+    int rdf_nbins = 0;
+    double rdf_rmax = 0.0;
+    long long rdf_frames = 0;
+    // CUDA graph of graph_steps steps
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 100;
+    int grid = 0;
+    int regrows = 0;
+    long long launches = 0;
+    std::string last_error;
+};
+
+namespace {
+
+using Engine = rdgpu_engine;
+
+#define CK(call)                                                                   \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) {                                                   \
+            E->last_error = std::string(#call) + ": " + cudaGetErrorString(e_);   \
+            return (e_ == cudaErrorMemoryAllocation) ? RDGPU_ERR_NOMEM : RDGPU_ERR_CUDA; \
+        }                                                                          \
+    } while (0)
+
+inline float i2f(int v) { float f; memcpy(&f, &v, 4); return f; }
+inline int f2i(float f) { int v; memcpy(&v, &f, 4); return v; }
+
+int fail(Engine* E, int code, const std::string& msg)
+{
+    E->last_error = msg;
+    return code;
+}
+
+template <class T> void dfree(T*& p)
+{
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+int ceil_log2(int v)
+{
+    int l = 0;
+    while ((1 << l) < v) ++l;
+    return l;
+}
+
+// ---------------------------------------------------------------------------
+// parameter tables
+// ---------------------------------------------------------------------------
+double pair_cutoff(const rdgpu_pair_pot& p, double r0pair, double maxc)
+{
+    double r0 = p.r0 >= 0.0 ? p.r0 : r0pair;
+    if (p.kind == RDGPU_P2_HARMONIC) return p.subtype == RDGPU_SUB_REPULSIVE ? r0 : maxc;
+    if (p.kind == RDGPU_P2_WEAK_PIECEWISE) return r0 + p.length;
+    return 0.0;
+}
+
+int validate(const rdgpu_system_desc& d, std::string& why)
+{
+    if (d.n_types < 1 || d.n_types > RDGPU_MAX_TYPES) { why = "n_types out of range"; return -1; }
+    if (d.n_pair < 0 || d.n_pair > RDGPU_MAX_PAIR_POTS) { why = "n_pair out of range"; return -1; }
+    if (d.n_ext < 0 || d.n_ext > RDGPU_MAX_EXT_POTS) { why = "n_ext out of range"; return -1; }
+    if (!(d.kB > 0 && d.T > 0 && d.dt > 0)) { why = "kB, T and dt must be positive"; return -1; }
+    for (int t = 0; t < d.n_types; ++t)
+        if (!(d.D[t] >= 0 && std::isfinite(d.D[t]))) { why = "diffusion constants must be finite and >= 0"; return -1; }
+    for (int p = 0; p < d.n_pair; ++p) {
+        const rdgpu_pair_pot& q = d.pair[p];
+        if (q.kind == RDGPU_P2_HARMONIC) {
+            if (q.subtype < 1 || q.subtype > 3) { why = "harmonic subtype must be attractive, repulsive or spring"; return -1; }
+            if (q.subtype != RDGPU_SUB_REPULSIVE && !(d.max_cutoff > 0)) {
+                why = "harmonic attractive/spring potentials need max_cutoff > 0";
+                return -1;
+            }
+        } else if (q.kind == RDGPU_P2_WEAK_PIECEWISE) {
+            if (!(q.length > 0)) { why = "weak interaction needs length > 0"; return -1; }
+        } else {
+            why = "unknown pair potential kind";
+            return -1;
+        }
+    }
+    for (int p = 0; p < d.n_ext; ++p) {
+        const rdgpu_ext_pot& q = d.ext[p];
+        if (q.kind < 1 || q.kind > 4) { why = "unknown external potential kind"; return -1; }
+        bool ok = (q.subtype == 1 || q.subtype == 2) || (q.kind == RDGPU_P1_SPHERE && q.subtype == 4);
+        if (!ok) { why = "invalid external potential subtype"; return -1; }
+        if (q.kind == 1 || q.kind == 2) {
+            double nn = std::sqrt(q.normal[0] * q.normal[0] + q.normal[1] * q.normal[1] + q.normal[2] * q.normal[2]);
+            if (!(nn > 0)) { why = "disk/cylinder normal must be non-zero"; return -1; }
+        }
+    }
+    return 0;
+}
+
+template <class R> void build_tab(const rdgpu_system_desc& d, TypeTab<R>& t, double& max_rc, std::string& why, int& bad)
+{
+    memset(&t, 0, sizeof(t));
+    t.S = d.n_types;
+    t.n_ext = d.n_ext;
+    max_rc = 0.0;
+    bad = 0;
+    const int M = RDGPU_MAX_TYPES;
+    for (int i = 0; i < d.n_types; ++i) {
+        t.a[i] = (R)(d.D[i] * d.dt / (d.kB * d.T));
+        t.b[i] = (R)std::sqrt(2.0 * d.D[i] * d.dt);
+        t.prad[i] = (R)d.p_radius[i];
+        for (int j = 0; j < d.n_types; ++j) {
+            double r0pair = d.coll_radius[i * M + j] + d.coll_radius[j * M + i];
+            double rc = 0.0;
+            int nt = 0;
+            for (int p = 0; p < d.n_pair; ++p) {
+                const rdgpu_pair_pot& q = d.pair[p];
+                if (!q.pairs[i * M + j] && !q.pairs[j * M + i]) continue;
+                double c = pair_cutoff(q, r0pair, d.max_cutoff);
+                if (c > rc) rc = c;
+                if (nt >= MAX_TERMS) { bad = 1; why = "more than 4 pair potentials on one type pair"; return; }
+                PairTerm<R>& pt = t.term[(i * MAXT + j) * MAX_TERMS + nt];
+                pt.kind = q.kind;
+                pt.sub = q.subtype;
+                pt.k = (R)q.k;
+                pt.r0 = (R)(q.r0 >= 0.0 ? q.r0 : r0pair);
+                pt.l = (R)q.length;
+                pt.d = (R)q.depth;
+                double qq = q.length > 0 ? (1.0 / (0.5 * q.length)) * (1.0 / (0.5 * q.length)) : 0.0;
+                pt.q = (R)qq;
+                ++nt;
+            }
+            t.nterm[i * MAXT + j] = nt;
+            t.rc2[i * MAXT + j] = (R)(rc * rc);
+            if (rc > max_rc) max_rc = rc;
+        }
+    }
+}
+
+template <class R> void build_ext(const rdgpu_system_desc& d, const rdgpu_box& b, ExtTerm<R>* out)
+{
+    for (int p = 0; p < d.n_ext; ++p) {
+        const rdgpu_ext_pot& q = d.ext[p];
+        ExtTerm<R> e;
+        memset(&e, 0, sizeof(e));
+        e.kind = q.kind;
+        e.sub = q.subtype;
+        e.k = (R)q.k;
+        double nn = std::sqrt(q.normal[0] * q.normal[0] + q.normal[1] * q.normal[1] + q.normal[2] * q.normal[2]);
+        for (int a = 0; a < 3; ++a) {
+            e.c[a] = (R)(q.center[a] - b.lo[a]);
+            e.nrm[a] = nn > 0 ? (R)(q.normal[a] / nn) : R(0);
+            double lo = q.origin[a], hi = q.origin[a] + q.extension[a];
+            if (!(lo < hi)) std::swap(lo, hi);
+            e.blo[a] = (R)(lo - b.lo[a]);
+            e.bhi[a] = (R)(hi - b.lo[a]);
+        }
+        e.rad = (R)q.radius;
+        e.h = (R)q.height;
+        e.consider = q.consider_radius;
+        e.tmask = 0;
+        for (int t = 0; t < d.n_types; ++t)
+            if (q.types[t]) e.tmask |= (1u << t);
+        out[p] = e;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// buffers
+// ---------------------------------------------------------------------------
+void free_state(Engine* E)
+{
+    for (int i = 0; i < 2; ++i) { dfree(E->bufA[i]); dfree(E->bufB[i]); }
+    for (int i = 0; i < 3; ++i) dfree(E->cnt[i]);
+    if (E->graph) { cudaGraphExecDestroy(E->graph); E->graph = nullptr; }
+}
+
+void free_particles(Engine* E)
+{
+    dfree(E->denseA); dfree(E->denseB); dfree(E->x0_d); dfree(E->vec_d); dfree(E->val_d);
+    dfree(E->ityp_d); dfree(E->u64_d);
+}
+
+size_t rec_bytes(int prec) { return prec == RDGPU_PREC_F32C ? 16 : 32; }
+
+// lay out cells/slots of all systems for the current caps and allocate
+int alloc_state(Engine* E)
+{
+    free_state(E);
+    long long cb = 0, sb = 0;
+    for (int s = 0; s < E->nsys; ++s) {
+        SysDev& d = E->sys_h[s];
+        d.cell_base = cb;
+        d.slot_base = sb;
+        cb += d.ncells;
+        sb += (long long)d.ncells << d.cap_log2;
+    }
+    E->ncells_tot = cb;
+    E->nslots_tot = sb;
+    const size_t rb = rec_bytes(E->prec);
+    for (int i = 0; i < 2; ++i) {
+        CK(cudaMalloc(&E->bufA[i], std::max<long long>(sb, 1) * rb));
+        if (E->prec == RDGPU_PREC_F32C) CK(cudaMalloc(&E->bufB[i], std::max<long long>(sb, 1) * 16));
+    }
+    for (int i = 0; i < 3; ++i) {
+        CK(cudaMalloc(&E->cnt[i], std::max<long long>(cb, 1) * sizeof(int)));
+        CK(cudaMemsetAsync(E->cnt[i], 0, std::max<long long>(cb, 1) * sizeof(int), E->stream));
+    }
+    CK(cudaMemcpyAsync(E->sys_d, E->sys_h.data(), E->nsys * sizeof(SysDev), cudaMemcpyHostToDevice, E->stream));
+    return RDGPU_OK;
+}
+
+// work items: runs of 32*cpl cells of one system
+int build_items(Engine* E)
+{
+    E->items_h.clear();
+    for (int s = 0; s < E->nsys; ++s) {
+        const SysDev& d = E->sys_h[s];
+        int cpl = E->opt.cells_per_lane;
+        if (cpl <= 0) {
+            double occ = d.ncells > 0 ? (double)d.npart / d.ncells : 0.0;
+            // about 96 particles per work item
+            cpl = occ > 0 ? (int)std::lround(96.0 / (32.0 * occ)) : CPL_MAX;
+        }
+        cpl = std::min(std::max(cpl, 1), CPL_MAX);
+        const int span = 32 * cpl;
+        for (int c0 = 0; c0 < d.ncells; c0 += span) {
+            WorkItem it;
+            it.sys = s;
+            it.c0 = c0;
+            it.c1 = std::min(d.ncells, c0 + span);
+            it.cpl = cpl;
+            E->items_h.push_back(it);
+        }
+    }
+    dfree(E->items_d);
+    CK(cudaMalloc(&E->items_d, std::max<size_t>(E->items_h.size(), 1) * sizeof(WorkItem)));
+    CK(cudaMemcpyAsync(E->items_d, E->items_h.data(), E->items_h.size() * sizeof(WorkItem),
+                       cudaMemcpyHostToDevice, E->stream));
+    return RDGPU_OK;
+}
+
+template <class R> StepArgs<R> make_args(Engine* E)
+{
+    StepArgs<R> a;
+    memset(&a, 0, sizeof(a));
+    a.sys = E->sys_d;
+    a.items = E->items_d;
+    a.nitems = (int)E->items_h.size();
+    a.n_ext = E->n_ext;
+    a.tab = (const TypeTab<R>*)E->tab_d;
+    a.ext = (const ExtTerm<R>*)E->ext_d;
+    for (int i = 0; i < 2; ++i) {
+        if constexpr (sizeof(R) == 4) {
+            a.buf[i].pos = (float4*)E->bufA[i];
+            a.buf[i].cmp = (float4*)E->bufB[i];
+        } else {
+            a.buf[i].st = (Rec64*)E->bufA[i];
+        }
+    }
+    for (int i = 0; i < 3; ++i) a.cnt[i] = E->cnt[i];
+    a.work_ctr = E->work_ctr;
+    a.err = E->err;
+    a.err_step = E->err_step;
+    a.step_ptr = E->step_d;
+    a.step_off = 0;
+    a.noise = nullptr;
+    return a;
+}
+
+template <class R> StateBuf<R> sbuf(Engine* E, int i)
+{
+    StateBuf<R> b;
+    if constexpr (sizeof(R) == 4) { b.pos = (float4*)E->bufA[i]; b.cmp = (float4*)E->bufB[i]; }
+    else b.st = (Rec64*)E->bufA[i];
+    return b;
+}
+
+template <class R> Dense<R> dense(Engine* E)
+{
+    Dense<R> d;
+    if constexpr (sizeof(R) == 4) { d.pos = (float4*)E->denseA; d.cmp = (float4*)E->denseB; }
+    else d.st = (Rec64*)E->denseA;
+    return d;
+}
+
+int grid_for(long long n, int block = 256)
+{
+    long long g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > 148 * 32) g = 148 * 32;
+    return (int)g;
+}
+
+// bin the dense arrays into buffer `bi` with counts `ci`; grows caps on overflow
+template <class R> int bin_dense(Engine* E, int bi, int ci)
+{
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        CK(cudaMemsetAsync(E->cnt[ci], 0, std::max<long long>(E->ncells_tot, 1) * sizeof(int), E->stream));
+        CK(cudaMemsetAsync(E->err, 0, sizeof(int), E->stream));
+        if (E->npart_tot > 0) {
+            bin_kernel<R><<<grid_for(E->npart_tot), 256, 0, E->stream>>>(
+                E->sys_d, E->nsys, E->npart_tot, dense<R>(E), sbuf<R>(E, bi), E->cnt[ci], E->err);
+            CK(cudaGetLastError());
+        }
+        CK(cudaMemcpyAsync(E->pinned_err, E->err, sizeof(int), cudaMemcpyDeviceToHost, E->stream));
+        CK(cudaStreamSynchronize(E->stream));
+        if (*E->pinned_err == 0) return RDGPU_OK;
+        // occupancy per system from the complete counts, then re-layout
+        std::vector<int> counts(E->ncells_tot);
+        CK(cudaMemcpy(counts.data(), E->cnt[ci], E->ncells_tot * sizeof(int), cudaMemcpyDeviceToHost));
+        for (int s = 0; s < E->nsys; ++s) {
+            SysDev& d = E->sys_h[s];
+            int m = 0;
+            for (int c = 0; c < d.ncells; ++c) m = std::max(m, counts[d.cell_base + c]);
+            int want = ceil_log2(std::max(8, 2 * m));
+            if (want > d.cap_log2) d.cap_log2 = want;
+        }
+        int rc = alloc_state(E);
+        if (rc) return rc;
+        ++E->regrows;
+    }
+    return fail(E, RDGPU_ERR_OVERFLOW, "cell occupancy cap could not be grown");
+}
+
+template <class R> int gather_dense(Engine* E, int bi, int ci)
+{
+    if (E->npart_tot == 0) return RDGPU_OK;
+    gather_kernel<R><<<grid_for(E->ncells_tot), 256, 0, E->stream>>>(E->sys_d, E->nsys, E->ncells_tot,
+                                                                       sbuf<R>(E, bi), E->cnt[ci], dense<R>(E));
+    CK(cudaGetLastError());
+    return RDGPU_OK;
+}
+
+int reset_counters(Engine* E, long long t)
+{
+    CK(cudaMemsetAsync(E->work_ctr, 0, 3 * sizeof(int), E->stream));
+    CK(cudaMemsetAsync(E->err, 0, sizeof(int), E->stream));
+    const long long big = 0x7fffffffffffffffLL;
+    CK(cudaMemcpyAsync(E->err_step, &big, sizeof(long long), cudaMemcpyHostToDevice, E->stream));
+    CK(cudaMemcpyAsync(E->step_d, &t, sizeof(long long), cudaMemcpyHostToDevice, E->stream));
+    CK(cudaStreamSynchronize(E->stream));
+    E->step_h = t;
+    return RDGPU_OK;
+}
+
+// the state of step t sits in buffer t&1 with counts t%3; counts (t+1)%3 must
+// be zero before step t runs
+int prepare_step_state(Engine* E, long long t)
+{
+    const int nxt = (int)((t + 1) % 3);
+    CK(cudaMemsetAsync(E->cnt[nxt], 0, std::max<long long>(E->ncells_tot, 1) * sizeof(int), E->stream));
+    return reset_counters(E, t);
+}
+
+template <class R> int launch_steps(Engine* E, int n, const double* noise_d)
+{
+    StepArgs<R> a = make_args<R>(E);
+    a.noise = noise_d;
+    for (int k = 0; k < n; ++k) {
+        a.step_off = k;
+        step_kernel<R, kBlock><<<E->grid, kBlock, 0, E->stream>>>(a);
+        ++E->launches;
+    }
+    advance_kernel<<<1, 32, 0, E->stream>>>(E->step_d, E->err, n);
+    ++E->launches;
+    CK(cudaGetLastError());
+    return RDGPU_OK;
+}
+
+template <class R> int capture_graph(Engine* E)
+{
+    if (E->graph) return RDGPU_OK;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(E->stream, cudaStreamCaptureModeThreadLocal));
+    long long l0 = E->launches;
+    int rc = launch_steps<R>(E, E->graph_steps, nullptr);
+    cudaError_t ce = cudaStreamEndCapture(E->stream, &g);
+    E->launches = l0;
+    if (rc) return rc;
+    CK(ce);
+    CK(cudaGraphInstantiate(&E->graph, g, 0));
+    cudaGraphDestroy(g);
+    return RDGPU_OK;
+}
+
+// after an overflow at step tf: regrow the caps of the next layout and resume
+template <class R> int recover_overflow(Engine* E, long long tf)
+{
+    const int bi = (int)(tf & 1), ci = (int)(tf % 3), nci = (int)((tf + 1) % 3);
+    // the claimed counts of the failed next layout are complete: size from them
+    std::vector<int> counts(E->ncells_tot);
+    CK(cudaMemcpy(counts.data(), E->cnt[nci], E->ncells_tot * sizeof(int), cudaMemcpyDeviceToHost));
+    int rc = gather_dense<R>(E, bi, ci);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(E->stream));
+    for (int s = 0; s < E->nsys; ++s) {
+        SysDev& d = E->sys_h[s];
+        int m = 0;
+        for (int c = 0; c < d.ncells; ++c) m = std::max(m, counts[d.cell_base + c]);
+        int want = ceil_log2(std::max(8, 2 * m));
+        if (want > d.cap_log2) d.cap_log2 = want;
+    }
+    rc = alloc_state(E);
+    if (rc) return rc;
+    rc = bin_dense<R>(E, bi, ci);
+    if (rc) return rc;
+    ++E->regrows;
+    return prepare_step_state(E, tf);
+}
+
+template <class R> int do_steps(Engine* E, long long nsteps, const double* noise_d)
+{
+    const long long target = E->step_h + nsteps;
+    for (int round = 0; round < 16; ++round) {
+        long long remaining = target - E->step_h;
+        if (remaining <= 0) return RDGPU_OK;
+        int rc;
+        if (E->graph_steps > 0 && !noise_d && remaining >= E->graph_steps) {
+            rc = capture_graph<R>(E);
+            if (rc) return rc;
+            long long ng = remaining / E->graph_steps;
+            for (long long g = 0; g < ng; ++g) {
+                CK(cudaGraphLaunch(E->graph, E->stream));
+                E->launches += E->graph_steps + 1;
+            }
+            remaining -= ng * E->graph_steps;
+        }
+        while (remaining > 0) {
+            int n = (int)std::min<long long>(remaining, 1000);
+            rc = launch_steps<R>(E, n, noise_d);
+            if (rc) return rc;
+            remaining -= n;
+        }
+        CK(cudaMemcpyAsync(E->pinned_err, E->err, sizeof(int), cudaMemcpyDeviceToHost, E->stream));
+        CK(cudaMemcpyAsync(E->pinned_step, E->err_step, sizeof(long long), cudaMemcpyDeviceToHost, E->stream));
+        CK(cudaStreamSynchronize(E->stream));
+        const int ef = *E->pinned_err;
+        if (ef == 0) {
+            E->step_h = target;
+            return RDGPU_OK;
+        }
+        const long long tf = *E->pinned_step;
+        if (ef & EF_NONFINITE) {
+            prepare_step_state(E, tf);
+            return fail(E, RDGPU_ERR_NONFINITE, "a particle position became non-finite at step " + std::to_string(tf));
+        }
+        if (ef & EF_JUMP) {
+            prepare_step_state(E, tf);
+            return fail(E, RDGPU_ERR_JUMP, "a particle moved more than a box length at step " + std::to_string(tf));
+        }
+        rc = recover_overflow<R>(E, tf);
+        if (rc) return rc;
+    }
+    return fail(E, RDGPU_ERR_OVERFLOW, "repeated cell overflow");
+}
+
+// host conversion of absolute coordinates into the stored representation
+// (the same IEEE operations as the oracle's orc_to_rel_f64 / orc_to_rel_f32)
+double wrap_rel(double x, double L, int per)
+{
+    if (!per) return x;
+    while (x >= L) x -= L;
+    while (x < 0.0) x += L;
+    if (x >= L) x = 0.0;
+    return x;
+}
+
+int setup_systems(Engine* E, std::string& why)
+{
+    const rdgpu_system_desc& d = E->desc;
+    double max_rc = 0.0;
+    int bad = 0;
+    size_t tabsz;
+    std::vector<char> tabbuf;
+    if (E->prec == RDGPU_PREC_F32C) {
+        tabsz = sizeof(TypeTab<float>);
+        tabbuf.resize(tabsz);
+        build_tab<float>(d, *(TypeTab<float>*)tabbuf.data(), max_rc, why, bad);
+    } else {
+        tabsz = sizeof(TypeTab<double>);
+        tabbuf.resize(tabsz);
+        build_tab<double>(d, *(TypeTab<double>*)tabbuf.data(), max_rc, why, bad);
+    }
+    if (bad) return -1;
+    double cut = d.cell_size > 0.0 ? d.cell_size : max_rc;
+    if (d.cell_size > 0.0 && d.cell_size < max_rc) { why = "cell_size is smaller than the largest pair cutoff"; return -1; }
+    E->sys_h.assign(E->nsys, SysDev{});
+    for (int s = 0; s < E->nsys; ++s) {
+        const rdgpu_box& b = E->boxes[s];
+        SysDev& v = E->sys_h[s];
+        memset(&v, 0, sizeof(v));
+        long long nc = 1;
+        for (int a = 0; a < 3; ++a) {
+            double L = b.hi[a] - b.lo[a];
+            if (!(L > 0)) { why = "box bounds must satisfy hi > lo"; return -1; }
+            float Lf = (float)L;
+            double Lp = (E->prec == RDGPU_PREC_F32C) ? (double)Lf : L;
+            if (b.periodic[a] && max_rc > 0.0 && Lp < 2.0 * max_rc) {
+                why = "periodic box edge shorter than twice the pair cutoff (minimum image)";
+                return -1;
+            }
+            int n = 1;
+            if (cut > 0.0) {
+                double q = std::floor(Lp / (cut * (1.0 + 1e-5)));
+                n = (int)std::max(1.0, std::min(q, 2048.0));
+            }
+            v.n[a] = n;
+            v.per[a] = b.periodic[a] ? 1 : 0;
+            v.Lf[a] = Lf;
+            v.halff[a] = 0.5f * Lf;
+            v.invcf[a] = (float)((double)n / (double)Lf);
+            v.L[a] = L;
+            v.half[a] = 0.5 * L;
+            v.invc[a] = (double)n / Lp;
+            v.lo[a] = b.lo[a];
+            nc *= n;
+        }
+        if (nc > (1LL << 26)) { why = "too many cells in one system (box / cutoff too large)"; return -1; }
+        v.ncells = (int)nc;
+        v.cap_log2 = E->opt.cell_cap > 0 ? ceil_log2(E->opt.cell_cap) : 3;
+        v.seed = b.seed;
+        v.lanes_log2 = 0;
+    }
+    if (cudaMalloc(&E->tab_d, tabsz) != cudaSuccess) { why = "cudaMalloc failed"; return -2; }
+    cudaMemcpy(E->tab_d, tabbuf.data(), tabsz, cudaMemcpyHostToDevice);
+    E->n_ext = d.n_ext;
+    size_t esz = (E->prec == RDGPU_PREC_F32C ? sizeof(ExtTerm<float>) : sizeof(ExtTerm<double>)) *
+                 std::max(1, E->nsys * d.n_ext);
+    std::vector<char> ebuf(esz);
+    for (int s = 0; s < E->nsys; ++s) {
+        if (E->prec == RDGPU_PREC_F32C) build_ext<float>(d, E->boxes[s], (ExtTerm<float>*)ebuf.data() + s * d.n_ext);
+        else build_ext<double>(d, E->boxes[s], (ExtTerm<double>*)ebuf.data() + s * d.n_ext);
+    }
+    if (cudaMalloc(&E->ext_d, esz) != cudaSuccess) { why = "cudaMalloc failed"; return -2; }
+    cudaMemcpy(E->ext_d, ebuf.data(), esz, cudaMemcpyHostToDevice);
+    return 0;
+}
+
+template <class R> int set_particles_impl(Engine* E, const long long* offsets, long long ntot,
+                                          const double* xyz, const int* types)
+{
+    // validate everything before touching the handle's state
+    std::vector<long long> off;
+    if (E->nsys == 1) {
+        off = {0, ntot};
+    } else {
+        if (!offsets) return fail(E, RDGPU_ERR_ARG, "offsets required for a batch");
+        off.assign(offsets, offsets + E->nsys + 1);
+        if (off[0] != 0 || off[E->nsys] != ntot)
+            return fail(E, RDGPU_ERR_ARG, "offsets must start at 0 and end at n_total");
+    }
+    for (int s = 0; s < E->nsys; ++s) {
+        long long n = off[s + 1] - off[s];
+        if (n < 0 || n > 0x7fffffff) return fail(E, RDGPU_ERR_ARG, "invalid particle count");
+    }
+    for (long long g = 0; g < ntot; ++g)
+        if (types[g] < 0 || types[g] >= E->desc.n_types) return fail(E, RDGPU_ERR_ARG, "particle type out of range");
+    for (long long g = 0; g < 3 * ntot; ++g)
+        if (!std::isfinite(xyz[g])) return fail(E, RDGPU_ERR_ARG, "non-finite coordinate");
+    E->part_off.clear();   // no valid state until this call completes
+    for (int s = 0; s < E->nsys; ++s) {
+        E->sys_h[s].part_base = off[s];
+        E->sys_h[s].npart = (int)(off[s + 1] - off[s]);
+    }
+    E->npart_tot = ntot;
+    E->types_h.assign(types, types + ntot);
+    free_particles(E);
+    const long long N = std::max<long long>(ntot, 1);
+    CK(cudaMalloc(&E->denseA, N * rec_bytes(E->prec)));
+    if (E->prec == RDGPU_PREC_F32C) CK(cudaMalloc(&E->denseB, N * 16));
+    CK(cudaMalloc(&E->x0_d, N * 3 * sizeof(double)));
+    CK(cudaMalloc(&E->vec_d, N * 3 * sizeof(double)));
+    CK(cudaMalloc(&E->val_d, N * sizeof(double)));
+    CK(cudaMalloc(&E->ityp_d, N * sizeof(int)));
+    CK(cudaMalloc(&E->u64_d, N * sizeof(unsigned long long)));
+    // host conversion into the stored representation
+    std::vector<double> x0(3 * N);
+    if constexpr (sizeof(R) == 4) {
+        std::vector<float4> hp(N), hc(N);
+        for (int s = 0; s < E->nsys; ++s) {
+            const SysDev& v = E->sys_h[s];
+            for (long long g = off[s]; g < off[s + 1]; ++g) {
+                float h[3], c[3];
+                for (int a = 0; a < 3; ++a) {
+                    const float Lf = v.Lf[a];
+                    double xr = wrap_rel(xyz[3 * g + a] - v.lo[a], (double)Lf, v.per[a]);
+                    float hh = (float)xr;
+                    if (v.per[a] && hh >= Lf) { hh = 0.0f; xr -= (double)Lf; }
+                    h[a] = hh;
+                    c[a] = (float)((double)hh - xr);
+                    x0[3 * g + a] = xr;
+                }
+                hp[g] = make_float4(h[0], h[1], h[2], i2f(types[g]));
+                hc[g] = make_float4(c[0], c[1], c[2], i2f((int)(g - off[s])));
+            }
+        }
+        CK(cudaMemcpyAsync(E->denseA, hp.data(), ntot * 16, cudaMemcpyHostToDevice, E->stream));
+        CK(cudaMemcpyAsync(E->denseB, hc.data(), ntot * 16, cudaMemcpyHostToDevice, E->stream));
+        CK(cudaMemcpyAsync(E->x0_d, x0.data(), ntot * 3 * sizeof(double), cudaMemcpyHostToDevice, E->stream));
+        CK(cudaStreamSynchronize(E->stream));
+    } else {
+        std::vector<Rec64> hr(N);
+        for (int s = 0; s < E->nsys; ++s) {
+            const SysDev& v = E->sys_h[s];
+            for (long long g = off[s]; g < off[s + 1]; ++g) {
+                Rec64 r;
+                double* xr[3] = {&r.x, &r.y, &r.z};
+                for (int a = 0; a < 3; ++a) {
+                    *xr[a] = wrap_rel(xyz[3 * g + a] - v.lo[a], v.L[a], v.per[a]);
+                    x0[3 * g + a] = *xr[a];
+                }
+                r.w = types[g];
+                r.id = (int)(g - off[s]);
+                hr[g] = r;
+            }
+        }
+        CK(cudaMemcpyAsync(E->denseA, hr.data(), ntot * 32, cudaMemcpyHostToDevice, E->stream));
+        CK(cudaMemcpyAsync(E->x0_d, x0.data(), ntot * 3 * sizeof(double), cudaMemcpyHostToDevice, E->stream));
+        CK(cudaStreamSynchronize(E->stream));
+    }
+    // lay out with the current caps and bin (caps grow on overflow)
+    int rc = alloc_state(E);
+    if (rc) return rc;
+    rc = bin_dense<R>(E, 0, 0);
+    if (rc) return rc;
+    rc = build_items(E);
+    if (rc) return rc;
+    // per-system lanes per particle: from the options or the size-bucket table
+    for (int s = 0; s < E->nsys; ++s) {
+        int L = E->opt.lanes_per_particle;
+        if (L <= 0) L = 1;
+        E->sys_h[s].lanes_log2 = ceil_log2(std::min(std::max(L, 1), 8));
+    }
+    CK(cudaMemcpyAsync(E->sys_d, E->sys_h.data(), E->nsys * sizeof(SysDev), cudaMemcpyHostToDevice, E->stream));
+    dfree(E->rdf_acc);
+    E->rdf_frames = 0;
+    E->rdf_nbins = 0;
+    rc = prepare_step_state(E, 0);
+    if (rc) return rc;
+    E->part_off = off;
+    return RDGPU_OK;
+}
+
+template <class R> int get_particles_impl(Engine* E, double* xyz, int* types)
+{
+    const long long t = E->step_h;
+    int rc = gather_dense<R>(E, (int)(t & 1), (int)(t % 3));
+    if (rc) return rc;
+    const long long N = E->npart_tot;
+    if constexpr (sizeof(R) == 4) {
+        std::vector<float4> hp(N), hc(N);
+        CK(cudaMemcpyAsync(hp.data(), E->denseA, N * 16, cudaMemcpyDeviceToHost, E->stream));
+        CK(cudaMemcpyAsync(hc.data(), E->denseB, N * 16, cudaMemcpyDeviceToHost, E->stream));
+        CK(cudaStreamSynchronize(E->stream));
+        for (int s = 0; s < E->nsys; ++s) {
+            const SysDev& v = E->sys_h[s];
+            for (long long g = E->part_off[s]; g < E->part_off[s + 1]; ++g) {
+                if (xyz) {
+                    xyz[3 * g + 0] = ((double)hp[g].x - (double)hc[g].x) + v.lo[0];
+                    xyz[3 * g + 1] = ((double)hp[g].y - (double)hc[g].y) + v.lo[1];
+                    xyz[3 * g + 2] = ((double)hp[g].z - (double)hc[g].z) + v.lo[2];
+                }
+                if (types) types[g] = f2i(hp[g].w) & 0xff;
+            }
+        }
+    } else {
+        std::vector<Rec64> hr(N);
+        CK(cudaMemcpyAsync(hr.data(), E->denseA, N * 32, cudaMemcpyDeviceToHost, E->stream));
+        CK(cudaStreamSynchronize(E->stream));
+        for (int s = 0; s < E->nsys; ++s) {
+            const SysDev& v = E->sys_h[s];
+            for (long long g = E->part_off[s]; g < E->part_off[s + 1]; ++g) {
+                if (xyz) {
+                    xyz[3 * g + 0] = hr[g].x + v.lo[0];
+                    xyz[3 * g + 1] = hr[g].y + v.lo[1];
+                    xyz[3 * g + 2] = hr[g].z + v.lo[2];
+                }
+                if (types) types[g] = hr[g].w & 0xff;
+            }
+        }
+    }
+    return RDGPU_OK;
+}
+
+template <class R> int forces_impl(Engine* E, double* forces, double* energy)
+{
+    const long long t = E->step_h;
+    StepArgs<R> a = make_args<R>(E);
+    diag_kernel<R, 1><<<grid_for(E->ncells_tot), 256, 0, E->stream>>>(
+        a, E->nsys, E->ncells_tot, (int)(t & 1), (int)(t % 3), E->vec_d, E->val_d, nullptr, nullptr);
+    CK(cudaGetLastError());
+    if (forces) CK(cudaMemcpyAsync(forces, E->vec_d, E->npart_tot * 3 * sizeof(double), cudaMemcpyDeviceToHost, E->stream));
+    if (energy) {
+        CK(cudaMemsetAsync(E->ityp_d, 0, std::max<long long>(E->npart_tot, 1) * sizeof(int), E->stream));
+        typed_sum_kernel<<<1, 256, 256 * 16, E->stream>>>(E->val_d, E->ityp_d, E->npart_tot, 0, E->red_d, E->redc_d);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(energy, E->red_d, sizeof(double), cudaMemcpyDeviceToHost, E->stream));
+    }
+    CK(cudaStreamSynchronize(E->stream));
+    return RDGPU_OK;
+}
+
+template <class R> int digest_impl(Engine* E, int* counts, unsigned long long* hashes)
+{
+    const long long t = E->step_h;
+    StepArgs<R> a = make_args<R>(E);
+    diag_kernel<R, 2><<<grid_for(E->ncells_tot), 256, 0, E->stream>>>(
+        a, E->nsys, E->ncells_tot, (int)(t & 1), (int)(t % 3), nullptr, nullptr, E->ityp_d, E->u64_d);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(counts, E->ityp_d, E->npart_tot * sizeof(int), cudaMemcpyDeviceToHost, E->stream));
+    CK(cudaMemcpyAsync(hashes, E->u64_d, E->npart_tot * sizeof(unsigned long long), cudaMemcpyDeviceToHost, E->stream));
+    CK(cudaStreamSynchronize(E->stream));
+    return RDGPU_OK;
+}
+
+__global__ void add_u64_kernel(unsigned long long* acc, const unsigned long long* v, int n)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) acc[i] += v[i];
+}
+
+// FP64 RDF normalisation on the device
+__global__ void rdf_norm_kernel(const unsigned long long* c, int S, int nbins, double w, double frames,
+                                double vol, const long long* nper, double* g)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S * S * nbins) return;
+    int k = i % nbins, tj = (i / nbins) % S, ti = i / (nbins * S);
+    const double pi = 3.14159265358979323846;
+    double r0 = k * w, r1 = (k + 1) * w;
+    double shell = 4.0 / 3.0 * pi * (r1 * r1 * r1 - r0 * r0 * r0);
+    double pairs = (double)nper[ti] * (double)(nper[tj] - (ti == tj ? 1 : 0));
+    double denom = frames * pairs / vol * shell;
+    g[i] = denom > 0 ? (double)c[i] / denom : 0.0;
+}
+
+template <class R> int rdf_impl(Engine* E, int nbins, double rmax, int accumulate, unsigned long long* out, long long* frames)
+{
+    const int S = E->desc.n_types;
+    const int H = S * S * nbins;
+    if (E->rdf_nbins != nbins || E->rdf_rmax != rmax) {
+        dfree(E->rdf_acc); dfree(E->rdf_tmp); dfree(E->rdf_e2);
+        CK(cudaMalloc(&E->rdf_acc, H * sizeof(unsigned long long)));
+        CK(cudaMalloc(&E->rdf_tmp, H * sizeof(unsigned long long)));
+        CK(cudaMalloc(&E->rdf_e2, (nbins + 1) * sizeof(double)));
+        CK(cudaMemsetAsync(E->rdf_acc, 0, H * sizeof(unsigned long long), E->stream));
+        std::vector<double> e2(nbins + 1);
+        const double w = rmax / (double)nbins;
+        for (int k = 0; k <= nbins; ++k) { double e = (double)k * w; e2[k] = e * e; }
+        CK(cudaMemcpyAsync(E->rdf_e2, e2.data(), (nbins + 1) * sizeof(double), cudaMemcpyHostToDevice, E->stream));
+        CK(cudaStreamSynchronize(E->stream));
+        E->rdf_nbins = nbins;
+        E->rdf_rmax = rmax;
+        E->rdf_frames = 0;
+    }
+    CK(cudaMemsetAsync(E->rdf_tmp, 0, H * sizeof(unsigned long long), E->stream));
+    const long long t = E->step_h;
+    const int use_smem = (H * 4 <= 48 * 1024) ? 1 : 0;
+    rdf_kernel<R><<<grid_for(E->ncells_tot, 128), 128, use_smem ? H * 4 : 0, E->stream>>>(
+        E->sys_d, E->nsys, E->ncells_tot, sbuf<R>(E, (int)(t & 1)), E->cnt[t % 3], S, nbins, E->rdf_e2,
+        rmax / (double)nbins, use_smem, E->rdf_tmp);
+    CK(cudaGetLastError());
+    if (accumulate) {
+        add_u64_kernel<<<(H + 255) / 256, 256, 0, E->stream>>>(E->rdf_acc, E->rdf_tmp, H);
+        CK(cudaGetLastError());
+        E->rdf_frames++;
+        if (out) CK(cudaMemcpyAsync(out, E->rdf_acc, H * sizeof(unsigned long long), cudaMemcpyDeviceToHost, E->stream));
+    } else if (out) {
+        CK(cudaMemcpyAsync(out, E->rdf_tmp, H * sizeof(unsigned long long), cudaMemcpyDeviceToHost, E->stream));
+    }
+    CK(cudaStreamSynchronize(E->stream));
+    if (frames) *frames = E->rdf_frames;
+    return RDGPU_OK;
+}
+
+template <class R> int msd_impl(Engine* E, rdgpu_metrics* m)
+{
+    const long long t = E->step_h;
+    const int S = E->desc.n_types;
+    msd_kernel<R><<<grid_for(E->ncells_tot), 256, 0, E->stream>>>(E->sys_d, E->nsys, E->ncells_tot,
+                                                                    sbuf<R>(E, (int)(t & 1)), E->cnt[t % 3],
+                                                                    E->x0_d, E->val_d, E->ityp_d);
+    CK(cudaGetLastError());
+    typed_sum_kernel<<<S, 256, 256 * 16, E->stream>>>(E->val_d, E->ityp_d, E->npart_tot, S, E->red_d, E->redc_d);
+    CK(cudaGetLastError());
+    std::vector<double> sums(S);
+    std::vector<long long> cnts(S);
+    CK(cudaMemcpyAsync(sums.data(), E->red_d, S * sizeof(double), cudaMemcpyDeviceToHost, E->stream));
+    CK(cudaMemcpyAsync(cnts.data(), E->redc_d, S * sizeof(long long), cudaMemcpyDeviceToHost, E->stream));
+    CK(cudaStreamSynchronize(E->stream));
+    for (int i = 0; i < S; ++i) {
+        m->count[i] = cnts[i];
+        m->msd[i] = cnts[i] > 0 ? sums[i] / (double)cnts[i] : 0.0;
+    }
+    return RDGPU_OK;
+}
+
+int create_impl(const rdgpu_system_desc* desc, int nsys, const rdgpu_box* boxes, const rdgpu_options* opt,
+                rdgpu_handle* out)
+{
+    if (!desc || !out || nsys < 1 || (nsys > 1 && !boxes)) {
+        g_create_error = "null argument or no systems";
+        return RDGPU_ERR_ARG;
+    }
+    std::string why;
+    if (validate(*desc, why)) {
+        g_create_error = why;
+        return RDGPU_ERR_ARG;
+    }
+    rdgpu_options o{};
+    if (opt) o = *opt;
+    if (o.precision != RDGPU_PREC_F64 && o.precision != RDGPU_PREC_F32C) {
+        g_create_error = "unknown precision";
+        return RDGPU_ERR_ARG;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) {
+        g_create_error = "no CUDA device (this library has no CPU fallback)";
+        return RDGPU_ERR_CUDA;
+    }
+    if (o.device < 0 || o.device >= ndev) {
+        g_create_error = "device ordinal out of range";
+        return RDGPU_ERR_ARG;
+    }
+    if (cudaSetDevice(o.device) != cudaSuccess) {
+        g_create_error = "cudaSetDevice failed";
+        return RDGPU_ERR_CUDA;
+    }
+    Engine* E = new Engine();
+    E->prec = o.precision;
+    E->device = o.device;
+    E->desc = *desc;
+    E->opt = o;
+    E->nsys = nsys;
+    if (nsys == 1 && !boxes) {
+        rdgpu_box b{};
+        for (int a = 0; a < 3; ++a) { b.lo[a] = desc->lo[a]; b.hi[a] = desc->hi[a]; b.periodic[a] = desc->periodic[a]; }
+        b.seed = o.seed;
+        E->boxes.assign(1, b);
+    } else {
+        E->boxes.assign(boxes, boxes + nsys);
+    }
+    E->graph_steps = o.graph_steps == 0 ? 100 : (o.graph_steps < 0 ? 0 : o.graph_steps);
+    auto bail = [&](int code, const std::string& msg) {
+        g_create_error = msg;
+        rdgpu_destroy(E);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(RDGPU_ERR_CUDA, "cudaStreamCreate failed");
+    if (cudaMalloc(&E->sys_d, nsys * sizeof(SysDev)) != cudaSuccess ||
+        cudaMalloc(&E->work_ctr, 3 * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&E->err, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&E->err_step, sizeof(long long)) != cudaSuccess ||
+        cudaMalloc(&E->step_d, sizeof(long long)) != cudaSuccess ||
+        cudaMalloc(&E->scratch_i, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&E->red_d, (RDGPU_MAX_TYPES + 1) * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&E->redc_d, (RDGPU_MAX_TYPES + 1) * sizeof(long long)) != cudaSuccess ||
+        cudaMallocHost(&E->pinned_err, sizeof(int)) != cudaSuccess ||
+        cudaMallocHost(&E->pinned_step, sizeof(long long)) != cudaSuccess)
+        return bail(RDGPU_ERR_NOMEM, "device allocation failed");
+    int rc = setup_systems(E, why);
+    if (rc) return bail(rc == -2 ? RDGPU_ERR_NOMEM : RDGPU_ERR_ARG, why);
+    int sms = 148, occ = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, E->device);
+    if (E->prec == RDGPU_PREC_F32C)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, step_kernel<float, kBlock>, kBlock, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, step_kernel<double, kBlock>, kBlock, 0);
+    E->grid = sms * std::max(occ, 1);
+    *out = E;
+    return RDGPU_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+int rdgpu_create(const rdgpu_system_desc* desc, const rdgpu_options* opt, rdgpu_handle* out)
+{
+    return create_impl(desc, 1, nullptr, opt, out);
+}
+
+int rdgpu_create_batch(const rdgpu_system_desc* desc, int32_t n_systems, const rdgpu_box* boxes,
+                       const rdgpu_options* opt, rdgpu_handle* out)
+{
+    return create_impl(desc, n_systems, boxes, opt, out);
+}
+
+int rdgpu_destroy(rdgpu_handle h)
+{
+    Engine* E = (Engine*)h;
+    if (!E) return RDGPU_ERR_ARG;
+    cudaSetDevice(E->device);
+    if (E->stream) cudaStreamSynchronize(E->stream);
+    free_state(E);
+    free_particles(E);
+    dfree(E->sys_d); dfree(E->items_d); dfree(E->tab_d); dfree(E->ext_d);
+    dfree(E->work_ctr); dfree(E->err); dfree(E->err_step); dfree(E->step_d); dfree(E->scratch_i);
+    dfree(E->red_d); dfree(E->redc_d); dfree(E->rdf_acc); dfree(E->rdf_tmp); dfree(E->rdf_e2);
+    if (E->pinned_err) cudaFreeHost(E->pinned_err);
+    if (E->pinned_step) cudaFreeHost(E->pinned_step);
+    if (E->stream) cudaStreamDestroy(E->stream);
+    delete E;
+    return RDGPU_OK;
+}
+
+const char* rdgpu_last_error(rdgpu_handle h)
+{
+    if (!h) return g_create_error.c_str();
+    return ((Engine*)h)->last_error.c_str();
+}
+
+#define DISPATCH(E, fn, ...) \
+    ((E)->prec == RDGPU_PREC_F32C ? fn<float>(__VA_ARGS__) : fn<double>(__VA_ARGS__))
+
+#define GUARD(E)                                                          \
+    if (!(E)) return RDGPU_ERR_ARG;                                       \
+    if (cudaSetDevice((E)->device) != cudaSuccess) return fail((E), RDGPU_ERR_CUDA, "cudaSetDevice failed")
+
+#define NEED_PARTICLES(E) \
+    if ((E)->part_off.empty()) return fail((E), RDGPU_ERR_STATE, "no particles set")
+
+int rdgpu_set_particles(rdgpu_handle h, const int64_t* offsets, int64_t n_total, const double* xyz,
+                        const int32_t* types)
+{
+    Engine* E = (Engine*)h;
+    GUARD(E);
+    if (n_total < 0 || (n_total > 0 && (!xyz || !types))) return fail(E, RDGPU_ERR_ARG, "invalid particle arrays");
+    return DISPATCH(E, set_particles_impl, E, (const long long*)offsets, (long long)n_total, xyz, (const int*)types);
+}
+
+int rdgpu_get_particles(rdgpu_handle h, double* xyz, int32_t* types)
+{
+    Engine* E = (Engine*)h;
+    GUARD(E);
+    NEED_PARTICLES(E);
+    return DISPATCH(E, get_particles_impl, E, xyz, (int*)types);
+}
+
+int rdgpu_num_particles(rdgpu_handle h, int64_t* n)
+{
+    Engine* E = (Engine*)h;
+    if (!E || !n) return RDGPU_ERR_ARG;
+    *n = E->npart_tot;
+    return RDGPU_OK;
+}
+
+int rdgpu_step(rdgpu_handle h, int64_t nsteps)
+{
+    Engine* E = (Engine*)h;
+    GUARD(E);
+    NEED_PARTICLES(E);
+    if (nsteps < 0) return fail(E, RDGPU_ERR_ARG, "nsteps < 0");
+    if (nsteps == 0 || E->npart_tot == 0) { E->step_h += nsteps; return prepare_step_state(E, E->step_h); }
+    return DISPATCH(E, do_steps, E, (long long)nsteps, (const double*)nullptr);
+}
+
+int rdgpu_step_with_noise(rdgpu_handle h, const double* noise)
+{
+    Engine* E = (Engine*)h;
+    GUARD(E);
+    NEED_PARTICLES(E);
+    if (!noise) return fail(E, RDGPU_ERR_ARG, "noise is null");
+    if (E->npart_tot == 0) return RDGPU_OK;
+    CK(cudaMemcpyAsync(E->vec_d, noise, E->npart_tot * 3 * sizeof(double), cudaMemcpyHostToDevice, E->stream));
+    return DISPATCH(E, do_steps, E, 1LL, (const double*)E->vec_d);
+}
+
+int rdgpu_set_seed(rdgpu_handle h, int32_t sys, uint64_t seed)
+{
+    Engine* E = (Engine*)h;
+    GUARD(E);
+    if (sys < 0 || sys >= E->nsys) return fail(E, RDGPU_ERR_ARG, "system index out of range");
+    E->sys_h[sys].seed = seed;
+    E->boxes[sys].seed = seed;
+    CK(cudaMemcpyAsync(E->sys_d + sys, &E->sys_h[sys], sizeof(SysDev), cudaMemcpyHostToDevice, E->stream));
+    CK(cudaStreamSynchronize(E->stream));
+    return RDGPU_OK;
+}
+
+int rdgpu_forces(rdgpu_handle h, double* forces, double* energy)
+{
+    Engine* E = (Engine*)h;
+    GUARD(E);
+    NEED_PARTICLES(E);
+    if (E->npart_tot == 0) { if (energy) *energy = 0.0; return RDGPU_OK; }
+    return DISPATCH(E, forces_impl, E, forces, energy);
+}
+
+int rdgpu_neighbor_digest(rdgpu_handle h, int32_t* counts, uint64_t* hashes)
+{
+    Engine* E = (Engine*)h;
+    GUARD(E);
+    NEED_PARTICLES(E);
+    if (!counts || !hashes) return fail(E, RDGPU_ERR_ARG, "null output");
+    if (E->npart_tot == 0) return RDGPU_OK;
+    return DISPATCH(E, digest_impl, E, (int*)counts, (unsigned long long*)hashes);
+}
+
+int rdgpu_debug_noise(rdgpu_handle h, int64_t step, double* noise)
+{
+    Engine* E = (Engine*)h;
+    GUARD(E);
+    NEED_PARTICLES(E);
+    if (!noise) return fail(E, RDGPU_ERR_ARG, "null output");
+    if (E->npart_tot == 0) return RDGPU_OK;
+    if (E->prec == RDGPU_PREC_F32C)
+        noise_kernel<float><<<grid_for(E->npart_tot), 256, 0, E->stream>>>(E->sys_d, E->nsys, E->npart_tot, step, E->vec_d);
+    else
+        noise_kernel<double><<<grid_for(E->npart_tot), 256, 0, E->stream>>>(E->sys_d, E->nsys, E->npart_tot, step, E->vec_d);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(noise, E->vec_d, E->npart_tot * 3 * sizeof(double), cudaMemcpyDeviceToHost, E->stream));
+    CK(cudaStreamSynchronize(E->stream));
+    return RDGPU_OK;
+}
+
+int rdgpu_rdf(rdgpu_handle h, int32_t nbins, double rmax, int32_t accumulate, uint64_t* counts, int64_t* frames)
+{
+    Engine* E = (Engine*)h;
+    GUARD(E);
+    NEED_PARTICLES(E);
+    if (nbins < 1 || nbins > 100000 || !(rmax > 0)) return fail(E, RDGPU_ERR_ARG, "invalid RDF bins/range");
+    return DISPATCH(E, rdf_impl, E, (int)nbins, rmax, (int)accumulate, (unsigned long long*)counts, (long long*)frames);
+}
+
+int rdgpu_rdf_normalized(rdgpu_handle h, double* g)
+{
+    Engine* E = (Engine*)h;
+    GUARD(E);
+    NEED_PARTICLES(E);
+    if (!E->rdf_acc || E->rdf_frames == 0) return fail(E, RDGPU_ERR_STATE, "no accumulated RDF frames");
+    if (E->nsys != 1) return fail(E, RDGPU_ERR_ARG, "normalised RDF is defined for a single system");
+    const int S = E->desc.n_types, H = S * S * E->rdf_nbins;
+    std::vector<long long> nper(S, 0);
+    for (int t : E->types_h) nper[t]++;
+    double vol = 1.0;
+    for (int a = 0; a < 3; ++a)
+        vol *= (E->prec == RDGPU_PREC_F32C) ? (double)E->sys_h[0].Lf[a] : E->sys_h[0].L[a];
+    long long* nper_d = nullptr;
+    double* g_d = nullptr;
+    CK(cudaMalloc(&nper_d, S * sizeof(long long)));
+    CK(cudaMalloc(&g_d, H * sizeof(double)));
+    CK(cudaMemcpyAsync(nper_d, nper.data(), S * sizeof(long long), cudaMemcpyHostToDevice, E->stream));
+    rdf_norm_kernel<<<(H + 255) / 256, 256, 0, E->stream>>>(E->rdf_acc, S, E->rdf_nbins, E->rdf_rmax / E->rdf_nbins,
+                                                            (double)E->rdf_frames, vol, nper_d, g_d);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(g, g_d, H * sizeof(double), cudaMemcpyDeviceToHost, E->stream));
+    CK(cudaStreamSynchronize(E->stream));
+    cudaFree(nper_d);
+    cudaFree(g_d);
+    return RDGPU_OK;
+}
+
+int rdgpu_metrics_get(rdgpu_handle h, rdgpu_metrics* m)
+{
+    Engine* E = (Engine*)h;
+    GUARD(E);
+    NEED_PARTICLES(E);
+    if (!m) return fail(E, RDGPU_ERR_ARG, "null output");
+    memset(m, 0, sizeof(*m));
+    m->step = E->step_h;
+    m->cell_cap = 1 << E->sys_h[0].cap_log2;
+    m->overflow_regrows = E->regrows;
+    if (E->npart_tot == 0) return RDGPU_OK;
+    int rc = rdgpu_forces(h, nullptr, &m->energy);
+    if (rc) return rc;
+    return DISPATCH(E, msd_impl, E, m);
+}
+
+void* rdgpu_stream(rdgpu_handle h)
+{
+    Engine* E = (Engine*)h;
+    return E ? (void*)E->stream : nullptr;
+}
+
+int64_t rdgpu_launch_count(rdgpu_handle h)
+{
+    Engine* E = (Engine*)h;
+    return E ? E->launches : 0;
+}
+
+}  // extern "C"

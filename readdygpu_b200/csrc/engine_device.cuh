@@ -1,0 +1,380 @@
+// engine_device.cuh -- device code of the B200 Brownian-dynamics engine.
+//
+// Data layout in HBM (per handle; all systems of a batch share the arrays):
+//   cells:  every system owns ncells = n0*n1*n2 cells of edge L/n (>= cutoff),
+//           cell id = (z*n1 + y)*n0 + x, placed at cell_base in the global cell
+//           arrays.  A cell owns 2^cap_log2 slots starting at
+//           slot_base + (cell << cap_log2).
+//   state:  FP32C: pos[slot] = float4(x, y, z, bits(type | images)),
+//                  cmp[slot] = float4(cx, cy, cz, bits(id)); true = pos - cmp.
+//           FP64:  Rec64{double x, y, z; int w (type | images); int id}.
+//           Coordinates are box-relative, in [0, L) on periodic axes.
+//   counts: cnt[3][cells] rotating: step t reads cnt[t%3], claims slots of
+//           the next layout in cnt[(t+1)%3] and clears cnt[(t+2)%3].
+//   Two state buffers alternate: step t reads buffer t&1, writes (t+1)&1.
+//
+// One BD step is ONE kernel (step_kernel): for every particle it sums the
+// pair forces over its 27-cell neighbourhood, adds the external forces, does
+// the Euler-Maruyama update with Philox noise, wraps, and writes the particle
+// into its new cell of the next buffer.  This replaces the reference's
+// orderOne / warpOrderTwo / update sequence with its linked-list relinking
+// (lib/ReaDDyGPU_Cpp/CudaKernels/CudaSimulation.cu:1034-1236, 1402-1782,
+// 1838-1919).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace rdgpu {
+
+constexpr int MAXT = 16;
+constexpr int MAX_TERMS = 4;
+constexpr unsigned FULL = 0xffffffffu;
+
+// error flags
+constexpr int EF_OVERFLOW = 1;
+constexpr int EF_NONFINITE = 2;
+constexpr int EF_JUMP = 4;
+
+// fixed-point scale of the FP32 force accumulator (2^32): order-independent,
+// hence deterministic, sums of FP32 pair forces.
+constexpr float FX_SCALE = 4294967296.0f;
+constexpr float FX_INV = 2.3283064365386963e-10f;
+
+struct SysDev {
+    int n[3];
+    int per[3];
+    int ncells;
+    int cap_log2;
+    long long cell_base;
+    long long slot_base;
+    long long part_base;
+    int npart;
+    int lanes_log2;
+    float Lf[3], halff[3], invcf[3];
+    double L[3], half[3], invc[3];
+    double lo[3];
+    unsigned long long seed;
+};
+
+template <class R> struct PairTerm {
+    int kind, sub;
+    R k, r0, l, d, q;
+};
+
+template <class R> struct ExtTerm {
+    int kind, sub;
+    R k;
+    R c[3], nrm[3];
+    R rad, h;
+    R blo[3], bhi[3];
+    int consider;
+    unsigned tmask;
+};
+
+template <class R> struct TypeTab {
+    int S;
+    int n_ext;
+    R a[MAXT];        // D dt / (kB T)
+    R b[MAXT];        // sqrt(2 D dt)
+    R prad[MAXT];     // default collision radius (external potentials)
+    R rc2[MAXT * MAXT];
+    int nterm[MAXT * MAXT];
+    PairTerm<R> term[MAXT * MAXT * MAX_TERMS];
+};
+
+struct alignas(32) Rec64 {
+    double x, y, z;
+    int w;
+    int id;
+};
+
+struct WorkItem {
+    int sys;
+    int c0, c1;
+    int cpl;          // cells per lane
+};
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw: "Parallel random numbers: as
+// easy as 1, 2, 3", SC'11).  Counter (index lo, index hi, step lo, step hi),
+// key = the system seed.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
+{
+    const unsigned M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+    const unsigned W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        unsigned hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
+        unsigned hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+        k.x += W0;
+        k.y += W1;
+    }
+    return c;
+}
+
+__device__ __forceinline__ uint4 bd_words(unsigned long long seed, long long step, long long index)
+{
+    uint4 c = make_uint4((unsigned)index, (unsigned)((unsigned long long)index >> 32),
+                         (unsigned)step, (unsigned)((unsigned long long)step >> 32));
+    return philox4x32_10(c, make_uint2((unsigned)seed, (unsigned)(seed >> 32)));
+}
+
+// Box-Muller on the uniforms (w + 1/2) 2^-32 of the four Philox words
+__device__ __forceinline__ void bd_normals(unsigned long long seed, long long step, long long index,
+                                           float out[3])
+{
+    uint4 w = bd_words(seed, step, index);
+    const float s = 2.3283064365386963e-10f;
+    float u0 = ((float)w.x + 0.5f) * s, u1 = ((float)w.y + 0.5f) * s;
+    float u2 = ((float)w.z + 0.5f) * s, u3 = ((float)w.w + 0.5f) * s;
+    float ra = sqrtf(-2.0f * logf(u0)), rb = sqrtf(-2.0f * logf(u2));
+    float sa, ca, sb, cb;
+    sincospif(2.0f * u1, &sa, &ca);
+    sincospif(2.0f * u3, &sb, &cb);
+    out[0] = ra * ca;
+    out[1] = ra * sa;
+    out[2] = rb * cb;
+}
+
+__device__ __forceinline__ void bd_normals(unsigned long long seed, long long step, long long index,
+                                           double out[3])
+{
+    uint4 w = bd_words(seed, step, index);
+    const double s = 2.3283064365386963e-10;
+    double u0 = ((double)w.x + 0.5) * s, u1 = ((double)w.y + 0.5) * s;
+    double u2 = ((double)w.z + 0.5) * s, u3 = ((double)w.w + 0.5) * s;
+    double ra = sqrt(-2.0 * log(u0)), rb = sqrt(-2.0 * log(u2));
+    double sa, ca, sb, cb;
+    sincospi(2.0 * u1, &sa, &ca);
+    sincospi(2.0 * u3, &sb, &cb);
+    out[0] = ra * ca;
+    out[1] = ra * sa;
+    out[2] = rb * cb;
+}
+
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+// ---------------------------------------------------------------------------
+// Non-contracted arithmetic: the neighbour predicate must round exactly like
+// the CPU oracle (no FMA), so dx, r^2 use explicit _rn intrinsics.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
+template <class R> struct Box;
+template <> struct Box<float> {
+    float L[3], half[3];
+    __device__ __forceinline__ void load(const SysDev& s)
+    {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) { L[a] = s.Lf[a]; half[a] = s.halff[a]; }
+    }
+};
+template <> struct Box<double> {
+    double L[3], half[3];
+    __device__ __forceinline__ void load(const SysDev& s)
+    {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) { L[a] = s.L[a]; half[a] = s.half[a]; }
+    }
+};
+
+// minimum image (CudaSimulation.cu:996-1002)
+template <class R>
+__device__ __forceinline__ R mimg(R dx, R L, R half, int per)
+{
+    if (per) {
+        if (dx > half) dx = sub_rn(dx, L);
+        else if (dx < -half) dx = add_rn(dx, L);
+    }
+    return dx;
+}
+
+// r^2 = (dx*dx + dy*dy) + dz*dz, rounded after every operation
+template <class R>
+__device__ __forceinline__ R dist2(R dx, R dy, R dz)
+{
+    return add_rn(add_rn(mul_rn(dx, dx), mul_rn(dy, dy)), mul_rn(dz, dz));
+}
+
+// pair term: the force on particle i is pre * (x_j - x_i); energy e.
+// P2_Harmonic.java:144-234, P2_WeakInteractionPiecewiseHarmonic.java:114-206.
+template <class R>
+__device__ __forceinline__ void pair_term(const PairTerm<R>& t, R r, R& pre, R& e)
+{
+    pre = R(0);
+    e = R(0);
+    if (t.kind == 1) {
+        R rr = (r == R(0)) ? R(1e-6) : r;
+        bool act = (t.sub == 3) || (t.sub == 2 && rr < t.r0) || (t.sub == 1 && rr > t.r0);
+        if (act) {
+            R dr = rr - t.r0;
+            pre = t.k * dr / rr;
+            e = R(0.5) * t.k * dr * dr;
+        }
+    } else {
+        const R r0 = t.r0, l = t.l, d = t.d, q = t.q;
+        if (r < r0) {
+            pre = (r > R(0)) ? t.k * (r - r0) / r : R(0);
+            e = t.k / R(2) * (r - r0) * (r - r0) - d;
+        } else if (r < r0 + R(0.5) * l) {
+            pre = d * q * (r - r0) / r;
+            e = R(0.5) * d * q * (r - r0) * (r - r0) - d;
+        } else if (r < r0 + l) {
+            pre = -d * q * (r - r0 - l) / r;
+            e = -R(0.5) * d * q * (r - r0 - l) * (r - r0 - l);
+        }
+    }
+}
+
+// external potential force (-grad V) and energy at box-relative x.
+// P1_Disk.java:112-320, P1_Cylinder.java:109-340, P1_Sphere.java:202-340,
+// P1_Cube.java:187-273.
+template <class R>
+__device__ __forceinline__ void ext_force(const ExtTerm<R>& p, R prad, const R x[3], R g[3], R& e)
+{
+    const R k = p.k;
+    if (p.kind == 1 || p.kind == 2) {
+        R s = (x[0] - p.c[0]) * p.nrm[0] + (x[1] - p.c[1]) * p.nrm[1] + (x[2] - p.c[2]) * p.nrm[2];
+        R pp[3] = {x[0] - p.nrm[0] * s, x[1] - p.nrm[1] * s, x[2] - p.nrm[2] * s};
+        R dpl = fabs(s);
+        R cp0 = pp[0] - p.c[0], cp1 = pp[1] - p.c[1], cp2 = pp[2] - p.c[2];
+        R din = sqrt(cp0 * cp0 + cp1 * cp1 + cp2 * cp2);
+        if (p.kind == 1) {
+            if (p.sub == 1) {
+                if (dpl > R(0)) {
+                    R pre = k;   // k (r - 0) / r
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) g[a] += pre * (pp[a] - x[a]);
+                    e += R(0.5) * k * dpl * dpl;
+                }
+                R r = din + prad;
+                if (r > p.rad) {
+                    R pre = k * (r - p.rad) / r;
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) g[a] += pre * (p.c[a] - pp[a]);
+                    e += R(0.5) * k * (r - p.rad) * (r - p.rad);
+                }
+            } else {
+                R r1 = din - prad;
+                if (dpl < prad && r1 < p.rad) {
+                    R pre = (dpl > R(0)) ? k * (dpl - prad) / dpl : R(0);
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) g[a] += pre * (pp[a] - x[a]);
+                    e += R(0.5) * k * (dpl - prad) * (dpl - prad);
+                }
+            }
+        } else {
+            if (p.sub == 1) {
+                R r = dpl + prad, r0 = R(0.5) * p.h;
+                if (r > r0) {
+                    R pre = k * (r - r0) / r;
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) g[a] += pre * (pp[a] - x[a]);
+                }
+                r = din + prad;
+                if (r > p.rad) {
+                    R pre = k * (r - p.rad) / r;
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) g[a] += pre * (p.c[a] - pp[a]);
+                }
+                if (dpl > p.h) e += R(0.5) * k * (dpl - p.h) * (dpl - p.h);
+                if (r > p.rad) e += R(0.5) * k * (r - p.rad) * (r - p.rad);
+            } else {
+                R r0 = prad + R(0.5) * p.h;
+                R r1 = din - prad;
+                if (r1 < p.rad) {
+                    R pre = (r1 != R(0)) ? k * (r1 - p.rad) / r1 : R(0);
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) g[a] += pre * (p.c[a] - pp[a]);
+                }
+                if (dpl < r0) {
+                    R pre = (dpl > R(0)) ? k * (dpl - r0) / dpl : R(0);
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) g[a] += pre * (pp[a] - x[a]);
+                }
+                R r0e = prad + p.h;
+                if (dpl < r0e) e += R(0.5) * k * (dpl - r0e) * (dpl - r0e);
+                if (r1 < p.rad) e += R(0.5) * k * (r1 - p.rad) * (r1 - p.rad);
+            }
+        }
+    } else if (p.kind == 3) {
+        R pr = p.consider ? prad : R(0);
+        R d0 = x[0] - p.c[0], d1 = x[1] - p.c[1], d2 = x[2] - p.c[2];
+        R d = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+        R r, r0;
+        bool act;
+        if (p.sub == 1) { r = d + pr; r0 = p.rad; act = r > r0; }
+        else if (p.sub == 2) { r = d; r0 = p.rad + pr; act = r < r0; }
+        else { r = d; r0 = p.rad; act = r != r0; }
+        if (act) {
+            R pre = (r != R(0)) ? k * (r - r0) / r : R(0);
+            g[0] += pre * (p.c[0] - x[0]);
+            g[1] += pre * (p.c[1] - x[1]);
+            g[2] += pre * (p.c[2] - x[2]);
+            e += R(0.5) * k * (r - r0) * (r - r0);
+        }
+    } else {
+        R pr = p.consider ? prad : R(0);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            R gi = R(0);
+            if (x[a] - pr >= p.blo[a] && x[a] + pr <= p.bhi[a]) {
+                gi = R(0);
+            } else if (x[a] - pr < p.blo[a]) {
+                R r = x[a] - pr;
+                gi = k * (r - p.blo[a]);
+                e += R(0.5) * k * (r - p.blo[a]) * (r - p.blo[a]);
+            } else {
+                R r = x[a] + pr;
+                gi = k * (r - p.bhi[a]);
+                e += R(0.5) * k * (r - p.bhi[a]) * (r - p.bhi[a]);
+            }
+            g[a] += (p.sub == 1) ? -gi : gi;
+        }
+    }
+}
+
+// neighbour offset d along an axis with n cells: valid and wrapped cell
+__device__ __forceinline__ bool axis_cell(int c, int d, int n, int per, int& out)
+{
+    int v = c + d;
+    if (!per) {
+        out = v;
+        return v >= 0 && v < n;
+    }
+    if (n >= 3) {
+        out = (v < 0) ? v + n : (v >= n ? v - n : v);
+        return true;
+    }
+    if (n == 2) {
+        out = v & 1;
+        return d != -1;   // -1 and +1 are the same cell
+    }
+    out = 0;
+    return d == 0;
+}
+
+__device__ __forceinline__ int warp_incl_scan(int v, int lane)
+{
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(FULL, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+}  // namespace rdgpu

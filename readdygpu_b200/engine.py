@@ -1,0 +1,167 @@
+"""Python handle over the C ABI (include/readdy_b200.h).
+
+Mirrors the operations of the reference's CudaSimulation host wrapper
+(lib/ReaDDyGPU_Cpp/CudaKernels/CudaSimulation.cuh:39-116): initialize ->
+Engine(...), copyPosToDevice/createNeighborList -> set_particles,
+simulate -> step, copyPosFromDevice -> get_particles, callRDFCalculation/
+copyRDFMatrix -> rdf.  Errors raise RdgpuError with the library's message
+(the reference returns 1 and prints, CudaSimulation.cu:138-455).
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _abi as A
+
+
+class RdgpuError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"rdgpu error {code}: {msg}")
+        self.code = code
+
+
+def _lib():
+    from . import lib
+    return lib
+
+
+def _p(a, ct):
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+class Engine:
+    """One handle: a single system, or a batch of systems sharing types and
+    potentials (boxes=[(lo, hi, periodic, seed), ...])."""
+
+    def __init__(self, system, precision="f64", device=0, seed=0, boxes=None, cell_cap=0,
+                 lanes_per_particle=0, cells_per_lane=0, graph_steps=0):
+        self.system = system
+        self._desc = system.to_desc()
+        opt = A.Options()
+        opt.precision = {"f64": A.PREC_F64, "f32c": A.PREC_F32C}[precision]
+        opt.device = device
+        opt.cell_cap = cell_cap
+        opt.lanes_per_particle = lanes_per_particle
+        opt.cells_per_lane = cells_per_lane
+        opt.graph_steps = graph_steps
+        opt.seed = seed
+        self.precision = precision
+        h = C.c_void_p()
+        L = _lib()
+        if boxes is None:
+            rc = L.rdgpu_create(C.byref(self._desc), C.byref(opt), C.byref(h))
+            self.n_systems = 1
+        else:
+            arr = (A.Box * len(boxes))()
+            for k, (lo, hi, per, sd) in enumerate(boxes):
+                for a in range(3):
+                    arr[k].lo[a], arr[k].hi[a], arr[k].periodic[a] = lo[a], hi[a], int(per[a])
+                arr[k].seed = sd
+            rc = L.rdgpu_create_batch(C.byref(self._desc), len(boxes), arr, C.byref(opt), C.byref(h))
+            self.n_systems = len(boxes)
+        if rc != 0:
+            raise RdgpuError(rc, L.rdgpu_last_error(None).decode())
+        self._h = h
+        self.n = 0
+
+    # -- plumbing --------------------------------------------------------
+    def _check(self, rc):
+        if rc != 0:
+            raise RdgpuError(rc, _lib().rdgpu_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib().rdgpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def stream(self):
+        return _lib().rdgpu_stream(self._h)
+
+    def launch_count(self):
+        return _lib().rdgpu_launch_count(self._h)
+
+    # -- state -----------------------------------------------------------
+    def set_particles(self, xyz, types, offsets=None):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        types = np.ascontiguousarray(types, dtype=np.int32).reshape(-1)
+        n = types.size
+        if offsets is not None:
+            off = np.ascontiguousarray(offsets, dtype=np.int64)
+            offp = _p(off, C.c_int64)
+        else:
+            offp = None
+        self._check(_lib().rdgpu_set_particles(self._h, offp, n, _p(xyz, C.c_double), _p(types, C.c_int32)))
+        self.n = n
+
+    def get_particles(self):
+        xyz = np.empty((self.n, 3))
+        types = np.empty(self.n, np.int32)
+        self._check(_lib().rdgpu_get_particles(self._h, _p(xyz, C.c_double), _p(types, C.c_int32)))
+        return xyz, types
+
+    # -- dynamics --------------------------------------------------------
+    def step(self, nsteps=1):
+        self._check(_lib().rdgpu_step(self._h, int(nsteps)))
+
+    def step_with_noise(self, noise):
+        noise = np.ascontiguousarray(noise, dtype=np.float64).reshape(-1)
+        assert noise.size == 3 * self.n
+        self._check(_lib().rdgpu_step_with_noise(self._h, _p(noise, C.c_double)))
+
+    def set_seed(self, seed, sys=0):
+        self._check(_lib().rdgpu_set_seed(self._h, sys, seed))
+
+    # -- observables -----------------------------------------------------
+    def forces(self):
+        F = np.empty((self.n, 3))
+        e = C.c_double()
+        self._check(_lib().rdgpu_forces(self._h, _p(F, C.c_double), C.byref(e)))
+        return F, e.value
+
+    def neighbor_digest(self):
+        cnt = np.empty(self.n, np.int32)
+        h = np.empty(self.n, np.uint64)
+        self._check(_lib().rdgpu_neighbor_digest(self._h, _p(cnt, C.c_int32), _p(h, C.c_uint64)))
+        return cnt, h
+
+    def debug_noise(self, step):
+        out = np.empty((self.n, 3))
+        self._check(_lib().rdgpu_debug_noise(self._h, int(step), _p(out, C.c_double)))
+        return out
+
+    def rdf(self, nbins, rmax, accumulate=True):
+        S = self.system.n_types
+        out = np.empty(S * S * nbins, np.uint64)
+        fr = C.c_int64()
+        self._check(_lib().rdgpu_rdf(self._h, nbins, rmax, int(accumulate), _p(out, C.c_uint64), C.byref(fr)))
+        return out.reshape(S, S, nbins), fr.value
+
+    def rdf_normalized(self, nbins):
+        S = self.system.n_types
+        g = np.empty(S * S * nbins)
+        self._check(_lib().rdgpu_rdf_normalized(self._h, _p(g, C.c_double)))
+        return g.reshape(S, S, nbins)
+
+    def metrics(self):
+        m = A.Metrics()
+        self._check(_lib().rdgpu_metrics_get(self._h, C.byref(m)))
+        S = self.system.n_types
+        return {"energy": m.energy, "msd": list(m.msd[:S]), "count": list(m.count[:S]),
+                "step": m.step, "cell_cap": m.cell_cap, "overflow_regrows": m.overflow_regrows}
