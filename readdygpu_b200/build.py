@@ -46,8 +46,9 @@ def build_jni(force=False):
     if not all(os.path.exists(s) for s in srcs):
         return None
     out = os.path.join(HERE, "libCReaDDyGPU.so")
-    deps = srcs + [os.path.join(CSRC, f) for f in ("jni_min.h", "xml_input.h")] + [
-        os.path.join(ROOT, "include", "readdy_b200.h"), os.path.join(ROOT, "include", "readdy_b200_jni.h"),
+    deps = srcs + [os.path.join(CSRC, "xml_input.h")] + [
+        os.path.join(ROOT, "include", h) for h in ("readdy_b200.h", "readdy_b200_jni.h",
+                                                    "readdy_b200_jni_types.h", "readdy_b200_inputs.h")] + [
         os.path.join(HERE, "libreaddy_b200.so")]
     if force or _stale(out, [d for d in deps if os.path.exists(d)]):
         _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall"] + srcs +
