@@ -48,6 +48,9 @@ def parse():
     p.add_argument("--precision", default="f32c", choices=["f32c", "f64"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--kernel", default="brick", choices=["brick", "warp"])
+    p.add_argument("--lanes", type=int, default=0, help="lanes per particle (0: engine default)")
+    p.add_argument("--brick", type=int, default=0, help="brick edge in cells (0: engine default)")
     return p.parse_args()
 
 
@@ -199,7 +202,9 @@ def run_ours(args):
     if w.boxes is not None:
         # each rank owns its own replicate ensemble: shift the seeds
         kw["boxes"] = [(lo, hi, per, sd + 7919 * rank) for (lo, hi, per, sd) in w.boxes]
-    eng = R.Engine(w.system, precision=args.precision, device=local, seed=11 + rank, **kw)
+    eng = R.Engine(w.system, precision=args.precision, device=local, seed=11 + rank,
+                   kernel_variant=0 if args.kernel == "brick" else 1, lanes_per_particle=args.lanes,
+                   cells_per_lane=args.brick, **kw)
     eng.set_particles(w.xyz, w.types, offsets=w.offsets)
     stream = torch.cuda.ExternalStream(eng.stream, device=local)
     eng.step(args.warmup)
@@ -277,7 +282,8 @@ def run_ours(args):
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_kind": peak_kind,
                              "traffic": (tpp * w.n if tpp else None),
-                             "kernel": "step_kernel", "alg_bytes_per_particle_step": ALG_BYTES[args.precision]},
+                             "kernel": "brick_step_kernel" if args.kernel == "brick" else "step_kernel",
+                             "alg_bytes_per_particle_step": ALG_BYTES[args.precision]},
                 "e2e": e2e, "cpu_baseline": cb, "gpu_launches": launches, "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     eng.close()

@@ -129,10 +129,11 @@ typedef struct {
     int32_t  device;              /* CUDA device ordinal                               */
     int32_t  cell_cap;            /* slots per cell, power of two; 0 = automatic       */
     int32_t  lanes_per_particle;  /* 1,2,4,8; 0 = automatic (autotuner table)          */
-    int32_t  cells_per_lane;      /* cells summed by one lane in a work item; 0 = auto */
+    int32_t  cells_per_lane;      /* warp-list kernel: cells per lane; brick kernel:
+                                     brick edge in cells; 0 = automatic                */
     int32_t  block_size;          /* threads per block of the step kernel; 0 = auto    */
     int32_t  graph_steps;         /* steps captured per CUDA graph; 0 = 100, <0 = off  */
-    int32_t  reserved;
+    int32_t  kernel_variant;      /* 0: brick-staged step kernel, 1: warp-list kernel  */
     uint64_t seed;                /* Philox seed of a single-system handle             */
 } rdgpu_options;
 

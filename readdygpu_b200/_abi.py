@@ -74,7 +74,7 @@ class Options(C.Structure):
     _fields_ = [("precision", C.c_int32), ("device", C.c_int32), ("cell_cap", C.c_int32),
                 ("lanes_per_particle", C.c_int32), ("cells_per_lane", C.c_int32),
                 ("block_size", C.c_int32), ("graph_steps", C.c_int32),
-                ("reserved", C.c_int32), ("seed", C.c_uint64)]
+                ("kernel_variant", C.c_int32), ("seed", C.c_uint64)]
 
 
 class Metrics(C.Structure):

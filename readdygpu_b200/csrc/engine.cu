@@ -21,7 +21,8 @@ namespace {
 
 thread_local std::string g_create_error;
 
-constexpr int kBlock = 256;
+constexpr int kBlock = 256;        // warp-list kernel
+constexpr int kBrickBlock = 128;   // brick-staged kernel
 
 }  // namespace
 
@@ -38,6 +39,9 @@ struct rdgpu_engine {
     SysDev* sys_d = nullptr;
     std::vector<WorkItem> items_h;
     WorkItem* items_d = nullptr;
+    std::vector<BrickItem> bricks_h;
+    BrickItem* bricks_d = nullptr;
+    int brick_grid = 0;
     void* tab_d = nullptr;
     void* ext_d = nullptr;
     int n_ext = 0;
@@ -248,7 +252,8 @@ void free_particles(Engine* E)
     dfree(E->ityp_d); dfree(E->u64_d);
 }
 
-size_t rec_bytes(int prec) { return prec == RDGPU_PREC_F32C ? 16 : 32; }
+// bytes of one slot record (FP32C: pos + compensation; FP64: Rec64)
+size_t rec_bytes(int) { return 32; }
 
 // lay out cells/slots of all systems for the current caps and allocate
 int alloc_state(Engine* E)
@@ -267,7 +272,6 @@ int alloc_state(Engine* E)
     const size_t rb = rec_bytes(E->prec);
     for (int i = 0; i < 2; ++i) {
         CK(cudaMalloc(&E->bufA[i], std::max<long long>(sb, 1) * rb));
-        if (E->prec == RDGPU_PREC_F32C) CK(cudaMalloc(&E->bufB[i], std::max<long long>(sb, 1) * 16));
     }
     for (int i = 0; i < 3; ++i) {
         CK(cudaMalloc(&E->cnt[i], std::max<long long>(cb, 1) * sizeof(int)));
@@ -307,6 +311,49 @@ int build_items(Engine* E)
     return RDGPU_OK;
 }
 
+// bricks: per system a tiling of the cell grid into ex*ey*ez bricks whose
+// one-cell halo fits the kernel's shared-memory stage
+int build_bricks(Engine* E)
+{
+    E->bricks_h.clear();
+    for (int s = 0; s < E->nsys; ++s) {
+        const SysDev& d = E->sys_h[s];
+        const double occ = d.ncells > 0 ? std::max(1e-3, (double)d.npart / d.ncells) : 1.0;
+        int e = E->opt.cells_per_lane;
+        if (e <= 0) {
+            // about 160 particles per brick, halo (e+2)^3 <= 512 cells
+            e = (int)std::lround(std::cbrt(160.0 / occ));
+        }
+        e = std::min(std::max(e, 1), 6);
+        int ext[3];
+        for (int a = 0; a < 3; ++a) ext[a] = std::min(e, d.n[a]);
+        // keep the expected staged particles well inside the stage
+        while ((ext[0] + 2) * (ext[1] + 2) * (ext[2] + 2) * occ > MAXP / 2 &&
+               (ext[0] > 1 || ext[1] > 1 || ext[2] > 1)) {
+            int a = (ext[0] >= ext[1] && ext[0] >= ext[2]) ? 0 : (ext[1] >= ext[2] ? 1 : 2);
+            ext[a]--;
+        }
+        const int lg = d.lanes_log2;
+        for (int z0 = 0; z0 < d.n[2]; z0 += ext[2])
+            for (int y0 = 0; y0 < d.n[1]; y0 += ext[1])
+                for (int x0 = 0; x0 < d.n[0]; x0 += ext[0]) {
+                    BrickItem b;
+                    const int ex = std::min(ext[0], d.n[0] - x0), ey = std::min(ext[1], d.n[1] - y0),
+                              ez = std::min(ext[2], d.n[2] - z0);
+                    b.sys = s;
+                    b.xy = x0 | (y0 << 16);
+                    b.z = z0;
+                    b.ext = ex | (ey << 8) | (ez << 16) | (lg << 24);
+                    E->bricks_h.push_back(b);
+                }
+    }
+    dfree(E->bricks_d);
+    CK(cudaMalloc(&E->bricks_d, std::max<size_t>(E->bricks_h.size(), 1) * sizeof(BrickItem)));
+    CK(cudaMemcpyAsync(E->bricks_d, E->bricks_h.data(), E->bricks_h.size() * sizeof(BrickItem),
+                       cudaMemcpyHostToDevice, E->stream));
+    return RDGPU_OK;
+}
+
 template <class R> StepArgs<R> make_args(Engine* E)
 {
     StepArgs<R> a;
@@ -319,8 +366,7 @@ template <class R> StepArgs<R> make_args(Engine* E)
     a.ext = (const ExtTerm<R>*)E->ext_d;
     for (int i = 0; i < 2; ++i) {
         if constexpr (sizeof(R) == 4) {
-            a.buf[i].pos = (float4*)E->bufA[i];
-            a.buf[i].cmp = (float4*)E->bufB[i];
+            a.buf[i].rec = (float4*)E->bufA[i];
         } else {
             a.buf[i].st = (Rec64*)E->bufA[i];
         }
@@ -338,7 +384,7 @@ template <class R> StepArgs<R> make_args(Engine* E)
 template <class R> StateBuf<R> sbuf(Engine* E, int i)
 {
     StateBuf<R> b;
-    if constexpr (sizeof(R) == 4) { b.pos = (float4*)E->bufA[i]; b.cmp = (float4*)E->bufB[i]; }
+    if constexpr (sizeof(R) == 4) b.rec = (float4*)E->bufA[i];
     else b.st = (Rec64*)E->bufA[i];
     return b;
 }
@@ -426,7 +472,11 @@ template <class R> int launch_steps(Engine* E, int n, const double* noise_d)
     a.noise = noise_d;
     for (int k = 0; k < n; ++k) {
         a.step_off = k;
-        step_kernel<R, kBlock><<<E->grid, kBlock, 0, E->stream>>>(a);
+        if (E->opt.kernel_variant == 1)
+            step_kernel<R, kBlock><<<E->grid, kBlock, 0, E->stream>>>(a);
+        else
+            brick_step_kernel<R, kBrickBlock><<<E->brick_grid, kBrickBlock, 0, E->stream>>>(
+                a, E->bricks_d, (int)E->bricks_h.size());
         ++E->launches;
     }
     advance_kernel<<<1, 32, 0, E->stream>>>(E->step_d, E->err, n);
@@ -634,7 +684,7 @@ template <class R> int set_particles_impl(Engine* E, const long long* offsets, l
     E->types_h.assign(types, types + ntot);
     free_particles(E);
     const long long N = std::max<long long>(ntot, 1);
-    CK(cudaMalloc(&E->denseA, N * rec_bytes(E->prec)));
+    CK(cudaMalloc(&E->denseA, N * (E->prec == RDGPU_PREC_F32C ? 16 : 32)));
     if (E->prec == RDGPU_PREC_F32C) CK(cudaMalloc(&E->denseB, N * 16));
     CK(cudaMalloc(&E->x0_d, N * 3 * sizeof(double)));
     CK(cudaMalloc(&E->vec_d, N * 3 * sizeof(double)));
@@ -700,6 +750,8 @@ template <class R> int set_particles_impl(Engine* E, const long long* offsets, l
         E->sys_h[s].lanes_log2 = ceil_log2(std::min(std::max(L, 1), 8));
     }
     CK(cudaMemcpyAsync(E->sys_d, E->sys_h.data(), E->nsys * sizeof(SysDev), cudaMemcpyHostToDevice, E->stream));
+    rc = build_bricks(E);
+    if (rc) return rc;
     dfree(E->rdf_acc);
     E->rdf_frames = 0;
     E->rdf_nbins = 0;
@@ -936,6 +988,12 @@ int create_impl(const rdgpu_system_desc* desc, int nsys, const rdgpu_box* boxes,
     else
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, step_kernel<double, kBlock>, kBlock, 0);
     E->grid = sms * std::max(occ, 1);
+    int bocc = 1;
+    if (E->prec == RDGPU_PREC_F32C)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bocc, brick_step_kernel<float, kBrickBlock>, kBrickBlock, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bocc, brick_step_kernel<double, kBrickBlock>, kBrickBlock, 0);
+    E->brick_grid = sms * std::max(bocc, 1);
     *out = E;
     return RDGPU_OK;
 }
@@ -966,7 +1024,7 @@ int rdgpu_destroy(rdgpu_handle h)
     if (E->stream) cudaStreamSynchronize(E->stream);
     free_state(E);
     free_particles(E);
-    dfree(E->sys_d); dfree(E->items_d); dfree(E->tab_d); dfree(E->ext_d);
+    dfree(E->sys_d); dfree(E->items_d); dfree(E->bricks_d); dfree(E->tab_d); dfree(E->ext_d);
     dfree(E->work_ctr); dfree(E->err); dfree(E->err_step); dfree(E->step_d); dfree(E->scratch_i);
     dfree(E->red_d); dfree(E->redc_d); dfree(E->rdf_acc); dfree(E->rdf_tmp); dfree(E->rdf_e2);
     if (E->pinned_err) cudaFreeHost(E->pinned_err);

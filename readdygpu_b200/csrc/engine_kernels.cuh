@@ -12,16 +12,17 @@ constexpr int LIST_CAP = 256;   // per-warp particle list window
 // ---------------------------------------------------------------------------
 template <class R> struct StateBuf;
 
+// FP32C slot record: rec[2s] = (x, y, z, bits(type|images)),
+// rec[2s+1] = (cx, cy, cz, bits(id)) -- one 32-byte sector per particle
 template <> struct StateBuf<float> {
-    float4* pos;
-    float4* cmp;
+    float4* rec;
     __device__ __forceinline__ void load_xyzw(long long s, float x[3], int& w) const
     {
-        float4 p = __ldg(pos + s);
+        float4 p = __ldg(rec + 2 * s);
         x[0] = p.x; x[1] = p.y; x[2] = p.z;
         w = __float_as_int(p.w);
     }
-    __device__ __forceinline__ int load_id(long long s) const { return __float_as_int(__ldg(&cmp[s].w)); }
+    __device__ __forceinline__ int load_id(long long s) const { return __float_as_int(__ldg(&rec[2 * s + 1].w)); }
 };
 
 template <> struct StateBuf<double> {
@@ -103,7 +104,36 @@ template <> struct Acc<double> {
     __device__ __forceinline__ void force(double F[3]) const { F[0] = fx; F[1] = fy; F[2] = fz; }
 };
 
-// MODE 0: forces; 1: forces + energy; 2: neighbour digest
+// One candidate pair (i, j): minimum image, the bit-exact neighbour predicate
+// r^2 < rc(ti,tj)^2, then the pair potentials of (ti, tj).
+// MODE 0: forces; 1: forces + energy; 2: neighbour digest (count, hash of id)
+template <class R, int MODE>
+__device__ __forceinline__ void pair_accum(const R xi[3], int ti, const R xj[3], int wj, const Box<R>& bx,
+                                           const int per[3], const TypeTab<R>* __restrict__ tab, Acc<R>& acc,
+                                           int& ncount, unsigned long long& hash, int idj)
+{
+    R dx = mimg(sub_rn(xi[0], xj[0]), bx.L[0], bx.half[0], per[0]);
+    R dy = mimg(sub_rn(xi[1], xj[1]), bx.L[1], bx.half[1], per[1]);
+    R dz = mimg(sub_rn(xi[2], xj[2]), bx.L[2], bx.half[2], per[2]);
+    R r2 = dist2(dx, dy, dz);
+    const int pidx = ti * MAXT + (wj & 0xff);
+    if (r2 < tab->rc2[pidx]) {
+        if (MODE == 2) {
+            ncount++;
+            hash += splitmix64((unsigned long long)idj);
+            return;
+        }
+        R r = sqrt(r2);
+        const int nt = tab->nterm[pidx];
+        for (int m = 0; m < nt; ++m) {
+            R pre, e;
+            pair_term(tab->term[pidx * MAX_TERMS + m], r, pre, e);
+            acc.add(pre, dx, dy, dz);
+            if (MODE == 1) acc.e += R(0.5) * e;
+        }
+    }
+}
+
 template <class R, int MODE>
 __device__ __forceinline__ void cell_pairs(const StateBuf<R>& b, long long sbase, int cnt,
                                            long long self, const R xi[3], int ti, const Box<R>& bx,
@@ -116,26 +146,7 @@ __device__ __forceinline__ void cell_pairs(const StateBuf<R>& b, long long sbase
         R xj[3];
         int wj;
         b.load_xyzw(s, xj, wj);
-        R dx = mimg(sub_rn(xi[0], xj[0]), bx.L[0], bx.half[0], per[0]);
-        R dy = mimg(sub_rn(xi[1], xj[1]), bx.L[1], bx.half[1], per[1]);
-        R dz = mimg(sub_rn(xi[2], xj[2]), bx.L[2], bx.half[2], per[2]);
-        R r2 = dist2(dx, dy, dz);
-        const int pidx = ti * MAXT + (wj & 0xff);
-        if (r2 < tab->rc2[pidx]) {
-            if (MODE == 2) {
-                ncount++;
-                hash += splitmix64((unsigned long long)b.load_id(s));
-                continue;
-            }
-            R r = sqrt(r2);
-            const int nt = tab->nterm[pidx];
-            for (int m = 0; m < nt; ++m) {
-                R pre, e;
-                pair_term(tab->term[pidx * MAX_TERMS + m], r, pre, e);
-                acc.add(pre, dx, dy, dz);
-                if (MODE == 1) acc.e += R(0.5) * e;
-            }
-        }
+        pair_accum<R, MODE>(xi, ti, xj, wj, bx, per, tab, acc, ncount, hash, MODE == 2 ? b.load_id(s) : 0);
     }
 }
 
@@ -247,6 +258,59 @@ __device__ __forceinline__ int cell_index(const SysDev& s, const R x[3])
 // one system), compact the particles of the run into a shared-memory list,
 // then groups of L lanes evaluate one particle each.
 // ---------------------------------------------------------------------------
+// external forces, Euler-Maruyama update, wrap, claim a slot of the new cell
+// in the next layout and write the particle there
+template <class R>
+__device__ __forceinline__ void finish_particle(const StepArgs<R>& a, const SysDev& s, int si, long long self,
+                                                R xi[3], int wi, R F[3], long long t, const StateBuf<R>& cur,
+                                                const StateBuf<R>& nxt, int* cnt_nxt)
+{
+    const int ti = wi & 0xff;
+    if (a.n_ext > 0) {
+        const ExtTerm<R>* ep = a.ext + (long long)si * a.n_ext;
+        R ee = R(0);
+        for (int e = 0; e < a.n_ext; ++e) {
+            if ((ep[e].tmask >> ti) & 1u) ext_force(ep[e], a.tab->prad[ti], xi, F, ee);
+        }
+    }
+    int id;
+    R c[3] = {R(0), R(0), R(0)};
+    if constexpr (sizeof(R) == 4) {
+        float4 q = __ldg(cur.rec + 2 * self + 1);
+        c[0] = q.x; c[1] = q.y; c[2] = q.z;
+        id = __float_as_int(q.w);
+    } else {
+        id = cur.st[self].id;
+    }
+    R xn[3];
+    if (a.noise) {
+        const double* nz = a.noise + 3 * (s.part_base + id);
+        xn[0] = (R)nz[0]; xn[1] = (R)nz[1]; xn[2] = (R)nz[2];
+    } else {
+        bd_normals(s.seed, t, (long long)id, xn);
+    }
+    int ef = em_update(xi, c, wi, F, xn, a.tab->a[ti], a.tab->b[ti], s);
+    const int ncell = cell_index(s, xi);
+    const int slot = atomicAdd(cnt_nxt + s.cell_base + ncell, 1);
+    if (slot >= (1 << s.cap_log2)) {
+        ef |= EF_OVERFLOW;
+    } else {
+        const long long dst = s.slot_base + ((long long)ncell << s.cap_log2) + slot;
+        if constexpr (sizeof(R) == 4) {
+            nxt.rec[2 * dst] = make_float4(xi[0], xi[1], xi[2], __int_as_float(wi));
+            nxt.rec[2 * dst + 1] = make_float4(c[0], c[1], c[2], __int_as_float(id));
+        } else {
+            Rec64 r;
+            r.x = xi[0]; r.y = xi[1]; r.z = xi[2]; r.w = wi; r.id = id;
+            nxt.st[dst] = r;
+        }
+    }
+    if (ef) {
+        atomicOr(a.err, ef);
+        atomicMin((unsigned long long*)a.err_step, (unsigned long long)t);
+    }
+}
+
 template <class R>
 __device__ __forceinline__ void step_particle(const StepArgs<R>& a, const SysDev& s, int si, int lslot,
                                               bool active, int sub, int L, long long t,
@@ -272,52 +336,9 @@ __device__ __forceinline__ void step_particle(const StepArgs<R>& a, const SysDev
         neighbourhood<R, 0>(cur, cnt_cur, s, cx, cy, cz, self, xi, ti, a.tab, sub, L, acc, nc, hh);
     acc.reduce_xor(L);
     if (!active || sub != 0) return;
-
     R F[3];
     acc.force(F);
-    if (a.n_ext > 0) {
-        const ExtTerm<R>* ep = a.ext + (long long)si * a.n_ext;
-        R ee = R(0);
-        for (int e = 0; e < a.n_ext; ++e) {
-            if ((ep[e].tmask >> ti) & 1u) ext_force(ep[e], a.tab->prad[ti], xi, F, ee);
-        }
-    }
-    int id;
-    R c[3] = {R(0), R(0), R(0)};
-    if constexpr (sizeof(R) == 4) {
-        float4 q = cur.cmp[self];
-        c[0] = q.x; c[1] = q.y; c[2] = q.z;
-        id = __float_as_int(q.w);
-    } else {
-        id = cur.st[self].id;
-    }
-    R xn[3];
-    if (a.noise) {
-        const double* nz = a.noise + 3 * (s.part_base + id);
-        xn[0] = (R)nz[0]; xn[1] = (R)nz[1]; xn[2] = (R)nz[2];
-    } else {
-        bd_normals(s.seed, t, (long long)id, xn);
-    }
-    int ef = em_update(xi, c, wi, F, xn, a.tab->a[ti], a.tab->b[ti], s);
-    const int ncell = cell_index(s, xi);
-    const int slot = atomicAdd(cnt_nxt + s.cell_base + ncell, 1);
-    if (slot >= (1 << s.cap_log2)) {
-        ef |= EF_OVERFLOW;
-    } else {
-        const long long dst = s.slot_base + ((long long)ncell << s.cap_log2) + slot;
-        if constexpr (sizeof(R) == 4) {
-            nxt.pos[dst] = make_float4(xi[0], xi[1], xi[2], __int_as_float(wi));
-            nxt.cmp[dst] = make_float4(c[0], c[1], c[2], __int_as_float(id));
-        } else {
-            Rec64 r;
-            r.x = xi[0]; r.y = xi[1]; r.z = xi[2]; r.w = wi; r.id = id;
-            nxt.st[dst] = r;
-        }
-    }
-    if (ef) {
-        atomicOr(a.err, ef);
-        atomicMin((unsigned long long*)a.err_step, (unsigned long long)t);
-    }
+    finish_particle<R>(a, s, si, self, xi, wi, F, t, cur, nxt, cnt_nxt);
 }
 
 template <class R, int BLOCK>
@@ -389,6 +410,215 @@ __global__ void __launch_bounds__(BLOCK) step_kernel(StepArgs<R> a)
     }
 }
 
+// ---------------------------------------------------------------------------
+// Brick-staged step kernel: a block takes a brick of ex*ey*ez cells of one
+// system, stages the positions of the brick and its one-cell halo into shared
+// memory (coalesced loads, all in flight together), then groups of L lanes
+// evaluate one particle each from shared memory and reduce with shuffles.
+// Bricks are strided statically over a persistent grid.
+// ---------------------------------------------------------------------------
+constexpr int MAXH = 512;     // halo cells per brick
+constexpr int MAXP = 1024;    // staged particles per brick
+
+struct BrickItem {
+    int sys;
+    int xy;       // x0 | y0 << 16
+    int z;        // z0
+    int ext;      // ex | ey << 8 | ez << 16 | lanes_log2 << 24
+};
+
+template <class R> struct SPos;
+template <> struct alignas(16) SPos<float> { float x, y, z; int w; };
+template <> struct alignas(16) SPos<double> { double x, y, z; int w, pad; };
+
+template <int BLOCK>
+__device__ __forceinline__ int block_excl_scan(const int* in, int* out, int n, int* s_warp)
+{
+    // out[0..n]: exclusive prefix of in[0..n), out[n] = total
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int per = (n + BLOCK - 1) / BLOCK;
+    const int b0 = tid * per;
+    int sum = 0;
+    for (int k = 0; k < per; ++k)
+        if (b0 + k < n) sum += in[b0 + k];
+    int incl = warp_incl_scan(sum, lane);
+    if (lane == 31) s_warp[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+        int v = lane < BLOCK / 32 ? s_warp[lane] : 0;
+        int vi = warp_incl_scan(v, lane);
+        if (lane < BLOCK / 32) s_warp[lane] = vi - v;
+    }
+    __syncthreads();
+    int run = s_warp[wid] + incl - sum;
+    for (int k = 0; k < per; ++k) {
+        if (b0 + k < n) {
+            out[b0 + k] = run;
+            run += in[b0 + k];
+        }
+    }
+    __syncthreads();
+    if (tid == BLOCK - 1) out[n] = run;
+    __syncthreads();
+    return out[n];
+}
+
+__device__ __forceinline__ bool halo_axis(int v, int n, int per, int& out)
+{
+    if (v >= 0 && v < n) { out = v; return true; }
+    if (!per) return false;
+    v %= n;
+    if (v < 0) v += n;
+    out = v;
+    return true;
+}
+
+// offsets valid on a periodic axis with fewer than 3 cells (each neighbour
+// cell once)
+__device__ __forceinline__ bool small_axis_ok(int d, int n, int per)
+{
+    if (!per || n >= 3) return true;
+    if (n == 2) return d != -1;
+    return d == 0;
+}
+
+template <class R, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) brick_step_kernel(StepArgs<R> a, const BrickItem* __restrict__ bricks,
+                                                           int nbricks)
+{
+    __shared__ int s_cnt[MAXH];
+    __shared__ int s_off[MAXH + 1];
+    __shared__ int s_gc[MAXH];
+    __shared__ int s_icnt[MAXH];
+    __shared__ int s_ioff[MAXH + 1];
+    __shared__ short s_ih[MAXH];
+    __shared__ int s_warp[BLOCK / 32];
+    __shared__ SPos<R> s_p[MAXP];
+
+    if (*((volatile int*)a.err)) return;   // an earlier step failed: keep its input intact
+    const int tid = threadIdx.x;
+    const long long t = (a.step_ptr ? *a.step_ptr : 0LL) + a.step_off;
+    const int b3 = (int)(t % 3);
+    const int* __restrict__ cnt_cur = a.cnt[b3];
+    int* cnt_nxt = a.cnt[(b3 + 1) % 3];
+    int* cnt_free = a.cnt[(b3 + 2) % 3];
+    const StateBuf<R> cur = a.buf[t & 1], nxt = a.buf[(t + 1) & 1];
+
+    for (int bi = blockIdx.x; bi < nbricks; bi += gridDim.x) {
+        const BrickItem it = bricks[bi];
+        const SysDev& s = a.sys[it.sys];
+        const int x0 = it.xy & 0xffff, y0 = it.xy >> 16, z0 = it.z;
+        const int ex = it.ext & 0xff, ey = (it.ext >> 8) & 0xff, ez = (it.ext >> 16) & 0xff;
+        const int lg = (it.ext >> 24) & 0x7;
+        const int hx = ex + 2, hy = ey + 2, hz = ez + 2;
+        const int H = hx * hy * hz, NI = ex * ey * ez;
+        const int cap_log2 = s.cap_log2, cap = 1 << cap_log2;
+        const int n0 = s.n[0], n1 = s.n[1], n2 = s.n[2];
+
+        // 1. halo cell counts; clear the brick's cells in the free count array
+        for (int h = tid; h < H; h += BLOCK) {
+            const int ix = h % hx, iy = (h / hx) % hy, iz = h / (hx * hy);
+            int gx, gy, gz;
+            const bool v = halo_axis(x0 - 1 + ix, n0, s.per[0], gx) && halo_axis(y0 - 1 + iy, n1, s.per[1], gy) &&
+                           halo_axis(z0 - 1 + iz, n2, s.per[2], gz);
+            const int gc = v ? (gz * n1 + gy) * n0 + gx : -1;
+            s_gc[h] = gc;
+            s_cnt[h] = v ? min(cnt_cur[s.cell_base + gc], cap) : 0;
+        }
+        for (int k = tid; k < NI; k += BLOCK) {
+            const int ix = 1 + k % ex, iy = 1 + (k / ex) % ey, iz = 1 + k / (ex * ey);
+            const int h = (iz * hy + iy) * hx + ix;
+            s_ih[k] = (short)h;
+            cnt_free[s.cell_base + ((z0 + iz - 1) * n1 + (y0 + iy - 1)) * n0 + (x0 + ix - 1)] = 0;
+        }
+        __syncthreads();
+        for (int k = tid; k < NI; k += BLOCK) s_icnt[k] = s_cnt[s_ih[k]];
+        const int T = block_excl_scan<BLOCK>(s_cnt, s_off, H, s_warp);
+        const int TI = block_excl_scan<BLOCK>(s_icnt, s_ioff, NI, s_warp);
+        const bool staged = T <= MAXP;
+
+        // 2. stage positions of the brick + halo
+        if (staged) {
+            for (int h = tid; h < H; h += BLOCK) {
+                const int c = s_cnt[h];
+                if (c == 0) continue;
+                const long long g = s.slot_base + ((long long)s_gc[h] << cap_log2);
+                const int o = s_off[h];
+                for (int q = 0; q < c; ++q) {
+                    R xq[3];
+                    int wq;
+                    cur.load_xyzw(g + q, xq, wq);
+                    SPos<R> sp;
+                    sp.x = xq[0]; sp.y = xq[1]; sp.z = xq[2]; sp.w = wq;
+                    s_p[o + q] = sp;
+                }
+            }
+        }
+        __syncthreads();
+
+        // 3. groups of L lanes, one particle each
+        const int L = 1 << lg, G = BLOCK >> lg, g = tid >> lg, sub = tid & (L - 1);
+        Box<R> bx;
+        bx.load(s);
+        const int per[3] = {s.per[0], s.per[1], s.per[2]};
+        for (int base = 0; base < TI; base += G) {
+            const int p = base + g;
+            const bool active = p < TI;
+            Acc<R> acc;
+            acc.zero();
+            int nc = 0;
+            unsigned long long hh = 0;
+            R xi[3] = {R(0), R(0), R(0)};
+            int wi = 0, h = 0, q = 0, si = 0;
+            if (active) {
+                int lo = 0, hi = NI - 1;           // inner cell of particle p
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (s_ioff[mid] <= p) lo = mid; else hi = mid - 1;
+                }
+                h = s_ih[lo];
+                q = p - s_ioff[lo];
+                si = s_off[h] + q;
+            }
+            const int ix = h % hx, iy = (h / hx) % hy, iz = h / (hx * hy);
+            const long long self = s.slot_base + ((long long)(active ? s_gc[h] : 0) << cap_log2) + q;
+            if (active && staged) {
+                const SPos<R> sp = s_p[si];
+                xi[0] = sp.x; xi[1] = sp.y; xi[2] = sp.z;
+                wi = sp.w;
+                const int ti = wi & 0xff;
+                for (int k = sub; k < 27; k += L) {
+                    const int dz = k / 9 - 1, dy = (k / 3) % 3 - 1, dx = k % 3 - 1;
+                    if (!small_axis_ok(dx, n0, per[0]) || !small_axis_ok(dy, n1, per[1]) ||
+                        !small_axis_ok(dz, n2, per[2]))
+                        continue;
+                    const int h2 = h + (dz * hy + dy) * hx + dx;
+                    const int c2 = s_cnt[h2], o2 = s_off[h2];
+                    for (int j = 0; j < c2; ++j) {
+                        const int tj = o2 + j;
+                        if (tj == si) continue;
+                        const SPos<R> pj = s_p[tj];
+                        const R xj[3] = {pj.x, pj.y, pj.z};
+                        pair_accum<R, 0>(xi, ti, xj, pj.w, bx, per, a.tab, acc, nc, hh, 0);
+                    }
+                }
+            } else if (active) {
+                // brick too dense for the shared-memory stage: global loads
+                cur.load_xyzw(self, xi, wi);
+                neighbourhood<R, 0>(cur, cnt_cur, s, x0 - 1 + ix, y0 - 1 + iy, z0 - 1 + iz, self, xi,
+                                    wi & 0xff, a.tab, sub, L, acc, nc, hh);
+            }
+            acc.reduce_xor(L);
+            if (active && sub == 0) {
+                R F[3];
+                acc.force(F);
+                finish_particle<R>(a, s, it.sys, self, xi, wi, F, t, cur, nxt, cnt_nxt);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 // advances the device step counter after a captured run of n steps, unless a
 // step failed (the host then resumes from the failing step)
 __global__ void advance_kernel(long long* step, const int* err, int n)
@@ -441,7 +671,7 @@ __global__ void bin_kernel(const SysDev* sys, int nsys, long long ntot, Dense<R>
         const int slot = atomicAdd(cnt + s.cell_base + c, 1);
         if (slot >= (1 << s.cap_log2)) { atomicOr(err, EF_OVERFLOW); continue; }
         const long long dst = s.slot_base + ((long long)c << s.cap_log2) + slot;
-        if constexpr (sizeof(R) == 4) { b.pos[dst] = d.pos[g]; b.cmp[dst] = d.cmp[g]; }
+        if constexpr (sizeof(R) == 4) { b.rec[2 * dst] = d.pos[g]; b.rec[2 * dst + 1] = d.cmp[g]; }
         else { b.st[dst] = d.st[g]; }
     }
 }
@@ -461,9 +691,9 @@ __global__ void gather_kernel(const SysDev* sys, int nsys, long long ncells_tot,
         const long long base = s.slot_base + ((gc - s.cell_base) << s.cap_log2);
         for (int q = 0; q < n && q < cap; ++q) {
             if constexpr (sizeof(R) == 4) {
-                float4 c = b.cmp[base + q];
+                float4 c = b.rec[2 * (base + q) + 1];
                 long long g = s.part_base + __float_as_int(c.w);
-                d.pos[g] = b.pos[base + q];
+                d.pos[g] = b.rec[2 * (base + q)];
                 d.cmp[g] = c;
             } else {
                 Rec64 r = b.st[base + q];
@@ -666,7 +896,7 @@ __global__ void msd_kernel(const SysDev* sys, int nsys, long long ncells_tot, St
             double u[3];
             int w, id;
             if constexpr (sizeof(R) == 4) {
-                float4 p = b.pos[base + q], c = b.cmp[base + q];
+                float4 p = b.rec[2 * (base + q)], c = b.rec[2 * (base + q) + 1];
                 u[0] = (double)p.x - (double)c.x;
                 u[1] = (double)p.y - (double)c.y;
                 u[2] = (double)p.z - (double)c.z;

@@ -34,7 +34,7 @@ class Engine:
     potentials (boxes=[(lo, hi, periodic, seed), ...])."""
 
     def __init__(self, system, precision="f64", device=0, seed=0, boxes=None, cell_cap=0,
-                 lanes_per_particle=0, cells_per_lane=0, graph_steps=0):
+                 lanes_per_particle=0, cells_per_lane=0, graph_steps=0, kernel_variant=0):
         self.system = system
         self._desc = system.to_desc()
         opt = A.Options()
@@ -44,6 +44,7 @@ class Engine:
         opt.lanes_per_particle = lanes_per_particle
         opt.cells_per_lane = cells_per_lane
         opt.graph_steps = graph_steps
+        opt.kernel_variant = kernel_variant
         opt.seed = seed
         self.precision = precision
         h = C.c_void_p()
