@@ -321,22 +321,28 @@ void orc_to_rel_f32(const rdgpu_system_desc* d, int64_t n, const double* xabs, f
     }
 }
 
-/* minimum image of one component (CudaSimulation.cu:996-1002) */
-static inline double mimg(double dx, double L, double half, int per)
+/* Minimum-image displacement of one component (CudaSimulation.cu:996-1002):
+   the image k in {-1, 0, +1} is chosen by comparing xi - xj with half a box,
+   and the displacement is then formed as xi - (xj + k L).  Both the oracle
+   and the engine round exactly this sequence; the engine's shared-memory
+   stage applies the same image shift to the staged xj.                      */
+static inline double mimg(double xi, double xj, double L, double half, int per)
 {
+    double d = xi - xj;
     if (per) {
-        if (dx > half) dx -= L;
-        else if (dx < -half) dx += L;
+        if (d > half) d = xi - (xj + L);
+        else if (d < -half) d = xi - (xj - L);
     }
-    return dx;
+    return d;
 }
-static inline float mimgf(float dx, float L, float half, int per)
+static inline float mimgf(float xi, float xj, float L, float half, int per)
 {
+    float d = xi - xj;
     if (per) {
-        if (dx > half) dx -= L;
-        else if (dx < -half) dx += L;
+        if (d > half) d = xi - (xj + L);
+        else if (d < -half) d = xi - (xj - L);
     }
-    return dx;
+    return d;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -452,9 +458,9 @@ static void particle_force(const rdgpu_system_desc* d, const tables_t* t,
         const int64_t j = NB_J(c, q);
         if (j == i) continue;
         const int tj = types[j];
-        double dx = mimg(x[3 * i + 0] - x[3 * j + 0], t->L[0], t->half[0], t->per[0]);
-        double dy = mimg(x[3 * i + 1] - x[3 * j + 1], t->L[1], t->half[1], t->per[1]);
-        double dz = mimg(x[3 * i + 2] - x[3 * j + 2], t->L[2], t->half[2], t->per[2]);
+        double dx = mimg(x[3 * i + 0], x[3 * j + 0], t->L[0], t->half[0], t->per[0]);
+        double dy = mimg(x[3 * i + 1], x[3 * j + 1], t->L[1], t->half[1], t->per[1]);
+        double dz = mimg(x[3 * i + 2], x[3 * j + 2], t->L[2], t->half[2], t->per[2]);
         double r2 = dx * dx + dy * dy + dz * dz;
         if (r2 < t->rc2[ti * MT + tj]) {
             double r = sqrt(r2);
@@ -529,9 +535,9 @@ void orc_neighbor_digest_f64(const rdgpu_system_desc* d, int64_t n, const double
         for (int64_t j = 0; j < n; ++j) {
             if (j == i) continue;
             const int tj = types[j];
-            double dx = mimg(x[3 * i + 0] - x[3 * j + 0], t.L[0], t.half[0], t.per[0]);
-            double dy = mimg(x[3 * i + 1] - x[3 * j + 1], t.L[1], t.half[1], t.per[1]);
-            double dz = mimg(x[3 * i + 2] - x[3 * j + 2], t.L[2], t.half[2], t.per[2]);
+            double dx = mimg(x[3 * i + 0], x[3 * j + 0], t.L[0], t.half[0], t.per[0]);
+            double dy = mimg(x[3 * i + 1], x[3 * j + 1], t.L[1], t.half[1], t.per[1]);
+            double dz = mimg(x[3 * i + 2], x[3 * j + 2], t.L[2], t.half[2], t.per[2]);
             double r2 = (dx * dx + dy * dy) + dz * dz;
             if (r2 < t.rc2[ti * MT + tj]) { cnt++; h += orc_splitmix64((uint64_t)j); }
         }
@@ -552,9 +558,9 @@ void orc_neighbor_digest_f32(const rdgpu_system_desc* d, int64_t n, const float*
         for (int64_t j = 0; j < n; ++j) {
             if (j == i) continue;
             const int tj = types[j];
-            float dx = mimgf(x[3 * i + 0] - x[3 * j + 0], t.Lf[0], t.halff[0], t.per[0]);
-            float dy = mimgf(x[3 * i + 1] - x[3 * j + 1], t.Lf[1], t.halff[1], t.per[1]);
-            float dz = mimgf(x[3 * i + 2] - x[3 * j + 2], t.Lf[2], t.halff[2], t.per[2]);
+            float dx = mimgf(x[3 * i + 0], x[3 * j + 0], t.Lf[0], t.halff[0], t.per[0]);
+            float dy = mimgf(x[3 * i + 1], x[3 * j + 1], t.Lf[1], t.halff[1], t.per[1]);
+            float dz = mimgf(x[3 * i + 2], x[3 * j + 2], t.Lf[2], t.halff[2], t.per[2]);
             float r2 = (dx * dx + dy * dy) + dz * dz;
             if (r2 < t.rc2f[ti * MT + tj]) { cnt++; h += orc_splitmix64((uint64_t)j); }
         }
@@ -645,9 +651,9 @@ static void rdf_core(const rdgpu_system_desc* d, int64_t n, const double* x,
             const int64_t j = NB_J(&c, q);
             if (j == i) continue;
             const int tj = types[j];
-            double dx = mimg(x[3 * i + 0] - x[3 * j + 0], t.L[0], t.half[0], t.per[0]);
-            double dy = mimg(x[3 * i + 1] - x[3 * j + 1], t.L[1], t.half[1], t.per[1]);
-            double dz = mimg(x[3 * i + 2] - x[3 * j + 2], t.L[2], t.half[2], t.per[2]);
+            double dx = mimg(x[3 * i + 0], x[3 * j + 0], t.L[0], t.half[0], t.per[0]);
+            double dy = mimg(x[3 * i + 1], x[3 * j + 1], t.L[1], t.half[1], t.per[1]);
+            double dz = mimg(x[3 * i + 2], x[3 * j + 2], t.L[2], t.half[2], t.per[2]);
             double r2 = (dx * dx + dy * dy) + dz * dz;
             if (r2 < e2[nbins]) {
                 int b = rdf_bin(e2, nbins, w, r2);

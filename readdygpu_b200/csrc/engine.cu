@@ -60,6 +60,7 @@ struct rdgpu_engine {
     // dense scratch (by global particle index)
     void* denseA = nullptr;
     void* denseB = nullptr;
+    long long cap_particles = 0;         // capacity of the per-particle scratch
     double* x0_d = nullptr;              // MSD origin, box-relative unwrapped
     double* vec_d = nullptr;             // 3N doubles scratch
     double* val_d = nullptr;             // N doubles scratch
@@ -98,9 +99,6 @@ using Engine = rdgpu_engine;
             return (e_ == cudaErrorMemoryAllocation) ? RDGPU_ERR_NOMEM : RDGPU_ERR_CUDA; \
         }                                                                          \
     } while (0)
-
-inline float i2f(int v) { float f; memcpy(&f, &v, 4); return f; }
-inline int f2i(float f) { int v; memcpy(&v, &f, 4); return v; }
 
 int fail(Engine* E, int code, const std::string& msg)
 {
@@ -250,6 +248,7 @@ void free_particles(Engine* E)
 {
     dfree(E->denseA); dfree(E->denseB); dfree(E->x0_d); dfree(E->vec_d); dfree(E->val_d);
     dfree(E->ityp_d); dfree(E->u64_d);
+    E->cap_particles = 0;
 }
 
 // bytes of one slot record (FP32C: pos + compensation; FP64: Rec64)
@@ -572,17 +571,6 @@ template <class R> int do_steps(Engine* E, long long nsteps, const double* noise
     return fail(E, RDGPU_ERR_OVERFLOW, "repeated cell overflow");
 }
 
-// host conversion of absolute coordinates into the stored representation
-// (the same IEEE operations as the oracle's orc_to_rel_f64 / orc_to_rel_f32)
-double wrap_rel(double x, double L, int per)
-{
-    if (!per) return x;
-    while (x >= L) x -= L;
-    while (x < 0.0) x += L;
-    if (x >= L) x = 0.0;
-    return x;
-}
-
 int setup_systems(Engine* E, std::string& why)
 {
     const rdgpu_system_desc& d = E->desc;
@@ -654,10 +642,28 @@ int setup_systems(Engine* E, std::string& why)
     return 0;
 }
 
+// grow-only device scratch sized by the particle count
+int ensure_particle_buffers(Engine* E, long long ntot)
+{
+    const long long N = std::max<long long>(ntot, 1);
+    if (N <= E->cap_particles) return RDGPU_OK;
+    free_particles(E);
+    const long long M = N + N / 4;      // headroom for reactions adding particles
+    CK(cudaMalloc(&E->denseA, M * (E->prec == RDGPU_PREC_F32C ? 16 : 32)));
+    if (E->prec == RDGPU_PREC_F32C) CK(cudaMalloc(&E->denseB, M * 16));
+    CK(cudaMalloc(&E->x0_d, M * 3 * sizeof(double)));
+    CK(cudaMalloc(&E->vec_d, M * 3 * sizeof(double)));
+    CK(cudaMalloc(&E->val_d, M * sizeof(double)));
+    CK(cudaMalloc(&E->ityp_d, M * sizeof(int)));
+    CK(cudaMalloc(&E->u64_d, M * sizeof(unsigned long long)));
+    E->cap_particles = M;
+    return RDGPU_OK;
+}
+
 template <class R> int set_particles_impl(Engine* E, const long long* offsets, long long ntot,
                                           const double* xyz, const int* types)
 {
-    // validate everything before touching the handle's state
+    // validate the layout before touching the handle's state
     std::vector<long long> off;
     if (E->nsys == 1) {
         off = {0, ntot};
@@ -671,90 +677,58 @@ template <class R> int set_particles_impl(Engine* E, const long long* offsets, l
         long long n = off[s + 1] - off[s];
         if (n < 0 || n > 0x7fffffff) return fail(E, RDGPU_ERR_ARG, "invalid particle count");
     }
-    for (long long g = 0; g < ntot; ++g)
-        if (types[g] < 0 || types[g] >= E->desc.n_types) return fail(E, RDGPU_ERR_ARG, "particle type out of range");
-    for (long long g = 0; g < 3 * ntot; ++g)
-        if (!std::isfinite(xyz[g])) return fail(E, RDGPU_ERR_ARG, "non-finite coordinate");
     E->part_off.clear();   // no valid state until this call completes
+    bool sizes_changed = false;
     for (int s = 0; s < E->nsys; ++s) {
+        const int n = (int)(off[s + 1] - off[s]);
+        const int old = E->sys_h[s].npart;
+        if (E->bricks_h.empty() || n > old + old / 4 + 8 || n < old - old / 4 - 8) sizes_changed = true;
         E->sys_h[s].part_base = off[s];
-        E->sys_h[s].npart = (int)(off[s + 1] - off[s]);
+        E->sys_h[s].npart = n;
     }
-    E->npart_tot = ntot;
-    E->types_h.assign(types, types + ntot);
-    free_particles(E);
-    const long long N = std::max<long long>(ntot, 1);
-    CK(cudaMalloc(&E->denseA, N * (E->prec == RDGPU_PREC_F32C ? 16 : 32)));
-    if (E->prec == RDGPU_PREC_F32C) CK(cudaMalloc(&E->denseB, N * 16));
-    CK(cudaMalloc(&E->x0_d, N * 3 * sizeof(double)));
-    CK(cudaMalloc(&E->vec_d, N * 3 * sizeof(double)));
-    CK(cudaMalloc(&E->val_d, N * sizeof(double)));
-    CK(cudaMalloc(&E->ityp_d, N * sizeof(int)));
-    CK(cudaMalloc(&E->u64_d, N * sizeof(unsigned long long)));
-    // host conversion into the stored representation
-    std::vector<double> x0(3 * N);
-    if constexpr (sizeof(R) == 4) {
-        std::vector<float4> hp(N), hc(N);
-        for (int s = 0; s < E->nsys; ++s) {
-            const SysDev& v = E->sys_h[s];
-            for (long long g = off[s]; g < off[s + 1]; ++g) {
-                float h[3], c[3];
-                for (int a = 0; a < 3; ++a) {
-                    const float Lf = v.Lf[a];
-                    double xr = wrap_rel(xyz[3 * g + a] - v.lo[a], (double)Lf, v.per[a]);
-                    float hh = (float)xr;
-                    if (v.per[a] && hh >= Lf) { hh = 0.0f; xr -= (double)Lf; }
-                    h[a] = hh;
-                    c[a] = (float)((double)hh - xr);
-                    x0[3 * g + a] = xr;
-                }
-                hp[g] = make_float4(h[0], h[1], h[2], i2f(types[g]));
-                hc[g] = make_float4(c[0], c[1], c[2], i2f((int)(g - off[s])));
-            }
-        }
-        CK(cudaMemcpyAsync(E->denseA, hp.data(), ntot * 16, cudaMemcpyHostToDevice, E->stream));
-        CK(cudaMemcpyAsync(E->denseB, hc.data(), ntot * 16, cudaMemcpyHostToDevice, E->stream));
-        CK(cudaMemcpyAsync(E->x0_d, x0.data(), ntot * 3 * sizeof(double), cudaMemcpyHostToDevice, E->stream));
-        CK(cudaStreamSynchronize(E->stream));
-    } else {
-        std::vector<Rec64> hr(N);
-        for (int s = 0; s < E->nsys; ++s) {
-            const SysDev& v = E->sys_h[s];
-            for (long long g = off[s]; g < off[s + 1]; ++g) {
-                Rec64 r;
-                double* xr[3] = {&r.x, &r.y, &r.z};
-                for (int a = 0; a < 3; ++a) {
-                    *xr[a] = wrap_rel(xyz[3 * g + a] - v.lo[a], v.L[a], v.per[a]);
-                    x0[3 * g + a] = *xr[a];
-                }
-                r.w = types[g];
-                r.id = (int)(g - off[s]);
-                hr[g] = r;
-            }
-        }
-        CK(cudaMemcpyAsync(E->denseA, hr.data(), ntot * 32, cudaMemcpyHostToDevice, E->stream));
-        CK(cudaMemcpyAsync(E->x0_d, x0.data(), ntot * 3 * sizeof(double), cudaMemcpyHostToDevice, E->stream));
-        CK(cudaStreamSynchronize(E->stream));
-    }
-    // lay out with the current caps and bin (caps grow on overflow)
-    int rc = alloc_state(E);
+    int rc = ensure_particle_buffers(E, ntot);
     if (rc) return rc;
+    E->npart_tot = ntot;
+    CK(cudaMemcpyAsync(E->sys_d, E->sys_h.data(), E->nsys * sizeof(SysDev), cudaMemcpyHostToDevice, E->stream));
+    CK(cudaMemsetAsync(E->err, 0, sizeof(int), E->stream));
+    if (ntot > 0) {
+        // inputs: coordinates into the 3N scratch, types into the N scratch
+        CK(cudaMemcpyAsync(E->vec_d, xyz, ntot * 3 * sizeof(double), cudaMemcpyHostToDevice, E->stream));
+        CK(cudaMemcpyAsync(E->ityp_d, types, ntot * sizeof(int), cudaMemcpyHostToDevice, E->stream));
+        ingest_kernel<R><<<grid_for(ntot), 256, 0, E->stream>>>(E->sys_d, E->nsys, ntot, E->vec_d, E->ityp_d,
+                                                                E->desc.n_types, dense<R>(E), E->x0_d, E->err);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(E->pinned_err, E->err, sizeof(int), cudaMemcpyDeviceToHost, E->stream));
+        CK(cudaStreamSynchronize(E->stream));
+        if (*E->pinned_err & EF_BADINPUT)
+            return fail(E, RDGPU_ERR_ARG, "particle type out of range, non-finite coordinate, or a coordinate "
+                                          "more than 64 box lengths outside the box");
+    }
+    E->types_h.assign(types, types + ntot);
+    // lay out (once, or after the caps grew) and bin
+    if (!E->bufA[0]) {
+        rc = alloc_state(E);
+        if (rc) return rc;
+    }
     rc = bin_dense<R>(E, 0, 0);
     if (rc) return rc;
-    rc = build_items(E);
-    if (rc) return rc;
-    // per-system lanes per particle: from the options or the size-bucket table
     for (int s = 0; s < E->nsys; ++s) {
         int L = E->opt.lanes_per_particle;
         if (L <= 0) L = 1;
         E->sys_h[s].lanes_log2 = ceil_log2(std::min(std::max(L, 1), 8));
     }
     CK(cudaMemcpyAsync(E->sys_d, E->sys_h.data(), E->nsys * sizeof(SysDev), cudaMemcpyHostToDevice, E->stream));
-    rc = build_bricks(E);
-    if (rc) return rc;
-    dfree(E->rdf_acc);
+    if (sizes_changed || E->items_h.empty()) {
+        rc = build_items(E);
+        if (rc) return rc;
+        rc = build_bricks(E);
+        if (rc) return rc;
+    }
     E->rdf_frames = 0;
-    E->rdf_nbins = 0;
+    if (E->rdf_acc && E->rdf_nbins > 0) {
+        const int S = E->desc.n_types;
+        CK(cudaMemsetAsync(E->rdf_acc, 0, (size_t)S * S * E->rdf_nbins * sizeof(unsigned long long), E->stream));
+    }
     rc = prepare_step_state(E, 0);
     if (rc) return rc;
     E->part_off = off;
@@ -767,38 +741,12 @@ template <class R> int get_particles_impl(Engine* E, double* xyz, int* types)
     int rc = gather_dense<R>(E, (int)(t & 1), (int)(t % 3));
     if (rc) return rc;
     const long long N = E->npart_tot;
-    if constexpr (sizeof(R) == 4) {
-        std::vector<float4> hp(N), hc(N);
-        CK(cudaMemcpyAsync(hp.data(), E->denseA, N * 16, cudaMemcpyDeviceToHost, E->stream));
-        CK(cudaMemcpyAsync(hc.data(), E->denseB, N * 16, cudaMemcpyDeviceToHost, E->stream));
-        CK(cudaStreamSynchronize(E->stream));
-        for (int s = 0; s < E->nsys; ++s) {
-            const SysDev& v = E->sys_h[s];
-            for (long long g = E->part_off[s]; g < E->part_off[s + 1]; ++g) {
-                if (xyz) {
-                    xyz[3 * g + 0] = ((double)hp[g].x - (double)hc[g].x) + v.lo[0];
-                    xyz[3 * g + 1] = ((double)hp[g].y - (double)hc[g].y) + v.lo[1];
-                    xyz[3 * g + 2] = ((double)hp[g].z - (double)hc[g].z) + v.lo[2];
-                }
-                if (types) types[g] = f2i(hp[g].w) & 0xff;
-            }
-        }
-    } else {
-        std::vector<Rec64> hr(N);
-        CK(cudaMemcpyAsync(hr.data(), E->denseA, N * 32, cudaMemcpyDeviceToHost, E->stream));
-        CK(cudaStreamSynchronize(E->stream));
-        for (int s = 0; s < E->nsys; ++s) {
-            const SysDev& v = E->sys_h[s];
-            for (long long g = E->part_off[s]; g < E->part_off[s + 1]; ++g) {
-                if (xyz) {
-                    xyz[3 * g + 0] = hr[g].x + v.lo[0];
-                    xyz[3 * g + 1] = hr[g].y + v.lo[1];
-                    xyz[3 * g + 2] = hr[g].z + v.lo[2];
-                }
-                if (types) types[g] = hr[g].w & 0xff;
-            }
-        }
-    }
+    if (N == 0) return RDGPU_OK;
+    emit_kernel<R><<<grid_for(N), 256, 0, E->stream>>>(E->sys_d, E->nsys, N, dense<R>(E), E->vec_d, E->ityp_d);
+    CK(cudaGetLastError());
+    if (xyz) CK(cudaMemcpyAsync(xyz, E->vec_d, N * 3 * sizeof(double), cudaMemcpyDeviceToHost, E->stream));
+    if (types) CK(cudaMemcpyAsync(types, E->ityp_d, N * sizeof(int), cudaMemcpyDeviceToHost, E->stream));
+    CK(cudaStreamSynchronize(E->stream));
     return RDGPU_OK;
 }
 

@@ -191,15 +191,19 @@ template <> struct Box<double> {
     }
 };
 
-// minimum image (CudaSimulation.cu:996-1002)
+// Minimum-image displacement of one component (CudaSimulation.cu:996-1002):
+// the image k in {-1, 0, +1} is chosen by comparing xi - xj with half a box,
+// the displacement is then formed as xi - (xj + k L).  The CPU oracle rounds
+// the same sequence, which keeps the neighbour predicate bit-exact.
 template <class R>
-__device__ __forceinline__ R mimg(R dx, R L, R half, int per)
+__device__ __forceinline__ R mimg(R xi, R xj, R L, R half, int per)
 {
+    R d = sub_rn(xi, xj);
     if (per) {
-        if (dx > half) dx = sub_rn(dx, L);
-        else if (dx < -half) dx = add_rn(dx, L);
+        if (d > half) d = sub_rn(xi, add_rn(xj, L));
+        else if (d < -half) d = sub_rn(xi, sub_rn(xj, L));
     }
-    return dx;
+    return d;
 }
 
 // r^2 = (dx*dx + dy*dy) + dz*dz, rounded after every operation

@@ -112,9 +112,9 @@ __device__ __forceinline__ void pair_accum(const R xi[3], int ti, const R xj[3],
                                            const int per[3], const TypeTab<R>* __restrict__ tab, Acc<R>& acc,
                                            int& ncount, unsigned long long& hash, int idj)
 {
-    R dx = mimg(sub_rn(xi[0], xj[0]), bx.L[0], bx.half[0], per[0]);
-    R dy = mimg(sub_rn(xi[1], xj[1]), bx.L[1], bx.half[1], per[1]);
-    R dz = mimg(sub_rn(xi[2], xj[2]), bx.L[2], bx.half[2], per[2]);
+    R dx = mimg(xi[0], xj[0], bx.L[0], bx.half[0], per[0]);
+    R dy = mimg(xi[1], xj[1], bx.L[1], bx.half[1], per[1]);
+    R dz = mimg(xi[2], xj[2], bx.L[2], bx.half[2], per[2]);
     R r2 = dist2(dx, dy, dz);
     const int pidx = ti * MAXT + (wj & 0xff);
     if (r2 < tab->rc2[pidx]) {
@@ -418,7 +418,9 @@ __global__ void __launch_bounds__(BLOCK) step_kernel(StepArgs<R> a)
 // Bricks are strided statically over a persistent grid.
 // ---------------------------------------------------------------------------
 constexpr int MAXH = 512;     // halo cells per brick
-constexpr int MAXP = 1024;    // staged particles per brick
+constexpr int MAXP = 1024;    // staged particles per brick (FP32)
+constexpr int MAXP64 = 896;   // staged particles per brick (FP64, 48 KB static smem)
+template <class R> struct StageCap { static constexpr int value = sizeof(R) == 4 ? MAXP : MAXP64; };
 
 struct BrickItem {
     int sys;
@@ -482,18 +484,54 @@ __device__ __forceinline__ bool small_axis_ok(int d, int n, int per)
     return d == 0;
 }
 
+// Pair term accumulation for a staged neighbour (image already applied)
+template <class R>
+__device__ __forceinline__ void staged_pair(R xi0, R xi1, R xi2, int ti, const SPos<R>& pj, bool notself,
+                                            const R* __restrict__ s_rc2, const TypeTab<R>* __restrict__ tab,
+                                            Acc<R>& acc)
+{
+    const R dx = sub_rn(xi0, pj.x), dy = sub_rn(xi1, pj.y), dz = sub_rn(xi2, pj.z);
+    const R r2 = dist2(dx, dy, dz);
+    const int pidx = ti * MAXT + (pj.w & 0xff);
+    if (r2 < s_rc2[pidx] && notself) {
+        const R r = sqrt(r2);
+        const int nt = tab->nterm[pidx];
+        for (int m = 0; m < nt; ++m) {
+            R pre, e;
+            pair_term(tab->term[pidx * MAX_TERMS + m], r, pre, e);
+            acc.add(pre, dx, dy, dz);
+        }
+    }
+}
+
+template <class R>
+__device__ __noinline__ void brick_fallback(const StateBuf<R> cur, const int* __restrict__ cnt_cur, const SysDev& s,
+                                            int gc, long long self, const TypeTab<R>* __restrict__ tab, int sub,
+                                            int L, Acc<R>& acc, R& xi0, R& xi1, R& xi2, int& wi)
+{
+    R xi[3];
+    cur.load_xyzw(self, xi, wi);
+    xi0 = xi[0]; xi1 = xi[1]; xi2 = xi[2];
+    const int cx = gc % s.n[0], cy = (gc / s.n[0]) % s.n[1], cz = gc / (s.n[0] * s.n[1]);
+    int nc = 0;
+    unsigned long long hh = 0;
+    neighbourhood<R, 0>(cur, cnt_cur, s, cx, cy, cz, self, xi, wi & 0xff, tab, sub, L, acc, nc, hh);
+}
+
 template <class R, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) brick_step_kernel(StepArgs<R> a, const BrickItem* __restrict__ bricks,
                                                            int nbricks)
 {
     __shared__ int s_cnt[MAXH];
     __shared__ int s_off[MAXH + 1];
-    __shared__ int s_gc[MAXH];
+    __shared__ int s_gc[MAXH];          // global cell | image code << 26 (2 bits per axis)
     __shared__ int s_icnt[MAXH];
     __shared__ int s_ioff[MAXH + 1];
-    __shared__ short s_ih[MAXH];
     __shared__ int s_warp[BLOCK / 32];
-    __shared__ SPos<R> s_p[MAXP];
+    constexpr int SCAP = StageCap<R>::value;
+    __shared__ int s_ilist[SCAP];       // inner particle -> staged index | halo cell << 12
+    __shared__ SPos<R> s_p[SCAP];
+    __shared__ R s_rc2[MAXT * MAXT];
 
     if (*((volatile int*)a.err)) return;   // an earlier step failed: keep its input intact
     const int tid = threadIdx.x;
@@ -503,6 +541,7 @@ __global__ void __launch_bounds__(BLOCK) brick_step_kernel(StepArgs<R> a, const 
     int* cnt_nxt = a.cnt[(b3 + 1) % 3];
     int* cnt_free = a.cnt[(b3 + 2) % 3];
     const StateBuf<R> cur = a.buf[t & 1], nxt = a.buf[(t + 1) & 1];
+    for (int i = tid; i < MAXT * MAXT; i += BLOCK) s_rc2[i] = a.tab->rc2[i];
 
     for (int bi = blockIdx.x; bi < nbricks; bi += gridDim.x) {
         const BrickItem it = bricks[bi];
@@ -514,104 +553,117 @@ __global__ void __launch_bounds__(BLOCK) brick_step_kernel(StepArgs<R> a, const 
         const int H = hx * hy * hz, NI = ex * ey * ez;
         const int cap_log2 = s.cap_log2, cap = 1 << cap_log2;
         const int n0 = s.n[0], n1 = s.n[1], n2 = s.n[2];
+        const int per0 = s.per[0], per1 = s.per[1], per2 = s.per[2];
 
-        // 1. halo cell counts; clear the brick's cells in the free count array
-        for (int h = tid; h < H; h += BLOCK) {
-            const int ix = h % hx, iy = (h / hx) % hy, iz = h / (hx * hy);
-            int gx, gy, gz;
-            const bool v = halo_axis(x0 - 1 + ix, n0, s.per[0], gx) && halo_axis(y0 - 1 + iy, n1, s.per[1], gy) &&
-                           halo_axis(z0 - 1 + iz, n2, s.per[2], gz);
-            const int gc = v ? (gz * n1 + gy) * n0 + gx : -1;
-            s_gc[h] = gc;
-            s_cnt[h] = v ? min(cnt_cur[s.cell_base + gc], cap) : 0;
-        }
-        for (int k = tid; k < NI; k += BLOCK) {
-            const int ix = 1 + k % ex, iy = 1 + (k / ex) % ey, iz = 1 + k / (ex * ey);
-            const int h = (iz * hy + iy) * hx + ix;
-            s_ih[k] = (short)h;
-            cnt_free[s.cell_base + ((z0 + iz - 1) * n1 + (y0 + iy - 1)) * n0 + (x0 + ix - 1)] = 0;
+        // 1. halo rows (y, z): global cell, image shift, count
+        for (int r = tid; r < hy * hz; r += BLOCK) {
+            const int iz = r / hy, iy = r - iz * hy;
+            int gy = y0 - 1 + iy, gz = z0 - 1 + iz, ky = 0, kz = 0;
+            bool vyz = true;
+            if (gy < 0) { if (per1) { gy += n1; ky = -1; } else vyz = false; }
+            else if (gy >= n1) { if (per1) { gy -= n1; ky = 1; } else vyz = false; }
+            if (gz < 0) { if (per2) { gz += n2; kz = -1; } else vyz = false; }
+            else if (gz >= n2) { if (per2) { gz -= n2; kz = 1; } else vyz = false; }
+            const int rowc = (gz * n1 + gy) * n0;
+            const bool inner_row = iy >= 1 && iy <= ey && iz >= 1 && iz <= ez;
+            for (int ix = 0; ix < hx; ++ix) {
+                int gx = x0 - 1 + ix, kx = 0;
+                bool v = vyz;
+                if (gx < 0) { if (per0) { gx += n0; kx = -1; } else v = false; }
+                else if (gx >= n0) { if (per0) { gx -= n0; kx = 1; } else v = false; }
+                const int h = r * hx + ix;
+                const int gc = rowc + gx;
+                s_gc[h] = v ? (gc | (((kx + 1) | ((ky + 1) << 2) | ((kz + 1) << 4)) << 26)) : -1;
+                s_cnt[h] = v ? min(cnt_cur[s.cell_base + gc], cap) : 0;
+                if (inner_row && ix >= 1 && ix <= ex) {
+                    const int kin = ((iz - 1) * ey + (iy - 1)) * ex + (ix - 1);
+                    s_icnt[kin] = s_cnt[h];
+                    cnt_free[s.cell_base + gc] = 0;
+                }
+            }
         }
         __syncthreads();
-        for (int k = tid; k < NI; k += BLOCK) s_icnt[k] = s_cnt[s_ih[k]];
         const int T = block_excl_scan<BLOCK>(s_cnt, s_off, H, s_warp);
         const int TI = block_excl_scan<BLOCK>(s_icnt, s_ioff, NI, s_warp);
-        const bool staged = T <= MAXP;
+        // systems with fewer than 3 cells on a periodic axis take the global path
+        const bool small = (per0 && n0 < 3) || (per1 && n1 < 3) || (per2 && n2 < 3);
+        const bool staged = T <= SCAP && !small;
 
-        // 2. stage positions of the brick + halo
+        // 2. stage brick + halo with the image shift applied; list the inner particles
         if (staged) {
+            R Lx, Ly, Lz;
+            if constexpr (sizeof(R) == 4) { Lx = s.Lf[0]; Ly = s.Lf[1]; Lz = s.Lf[2]; }
+            else { Lx = s.L[0]; Ly = s.L[1]; Lz = s.L[2]; }
             for (int h = tid; h < H; h += BLOCK) {
                 const int c = s_cnt[h];
                 if (c == 0) continue;
-                const long long g = s.slot_base + ((long long)s_gc[h] << cap_log2);
+                const int code = s_gc[h];
+                const int gc = code & ((1 << 26) - 1);
+                const int kx = ((code >> 26) & 3) - 1, ky = ((code >> 28) & 3) - 1, kz = ((code >> 30) & 3) - 1;
+                const long long g = s.slot_base + ((long long)gc << cap_log2);
                 const int o = s_off[h];
                 for (int q = 0; q < c; ++q) {
                     R xq[3];
                     int wq;
                     cur.load_xyzw(g + q, xq, wq);
                     SPos<R> sp;
-                    sp.x = xq[0]; sp.y = xq[1]; sp.z = xq[2]; sp.w = wq;
+                    sp.x = kx == 0 ? xq[0] : add_rn(xq[0], kx > 0 ? Lx : -Lx);
+                    sp.y = ky == 0 ? xq[1] : add_rn(xq[1], ky > 0 ? Ly : -Ly);
+                    sp.z = kz == 0 ? xq[2] : add_rn(xq[2], kz > 0 ? Lz : -Lz);
+                    sp.w = wq;
                     s_p[o + q] = sp;
                 }
             }
         }
+        for (int kin = tid; kin < NI; kin += BLOCK) {
+            const int c = s_icnt[kin];
+            if (c == 0) continue;
+            const int ix = kin % ex, rest = kin / ex, iy = rest % ey, iz = rest / ey;
+            const int h = ((iz + 1) * hy + (iy + 1)) * hx + (ix + 1);
+            const int o = s_off[h], io = s_ioff[kin];
+            for (int q = 0; q < c; ++q) s_ilist[io + q] = (o + q) | (h << 12);
+        }
         __syncthreads();
 
-        // 3. groups of L lanes, one particle each
+        // 3. groups of L lanes, one particle each: 9 contiguous row ranges
         const int L = 1 << lg, G = BLOCK >> lg, g = tid >> lg, sub = tid & (L - 1);
-        Box<R> bx;
-        bx.load(s);
-        const int per[3] = {s.per[0], s.per[1], s.per[2]};
         for (int base = 0; base < TI; base += G) {
             const int p = base + g;
             const bool active = p < TI;
             Acc<R> acc;
             acc.zero();
-            int nc = 0;
-            unsigned long long hh = 0;
-            R xi[3] = {R(0), R(0), R(0)};
-            int wi = 0, h = 0, q = 0, si = 0;
+            int si = 0, h = 0;
+            R xi0 = R(0), xi1 = R(0), xi2 = R(0);
+            int wi = 0;
             if (active) {
-                int lo = 0, hi = NI - 1;           // inner cell of particle p
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (s_ioff[mid] <= p) lo = mid; else hi = mid - 1;
-                }
-                h = s_ih[lo];
-                q = p - s_ioff[lo];
-                si = s_off[h] + q;
+                const int e = s_ilist[p];
+                si = e & 0xfff;
+                h = e >> 12;
             }
-            const int ix = h % hx, iy = (h / hx) % hy, iz = h / (hx * hy);
-            const long long self = s.slot_base + ((long long)(active ? s_gc[h] : 0) << cap_log2) + q;
+            const int q = si - s_off[h];
+            const long long self = s.slot_base + ((long long)(s_gc[h] & ((1 << 26) - 1)) << cap_log2) + q;
             if (active && staged) {
                 const SPos<R> sp = s_p[si];
-                xi[0] = sp.x; xi[1] = sp.y; xi[2] = sp.z;
+                xi0 = sp.x; xi1 = sp.y; xi2 = sp.z;
                 wi = sp.w;
                 const int ti = wi & 0xff;
-                for (int k = sub; k < 27; k += L) {
-                    const int dz = k / 9 - 1, dy = (k / 3) % 3 - 1, dx = k % 3 - 1;
-                    if (!small_axis_ok(dx, n0, per[0]) || !small_axis_ok(dy, n1, per[1]) ||
-                        !small_axis_ok(dz, n2, per[2]))
-                        continue;
-                    const int h2 = h + (dz * hy + dy) * hx + dx;
-                    const int c2 = s_cnt[h2], o2 = s_off[h2];
-                    for (int j = 0; j < c2; ++j) {
-                        const int tj = o2 + j;
-                        if (tj == si) continue;
-                        const SPos<R> pj = s_p[tj];
-                        const R xj[3] = {pj.x, pj.y, pj.z};
-                        pair_accum<R, 0>(xi, ti, xj, pj.w, bx, per, a.tab, acc, nc, hh, 0);
-                    }
+                for (int rr = sub; rr < 9; rr += L) {
+                    const int dz = rr / 3 - 1, dy = rr - (rr / 3) * 3 - 1;
+                    const int hrow = h + (dz * hy + dy) * hx;
+                    const int t0 = s_off[hrow - 1], t1 = s_off[hrow + 2];
+                    for (int tj = t0; tj < t1; ++tj)
+                        staged_pair<R>(xi0, xi1, xi2, ti, s_p[tj], tj != si, s_rc2, a.tab, acc);
                 }
             } else if (active) {
-                // brick too dense for the shared-memory stage: global loads
-                cur.load_xyzw(self, xi, wi);
-                neighbourhood<R, 0>(cur, cnt_cur, s, x0 - 1 + ix, y0 - 1 + iy, z0 - 1 + iz, self, xi,
-                                    wi & 0xff, a.tab, sub, L, acc, nc, hh);
+                // brick too dense for the stage, or a tiny periodic box: global loads
+                brick_fallback<R>(cur, cnt_cur, s, s_gc[h] & ((1 << 26) - 1), self, a.tab, sub, L, acc,
+                                  xi0, xi1, xi2, wi);
             }
             acc.reduce_xor(L);
             if (active && sub == 0) {
                 R F[3];
                 acc.force(F);
+                R xi[3] = {xi0, xi1, xi2};
                 finish_particle<R>(a, s, it.sys, self, xi, wi, F, t, cur, nxt, cnt_nxt);
             }
         }
@@ -673,6 +725,91 @@ __global__ void bin_kernel(const SysDev* sys, int nsys, long long ntot, Dense<R>
         const long long dst = s.slot_base + ((long long)c << s.cap_log2) + slot;
         if constexpr (sizeof(R) == 4) { b.rec[2 * dst] = d.pos[g]; b.rec[2 * dst + 1] = d.cmp[g]; }
         else { b.st[dst] = d.st[g]; }
+    }
+}
+
+constexpr int EF_BADINPUT = 8;
+
+// absolute coordinates -> the stored representation (the oracle's
+// orc_to_rel_f64 / orc_to_rel_f32: the same IEEE double operations), with
+// validation of types and coordinates.  The wrap loop is bounded: a
+// coordinate more than 64 box lengths outside the box is rejected.
+__device__ __forceinline__ bool wrap_rel_dev(double& x, double L, int per)
+{
+    if (!per) return true;
+    for (int k = 0; k < 64 && x >= L; ++k) x -= L;
+    for (int k = 0; k < 64 && x < 0.0; ++k) x += L;
+    if (x >= L || x < 0.0) {
+        if (x >= L && x - L < L) x = 0.0;   // x == L after rounding
+        else return false;
+    }
+    return true;
+}
+
+template <class R>
+__global__ void ingest_kernel(const SysDev* sys, int nsys, long long ntot, const double* __restrict__ xyz,
+                              const int* __restrict__ types, int ntypes, Dense<R> d, double* x0, int* err)
+{
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ntot;
+         g += (long long)gridDim.x * blockDim.x) {
+        const int si = find_sys_by_part(sys, nsys, g);
+        const SysDev& s = sys[si];
+        const int t = types[g];
+        bool ok = t >= 0 && t < ntypes;
+        const int id = (int)(g - s.part_base);
+        if constexpr (sizeof(R) == 4) {
+            float h[3], c[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const float Lf = s.Lf[a];
+                double xr = __dsub_rn(xyz[3 * g + a], s.lo[a]);
+                ok = ok && isfinite(xr) && wrap_rel_dev(xr, (double)Lf, s.per[a]);
+                float hh = __double2float_rn(xr);
+                if (s.per[a] && hh >= Lf) { hh = 0.0f; xr = __dsub_rn(xr, (double)Lf); }
+                h[a] = hh;
+                c[a] = __double2float_rn(__dsub_rn((double)hh, xr));
+                x0[3 * g + a] = xr;
+            }
+            d.pos[g] = make_float4(h[0], h[1], h[2], __int_as_float(t));
+            d.cmp[g] = make_float4(c[0], c[1], c[2], __int_as_float(id));
+        } else {
+            double x[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                double xr = __dsub_rn(xyz[3 * g + a], s.lo[a]);
+                ok = ok && isfinite(xr) && wrap_rel_dev(xr, s.L[a], s.per[a]);
+                x[a] = xr;
+                x0[3 * g + a] = xr;
+            }
+            Rec64 r;
+            r.x = x[0]; r.y = x[1]; r.z = x[2]; r.w = t; r.id = id;
+            d.st[g] = r;
+        }
+        if (!ok) atomicOr(err, EF_BADINPUT);
+    }
+}
+
+// dense arrays -> absolute coordinates and types (by global index)
+template <class R>
+__global__ void emit_kernel(const SysDev* sys, int nsys, long long ntot, Dense<R> d, double* xyz, int* types)
+{
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ntot;
+         g += (long long)gridDim.x * blockDim.x) {
+        const int si = find_sys_by_part(sys, nsys, g);
+        const SysDev& s = sys[si];
+        if constexpr (sizeof(R) == 4) {
+            const float4 p = d.pos[g], c = d.cmp[g];
+            xyz[3 * g + 0] = __dadd_rn(__dsub_rn((double)p.x, (double)c.x), s.lo[0]);
+            xyz[3 * g + 1] = __dadd_rn(__dsub_rn((double)p.y, (double)c.y), s.lo[1]);
+            xyz[3 * g + 2] = __dadd_rn(__dsub_rn((double)p.z, (double)c.z), s.lo[2]);
+            types[g] = __float_as_int(p.w) & 0xff;
+        } else {
+            const Rec64 r = d.st[g];
+            xyz[3 * g + 0] = __dadd_rn(r.x, s.lo[0]);
+            xyz[3 * g + 1] = __dadd_rn(r.y, s.lo[1]);
+            xyz[3 * g + 2] = __dadd_rn(r.z, s.lo[2]);
+            types[g] = r.w & 0xff;
+        }
     }
 }
 
@@ -852,9 +989,9 @@ __global__ void rdf_kernel(const SysDev* sys, int nsys, long long ncells_tot, St
                             R xq[3];
                             int wj;
                             b.load_xyzw(sb + j, xq, wj);
-                            double dx = mimg(__dsub_rn(xi0, (double)xq[0]), L[0], half[0], s.per[0]);
-                            double dy = mimg(__dsub_rn(xi1, (double)xq[1]), L[1], half[1], s.per[1]);
-                            double dz = mimg(__dsub_rn(xi2, (double)xq[2]), L[2], half[2], s.per[2]);
+                            double dx = mimg(xi0, (double)xq[0], L[0], half[0], s.per[0]);
+                            double dy = mimg(xi1, (double)xq[1], L[1], half[1], s.per[1]);
+                            double dz = mimg(xi2, (double)xq[2], L[2], half[2], s.per[2]);
                             double r2 = dist2(dx, dy, dz);
                             if (!(r2 < rmax2)) continue;
                             int k = (int)(sqrt(r2) / w);
