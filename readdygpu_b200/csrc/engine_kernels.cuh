@@ -311,6 +311,57 @@ __device__ __forceinline__ void finish_particle(const StepArgs<R>& a, const SysD
     }
 }
 
+// finish_particle with the compensation (FP32C) or id (FP64) already loaded
+template <class R>
+__device__ __forceinline__ void finish_particle_pre(const StepArgs<R>& a, const SysDev& s, int si, R xi[3], int wi,
+                                                    R F[3], long long t, float4 crec, int idpre,
+                                                    const StateBuf<R>& nxt, int* cnt_nxt)
+{
+    const int ti = wi & 0xff;
+    if (a.n_ext > 0) {
+        const ExtTerm<R>* ep = a.ext + (long long)si * a.n_ext;
+        R ee = R(0);
+        for (int e = 0; e < a.n_ext; ++e) {
+            if ((ep[e].tmask >> ti) & 1u) ext_force(ep[e], a.tab->prad[ti], xi, F, ee);
+        }
+    }
+    int id;
+    R c[3] = {R(0), R(0), R(0)};
+    if constexpr (sizeof(R) == 4) {
+        c[0] = crec.x; c[1] = crec.y; c[2] = crec.z;
+        id = __float_as_int(crec.w);
+    } else {
+        id = idpre;
+    }
+    R xn[3];
+    if (a.noise) {
+        const double* nz = a.noise + 3 * (s.part_base + id);
+        xn[0] = (R)nz[0]; xn[1] = (R)nz[1]; xn[2] = (R)nz[2];
+    } else {
+        bd_normals(s.seed, t, (long long)id, xn);
+    }
+    int ef = em_update(xi, c, wi, F, xn, a.tab->a[ti], a.tab->b[ti], s);
+    const int ncell = cell_index(s, xi);
+    const int slot = atomicAdd(cnt_nxt + s.cell_base + ncell, 1);
+    if (slot >= (1 << s.cap_log2)) {
+        ef |= EF_OVERFLOW;
+    } else {
+        const long long dst = s.slot_base + ((long long)ncell << s.cap_log2) + slot;
+        if constexpr (sizeof(R) == 4) {
+            nxt.rec[2 * dst] = make_float4(xi[0], xi[1], xi[2], __int_as_float(wi));
+            nxt.rec[2 * dst + 1] = make_float4(c[0], c[1], c[2], __int_as_float(id));
+        } else {
+            Rec64 r;
+            r.x = xi[0]; r.y = xi[1]; r.z = xi[2]; r.w = wi; r.id = id;
+            nxt.st[dst] = r;
+        }
+    }
+    if (ef) {
+        atomicOr(a.err, ef);
+        atomicMin((unsigned long long*)a.err_step, (unsigned long long)t);
+    }
+}
+
 template <class R>
 __device__ __forceinline__ void step_particle(const StepArgs<R>& a, const SysDev& s, int si, int lslot,
                                               bool active, int sub, int L, long long t,
@@ -518,17 +569,29 @@ __device__ __noinline__ void brick_fallback(const StateBuf<R> cur, const int* __
     neighbourhood<R, 0>(cur, cnt_cur, s, cx, cy, cz, self, xi, wi & 0xff, tab, sub, L, acc, nc, hh);
 }
 
+// asynchronous 16-byte global -> shared copy (no register round trip)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 template <class R, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) brick_step_kernel(StepArgs<R> a, const BrickItem* __restrict__ bricks,
                                                            int nbricks)
 {
+    constexpr int SCAP = StageCap<R>::value;
+    constexpr int HPT = MAXH / BLOCK;   // halo cells per thread
     __shared__ int s_cnt[MAXH];
     __shared__ int s_off[MAXH + 1];
     __shared__ int s_gc[MAXH];          // global cell | image code << 26 (2 bits per axis)
     __shared__ int s_icnt[MAXH];
     __shared__ int s_ioff[MAXH + 1];
     __shared__ int s_warp[BLOCK / 32];
-    constexpr int SCAP = StageCap<R>::value;
     __shared__ int s_ilist[SCAP];       // inner particle -> staged index | halo cell << 12
     __shared__ SPos<R> s_p[SCAP];
     __shared__ R s_rc2[MAXT * MAXT];
@@ -538,8 +601,8 @@ __global__ void __launch_bounds__(BLOCK) brick_step_kernel(StepArgs<R> a, const 
     const long long t = (a.step_ptr ? *a.step_ptr : 0LL) + a.step_off;
     const int b3 = (int)(t % 3);
     const int* __restrict__ cnt_cur = a.cnt[b3];
-    int* cnt_nxt = a.cnt[(b3 + 1) % 3];
-    int* cnt_free = a.cnt[(b3 + 2) % 3];
+    int* __restrict__ cnt_nxt = a.cnt[(b3 + 1) % 3];
+    int* __restrict__ cnt_free = a.cnt[(b3 + 2) % 3];
     const StateBuf<R> cur = a.buf[t & 1], nxt = a.buf[(t + 1) & 1];
     for (int i = tid; i < MAXT * MAXT; i += BLOCK) s_rc2[i] = a.tab->rc2[i];
 
@@ -555,30 +618,44 @@ __global__ void __launch_bounds__(BLOCK) brick_step_kernel(StepArgs<R> a, const 
         const int n0 = s.n[0], n1 = s.n[1], n2 = s.n[2];
         const int per0 = s.per[0], per1 = s.per[1], per2 = s.per[2];
 
-        // 1. halo rows (y, z): global cell, image shift, count
-        for (int r = tid; r < hy * hz; r += BLOCK) {
-            const int iz = r / hy, iy = r - iz * hy;
-            int gy = y0 - 1 + iy, gz = z0 - 1 + iz, ky = 0, kz = 0;
-            bool vyz = true;
-            if (gy < 0) { if (per1) { gy += n1; ky = -1; } else vyz = false; }
-            else if (gy >= n1) { if (per1) { gy -= n1; ky = 1; } else vyz = false; }
-            if (gz < 0) { if (per2) { gz += n2; kz = -1; } else vyz = false; }
-            else if (gz >= n2) { if (per2) { gz -= n2; kz = 1; } else vyz = false; }
-            const int rowc = (gz * n1 + gy) * n0;
-            const bool inner_row = iy >= 1 && iy <= ey && iz >= 1 && iz <= ez;
-            for (int ix = 0; ix < hx; ++ix) {
-                int gx = x0 - 1 + ix, kx = 0;
-                bool v = vyz;
+        // 1. halo cells: global cell, image shift, count -- all count loads in
+        //    flight together, then the shared-memory stores
+        int gcode[HPT], cval[HPT];
+#pragma unroll
+        for (int k = 0; k < HPT; ++k) {
+            const int h = tid + k * BLOCK;
+            gcode[k] = -1;
+            cval[k] = 0;
+            if (h < H) {
+                const int r = h / hx, ix = h - r * hx;
+                const int iz = r / hy, iy = r - iz * hy;
+                int gx = x0 - 1 + ix, gy = y0 - 1 + iy, gz = z0 - 1 + iz, kx = 0, ky = 0, kz = 0;
+                bool v = true;
                 if (gx < 0) { if (per0) { gx += n0; kx = -1; } else v = false; }
                 else if (gx >= n0) { if (per0) { gx -= n0; kx = 1; } else v = false; }
-                const int h = r * hx + ix;
-                const int gc = rowc + gx;
-                s_gc[h] = v ? (gc | (((kx + 1) | ((ky + 1) << 2) | ((kz + 1) << 4)) << 26)) : -1;
-                s_cnt[h] = v ? min(cnt_cur[s.cell_base + gc], cap) : 0;
-                if (inner_row && ix >= 1 && ix <= ex) {
-                    const int kin = ((iz - 1) * ey + (iy - 1)) * ex + (ix - 1);
-                    s_icnt[kin] = s_cnt[h];
-                    cnt_free[s.cell_base + gc] = 0;
+                if (gy < 0) { if (per1) { gy += n1; ky = -1; } else v = false; }
+                else if (gy >= n1) { if (per1) { gy -= n1; ky = 1; } else v = false; }
+                if (gz < 0) { if (per2) { gz += n2; kz = -1; } else v = false; }
+                else if (gz >= n2) { if (per2) { gz -= n2; kz = 1; } else v = false; }
+                if (v) {
+                    const int gc = (gz * n1 + gy) * n0 + gx;
+                    gcode[k] = gc | (((kx + 1) | ((ky + 1) << 2) | ((kz + 1) << 4)) << 26);
+                    cval[k] = __ldg(cnt_cur + s.cell_base + gc);
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < HPT; ++k) {
+            const int h = tid + k * BLOCK;
+            if (h < H) {
+                const int c = min(cval[k], cap);
+                s_gc[h] = gcode[k];
+                s_cnt[h] = c;
+                const int r = h / hx, ix = h - r * hx;
+                const int iz = r / hy, iy = r - iz * hy;
+                if (ix >= 1 && ix <= ex && iy >= 1 && iy <= ey && iz >= 1 && iz <= ez) {
+                    s_icnt[((iz - 1) * ey + (iy - 1)) * ex + (ix - 1)] = c;
+                    cnt_free[s.cell_base + (gcode[k] & ((1 << 26) - 1))] = 0;
                 }
             }
         }
@@ -589,29 +666,21 @@ __global__ void __launch_bounds__(BLOCK) brick_step_kernel(StepArgs<R> a, const 
         const bool small = (per0 && n0 < 3) || (per1 && n1 < 3) || (per2 && n2 < 3);
         const bool staged = T <= SCAP && !small;
 
-        // 2. stage brick + halo with the image shift applied; list the inner particles
+        // 2. stage brick + halo with asynchronous copies; list the inner particles
         if (staged) {
-            R Lx, Ly, Lz;
-            if constexpr (sizeof(R) == 4) { Lx = s.Lf[0]; Ly = s.Lf[1]; Lz = s.Lf[2]; }
-            else { Lx = s.L[0]; Ly = s.L[1]; Lz = s.L[2]; }
             for (int h = tid; h < H; h += BLOCK) {
                 const int c = s_cnt[h];
                 if (c == 0) continue;
-                const int code = s_gc[h];
-                const int gc = code & ((1 << 26) - 1);
-                const int kx = ((code >> 26) & 3) - 1, ky = ((code >> 28) & 3) - 1, kz = ((code >> 30) & 3) - 1;
-                const long long g = s.slot_base + ((long long)gc << cap_log2);
+                const long long g = s.slot_base + ((long long)(s_gc[h] & ((1 << 26) - 1)) << cap_log2);
                 const int o = s_off[h];
                 for (int q = 0; q < c; ++q) {
-                    R xq[3];
-                    int wq;
-                    cur.load_xyzw(g + q, xq, wq);
-                    SPos<R> sp;
-                    sp.x = kx == 0 ? xq[0] : add_rn(xq[0], kx > 0 ? Lx : -Lx);
-                    sp.y = ky == 0 ? xq[1] : add_rn(xq[1], ky > 0 ? Ly : -Ly);
-                    sp.z = kz == 0 ? xq[2] : add_rn(xq[2], kz > 0 ? Lz : -Lz);
-                    sp.w = wq;
-                    s_p[o + q] = sp;
+                    if constexpr (sizeof(R) == 4) {
+                        cp_async16(&s_p[o + q], cur.rec + 2 * (g + q));
+                    } else {
+                        cp_async16(&s_p[o + q], cur.st + g + q);
+                        cp_async16(reinterpret_cast<char*>(&s_p[o + q]) + 16,
+                                   reinterpret_cast<const char*>(cur.st + g + q) + 16);
+                    }
                 }
             }
         }
@@ -622,6 +691,27 @@ __global__ void __launch_bounds__(BLOCK) brick_step_kernel(StepArgs<R> a, const 
             const int h = ((iz + 1) * hy + (iy + 1)) * hx + (ix + 1);
             const int o = s_off[h], io = s_ioff[kin];
             for (int q = 0; q < c; ++q) s_ilist[io + q] = (o + q) | (h << 12);
+        }
+        if (staged) {
+            cp_async_wait_all();
+            // apply the periodic image shift of wrapped halo cells to the copies
+            // this thread issued (the FP64 record's w/id word comes along as is)
+            R Lx, Ly, Lz;
+            if constexpr (sizeof(R) == 4) { Lx = s.Lf[0]; Ly = s.Lf[1]; Lz = s.Lf[2]; }
+            else { Lx = s.L[0]; Ly = s.L[1]; Lz = s.L[2]; }
+            for (int h = tid; h < H; h += BLOCK) {
+                const int code = s_gc[h];
+                const int c = s_cnt[h];
+                if (c == 0 || (((unsigned)code >> 26) == 0x15u)) continue;   // 0x15: no shift on any axis
+                const int kx = ((code >> 26) & 3) - 1, ky = ((code >> 28) & 3) - 1, kz = ((code >> 30) & 3) - 1;
+                const int o = s_off[h];
+                for (int q = 0; q < c; ++q) {
+                    SPos<R>& sp = s_p[o + q];
+                    if (kx) sp.x = add_rn(sp.x, kx > 0 ? Lx : -Lx);
+                    if (ky) sp.y = add_rn(sp.y, ky > 0 ? Ly : -Ly);
+                    if (kz) sp.z = add_rn(sp.z, kz > 0 ? Lz : -Lz);
+                }
+            }
         }
         __syncthreads();
 
@@ -642,6 +732,13 @@ __global__ void __launch_bounds__(BLOCK) brick_step_kernel(StepArgs<R> a, const 
             }
             const int q = si - s_off[h];
             const long long self = s.slot_base + ((long long)(s_gc[h] & ((1 << 26) - 1)) << cap_log2) + q;
+            // the particle's compensation/id record, fetched before the pair loop
+            float4 crec = make_float4(0.f, 0.f, 0.f, 0.f);
+            int idpre = 0;
+            if (active && sub == 0) {
+                if constexpr (sizeof(R) == 4) crec = __ldg(cur.rec + 2 * self + 1);
+                else idpre = __ldg(&cur.st[self].id);
+            }
             if (active && staged) {
                 const SPos<R> sp = s_p[si];
                 xi0 = sp.x; xi1 = sp.y; xi2 = sp.z;
@@ -664,7 +761,7 @@ __global__ void __launch_bounds__(BLOCK) brick_step_kernel(StepArgs<R> a, const 
                 R F[3];
                 acc.force(F);
                 R xi[3] = {xi0, xi1, xi2};
-                finish_particle<R>(a, s, it.sys, self, xi, wi, F, t, cur, nxt, cnt_nxt);
+                finish_particle_pre<R>(a, s, it.sys, xi, wi, F, t, crec, idpre, nxt, cnt_nxt);
             }
         }
         __syncthreads();
