@@ -4,7 +4,8 @@
 // Replaces the reference's CudaSimulation host wrapper
 // (lib/ReaDDyGPU_Cpp/CudaKernels/CudaSimulation.cu:138-626, 2309-2476):
 // device state, cell binning, per-step launches.  One stream per handle; the
-// steps of rdgpu_step are replayed from a captured CUDA graph.
+// steps of rdgpu_step are replayed from a captured CUDA graph of
+// step_kernel -> scan_tiles -> scan_apply -> scatter per step.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -18,13 +19,11 @@
 using namespace rdgpu;
 
 namespace {
-
 thread_local std::string g_create_error;
-
-constexpr int kBlock = 256;        // warp-list kernel
-constexpr int kBrickBlock = 128;   // brick-staged kernel
-
+constexpr int kStepBlock = 128;
 }  // namespace
+
+std::string& rdgpu_global_error() { return g_create_error; }
 
 // the opaque handle type of the C ABI
 struct rdgpu_engine {
@@ -34,39 +33,40 @@ struct rdgpu_engine {
     rdgpu_system_desc desc{};
     rdgpu_options opt{};
     int nsys = 0;
+    bool value_image = false;            // some periodic axis has fewer than 3 cells
     std::vector<rdgpu_box> boxes;
     std::vector<SysDev> sys_h;
     SysDev* sys_d = nullptr;
-    std::vector<WorkItem> items_h;
-    WorkItem* items_d = nullptr;
-    std::vector<BrickItem> bricks_h;
-    BrickItem* bricks_d = nullptr;
-    int brick_grid = 0;
     void* tab_d = nullptr;
     void* ext_d = nullptr;
     int n_ext = 0;
-    // state
-    void* bufA[2] = {nullptr, nullptr};   // FP32: pos, FP64: records
-    void* bufB[2] = {nullptr, nullptr};   // FP32: cmp
-    int* cnt[3] = {nullptr, nullptr, nullptr};
-    int* work_ctr = nullptr;
-    int* err = nullptr;
-    long long* err_step = nullptr;
-    long long* step_d = nullptr;
-    int* scratch_i = nullptr;
-    long long ncells_tot = 0, nslots_tot = 0, npart_tot = 0;
+    // cells
+    long long ncells_tot = 0;
+    int ntiles = 0;
+    int* start = nullptr;                // ncells_tot + 1
+    int* counts = nullptr;               // ncells_tot
+    int* tile_sum = nullptr;             // ntiles
+    // particles
+    long long npart_tot = 0, cap_particles = 0;
     std::vector<long long> part_off;     // n_sys + 1
     std::vector<int> types_h;            // by global index
-    // dense scratch (by global particle index)
-    void* denseA = nullptr;
-    void* denseB = nullptr;
-    long long cap_particles = 0;         // capacity of the per-particle scratch
+    void* curA = nullptr;                // FP32: pos, FP64: records
+    void* curB = nullptr;                // FP32: aux
+    void* stgA = nullptr;
+    void* stgB = nullptr;
+    int* tcell = nullptr;
+    int* tslot = nullptr;
+    unsigned short* sys_of = nullptr;
     double* x0_d = nullptr;              // MSD origin, box-relative unwrapped
     double* vec_d = nullptr;             // 3N doubles scratch
     double* val_d = nullptr;             // N doubles scratch
     int* ityp_d = nullptr;               // N ints scratch
     unsigned long long* u64_d = nullptr; // N scratch
-    double* red_d = nullptr;             // reduction output
+    // control
+    int* err = nullptr;
+    long long* err_step = nullptr;
+    long long* step_d = nullptr;
+    double* red_d = nullptr;
     long long* redc_d = nullptr;
     int* pinned_err = nullptr;
     long long* pinned_step = nullptr;
@@ -81,8 +81,6 @@ struct rdgpu_engine {
     // CUDA graph of graph_steps steps
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 100;
-    int grid = 0;
-    int regrows = 0;
     long long launches = 0;
     std::string last_error;
 };
@@ -112,12 +110,7 @@ template <class T> void dfree(T*& p)
     p = nullptr;
 }
 
-int ceil_log2(int v)
-{
-    int l = 0;
-    while ((1 << l) < v) ++l;
-    return l;
-}
+
 
 // ---------------------------------------------------------------------------
 // parameter tables
@@ -237,163 +230,74 @@ template <class R> void build_ext(const rdgpu_system_desc& d, const rdgpu_box& b
 // ---------------------------------------------------------------------------
 // buffers
 // ---------------------------------------------------------------------------
-void free_state(Engine* E)
-{
-    for (int i = 0; i < 2; ++i) { dfree(E->bufA[i]); dfree(E->bufB[i]); }
-    for (int i = 0; i < 3; ++i) dfree(E->cnt[i]);
-    if (E->graph) { cudaGraphExecDestroy(E->graph); E->graph = nullptr; }
-}
 
+
+// ---------------------------------------------------------------------------
+// buffers
+// ---------------------------------------------------------------------------
 void free_particles(Engine* E)
 {
-    dfree(E->denseA); dfree(E->denseB); dfree(E->x0_d); dfree(E->vec_d); dfree(E->val_d);
-    dfree(E->ityp_d); dfree(E->u64_d);
+    dfree(E->curA); dfree(E->curB); dfree(E->stgA); dfree(E->stgB); dfree(E->tcell); dfree(E->tslot);
+    dfree(E->sys_of); dfree(E->x0_d); dfree(E->vec_d); dfree(E->val_d); dfree(E->ityp_d); dfree(E->u64_d);
     E->cap_particles = 0;
 }
 
-// bytes of one slot record (FP32C: pos + compensation; FP64: Rec64)
-size_t rec_bytes(int) { return 32; }
-
-// lay out cells/slots of all systems for the current caps and allocate
-int alloc_state(Engine* E)
+// grow-only per-particle buffers
+int ensure_particle_buffers(Engine* E, long long ntot)
 {
-    free_state(E);
-    long long cb = 0, sb = 0;
-    for (int s = 0; s < E->nsys; ++s) {
-        SysDev& d = E->sys_h[s];
-        d.cell_base = cb;
-        d.slot_base = sb;
-        cb += d.ncells;
-        sb += (long long)d.ncells << d.cap_log2;
+    const long long N = std::max<long long>(ntot, 1);
+    if (N <= E->cap_particles) return RDGPU_OK;
+    if (E->graph) { cudaGraphExecDestroy(E->graph); E->graph = nullptr; }
+    free_particles(E);
+    const long long M = N + N / 4;      // headroom for reactions adding particles
+    const size_t rec = E->prec == RDGPU_PREC_F32C ? 16 : 32;
+    CK(cudaMalloc(&E->curA, M * rec));
+    CK(cudaMalloc(&E->stgA, M * rec));
+    if (E->prec == RDGPU_PREC_F32C) {
+        CK(cudaMalloc(&E->curB, M * 16));
+        CK(cudaMalloc(&E->stgB, M * 16));
     }
-    E->ncells_tot = cb;
-    E->nslots_tot = sb;
-    const size_t rb = rec_bytes(E->prec);
-    for (int i = 0; i < 2; ++i) {
-        CK(cudaMalloc(&E->bufA[i], std::max<long long>(sb, 1) * rb));
-    }
-    for (int i = 0; i < 3; ++i) {
-        CK(cudaMalloc(&E->cnt[i], std::max<long long>(cb, 1) * sizeof(int)));
-        CK(cudaMemsetAsync(E->cnt[i], 0, std::max<long long>(cb, 1) * sizeof(int), E->stream));
-    }
-    CK(cudaMemcpyAsync(E->sys_d, E->sys_h.data(), E->nsys * sizeof(SysDev), cudaMemcpyHostToDevice, E->stream));
+    CK(cudaMalloc(&E->tcell, M * sizeof(int)));
+    CK(cudaMalloc(&E->tslot, M * sizeof(int)));
+    CK(cudaMalloc(&E->sys_of, M * sizeof(unsigned short)));
+    CK(cudaMalloc(&E->x0_d, M * 3 * sizeof(double)));
+    CK(cudaMalloc(&E->vec_d, M * 3 * sizeof(double)));
+    CK(cudaMalloc(&E->val_d, M * sizeof(double)));
+    CK(cudaMalloc(&E->ityp_d, M * sizeof(int)));
+    CK(cudaMalloc(&E->u64_d, M * sizeof(unsigned long long)));
+    E->cap_particles = M;
     return RDGPU_OK;
 }
 
-// work items: runs of 32*cpl cells of one system
-int build_items(Engine* E)
+template <class R> State<R> state(void* A, void* B)
 {
-    E->items_h.clear();
-    for (int s = 0; s < E->nsys; ++s) {
-        const SysDev& d = E->sys_h[s];
-        int cpl = E->opt.cells_per_lane;
-        if (cpl <= 0) {
-            double occ = d.ncells > 0 ? (double)d.npart / d.ncells : 0.0;
-            // about 96 particles per work item
-            cpl = occ > 0 ? (int)std::lround(96.0 / (32.0 * occ)) : CPL_MAX;
-        }
-        cpl = std::min(std::max(cpl, 1), CPL_MAX);
-        const int span = 32 * cpl;
-        for (int c0 = 0; c0 < d.ncells; c0 += span) {
-            WorkItem it;
-            it.sys = s;
-            it.c0 = c0;
-            it.c1 = std::min(d.ncells, c0 + span);
-            it.cpl = cpl;
-            E->items_h.push_back(it);
-        }
-    }
-    dfree(E->items_d);
-    CK(cudaMalloc(&E->items_d, std::max<size_t>(E->items_h.size(), 1) * sizeof(WorkItem)));
-    CK(cudaMemcpyAsync(E->items_d, E->items_h.data(), E->items_h.size() * sizeof(WorkItem),
-                       cudaMemcpyHostToDevice, E->stream));
-    return RDGPU_OK;
+    State<R> s;
+    if constexpr (sizeof(R) == 4) { s.pos = (float4*)A; s.aux = (float4*)B; }
+    else s.rec = (Rec64*)A;
+    return s;
 }
 
-// bricks: per system a tiling of the cell grid into ex*ey*ez bricks whose
-// one-cell halo fits the kernel's shared-memory stage
-int build_bricks(Engine* E)
+template <class R> Args<R> make_args(Engine* E)
 {
-    E->bricks_h.clear();
-    for (int s = 0; s < E->nsys; ++s) {
-        const SysDev& d = E->sys_h[s];
-        const double occ = d.ncells > 0 ? std::max(1e-3, (double)d.npart / d.ncells) : 1.0;
-        int e = E->opt.cells_per_lane;
-        if (e <= 0) {
-            // about 160 particles per brick, halo (e+2)^3 <= 512 cells
-            e = (int)std::lround(std::cbrt(160.0 / occ));
-        }
-        e = std::min(std::max(e, 1), 6);
-        int ext[3];
-        for (int a = 0; a < 3; ++a) ext[a] = std::min(e, d.n[a]);
-        // keep the expected staged particles well inside the stage
-        while ((ext[0] + 2) * (ext[1] + 2) * (ext[2] + 2) * occ > MAXP / 2 &&
-               (ext[0] > 1 || ext[1] > 1 || ext[2] > 1)) {
-            int a = (ext[0] >= ext[1] && ext[0] >= ext[2]) ? 0 : (ext[1] >= ext[2] ? 1 : 2);
-            ext[a]--;
-        }
-        const int lg = d.lanes_log2;
-        for (int z0 = 0; z0 < d.n[2]; z0 += ext[2])
-            for (int y0 = 0; y0 < d.n[1]; y0 += ext[1])
-                for (int x0 = 0; x0 < d.n[0]; x0 += ext[0]) {
-                    BrickItem b;
-                    const int ex = std::min(ext[0], d.n[0] - x0), ey = std::min(ext[1], d.n[1] - y0),
-                              ez = std::min(ext[2], d.n[2] - z0);
-                    b.sys = s;
-                    b.xy = x0 | (y0 << 16);
-                    b.z = z0;
-                    b.ext = ex | (ey << 8) | (ez << 16) | (lg << 24);
-                    E->bricks_h.push_back(b);
-                }
-    }
-    dfree(E->bricks_d);
-    CK(cudaMalloc(&E->bricks_d, std::max<size_t>(E->bricks_h.size(), 1) * sizeof(BrickItem)));
-    CK(cudaMemcpyAsync(E->bricks_d, E->bricks_h.data(), E->bricks_h.size() * sizeof(BrickItem),
-                       cudaMemcpyHostToDevice, E->stream));
-    return RDGPU_OK;
-}
-
-template <class R> StepArgs<R> make_args(Engine* E)
-{
-    StepArgs<R> a;
+    Args<R> a;
     memset(&a, 0, sizeof(a));
     a.sys = E->sys_d;
-    a.items = E->items_d;
-    a.nitems = (int)E->items_h.size();
+    a.sys_of = E->sys_of;
+    a.ntot = E->npart_tot;
+    a.nsys = E->nsys;
     a.n_ext = E->n_ext;
     a.tab = (const TypeTab<R>*)E->tab_d;
     a.ext = (const ExtTerm<R>*)E->ext_d;
-    for (int i = 0; i < 2; ++i) {
-        if constexpr (sizeof(R) == 4) {
-            a.buf[i].rec = (float4*)E->bufA[i];
-        } else {
-            a.buf[i].st = (Rec64*)E->bufA[i];
-        }
-    }
-    for (int i = 0; i < 3; ++i) a.cnt[i] = E->cnt[i];
-    a.work_ctr = E->work_ctr;
+    a.cur = state<R>(E->curA, E->curB);
+    a.stg = state<R>(E->stgA, E->stgB);
+    a.start = E->start;
+    a.counts = E->counts;
+    a.tcell = E->tcell;
+    a.tslot = E->tslot;
     a.err = E->err;
     a.err_step = E->err_step;
     a.step_ptr = E->step_d;
-    a.step_off = 0;
-    a.noise = nullptr;
     return a;
-}
-
-template <class R> StateBuf<R> sbuf(Engine* E, int i)
-{
-    StateBuf<R> b;
-    if constexpr (sizeof(R) == 4) b.rec = (float4*)E->bufA[i];
-    else b.st = (Rec64*)E->bufA[i];
-    return b;
-}
-
-template <class R> Dense<R> dense(Engine* E)
-{
-    Dense<R> d;
-    if constexpr (sizeof(R) == 4) { d.pos = (float4*)E->denseA; d.cmp = (float4*)E->denseB; }
-    else d.st = (Rec64*)E->denseA;
-    return d;
 }
 
 int grid_for(long long n, int block = 256)
@@ -404,49 +308,21 @@ int grid_for(long long n, int block = 256)
     return (int)g;
 }
 
-// bin the dense arrays into buffer `bi` with counts `ci`; grows caps on overflow
-template <class R> int bin_dense(Engine* E, int bi, int ci)
+// scan + scatter of the staging arrays (tcell/tslot/counts filled)
+template <class R> void launch_sort(Engine* E)
 {
-    for (int attempt = 0; attempt < 8; ++attempt) {
-        CK(cudaMemsetAsync(E->cnt[ci], 0, std::max<long long>(E->ncells_tot, 1) * sizeof(int), E->stream));
-        CK(cudaMemsetAsync(E->err, 0, sizeof(int), E->stream));
-        if (E->npart_tot > 0) {
-            bin_kernel<R><<<grid_for(E->npart_tot), 256, 0, E->stream>>>(
-                E->sys_d, E->nsys, E->npart_tot, dense<R>(E), sbuf<R>(E, bi), E->cnt[ci], E->err);
-            CK(cudaGetLastError());
-        }
-        CK(cudaMemcpyAsync(E->pinned_err, E->err, sizeof(int), cudaMemcpyDeviceToHost, E->stream));
-        CK(cudaStreamSynchronize(E->stream));
-        if (*E->pinned_err == 0) return RDGPU_OK;
-        // occupancy per system from the complete counts, then re-layout
-        std::vector<int> counts(E->ncells_tot);
-        CK(cudaMemcpy(counts.data(), E->cnt[ci], E->ncells_tot * sizeof(int), cudaMemcpyDeviceToHost));
-        for (int s = 0; s < E->nsys; ++s) {
-            SysDev& d = E->sys_h[s];
-            int m = 0;
-            for (int c = 0; c < d.ncells; ++c) m = std::max(m, counts[d.cell_base + c]);
-            int want = ceil_log2(std::max(8, 2 * m));
-            if (want > d.cap_log2) d.cap_log2 = want;
-        }
-        int rc = alloc_state(E);
-        if (rc) return rc;
-        ++E->regrows;
-    }
-    return fail(E, RDGPU_ERR_OVERFLOW, "cell occupancy cap could not be grown");
-}
-
-template <class R> int gather_dense(Engine* E, int bi, int ci)
-{
-    if (E->npart_tot == 0) return RDGPU_OK;
-    gather_kernel<R><<<grid_for(E->ncells_tot), 256, 0, E->stream>>>(E->sys_d, E->nsys, E->ncells_tot,
-                                                                       sbuf<R>(E, bi), E->cnt[ci], dense<R>(E));
-    CK(cudaGetLastError());
-    return RDGPU_OK;
+    scan_tiles_kernel<<<E->ntiles, SCAN_BLOCK, 0, E->stream>>>(E->counts, E->ncells_tot, E->tile_sum, E->err);
+    scan_apply_kernel<<<E->ntiles, SCAN_BLOCK, 0, E->stream>>>(E->counts, E->ncells_tot, E->tile_sum, E->ntiles,
+                                                               E->start, E->err);
+    if (E->npart_tot > 0)
+        scatter_kernel<R><<<grid_for(E->npart_tot), 256, 0, E->stream>>>(
+            state<R>(E->stgA, E->stgB), state<R>(E->curA, E->curB), E->tcell, E->tslot, E->start, E->npart_tot,
+            E->err);
+    E->launches += (E->npart_tot > 0) ? 3 : 2;
 }
 
 int reset_counters(Engine* E, long long t)
 {
-    CK(cudaMemsetAsync(E->work_ctr, 0, 3 * sizeof(int), E->stream));
     CK(cudaMemsetAsync(E->err, 0, sizeof(int), E->stream));
     const long long big = 0x7fffffffffffffffLL;
     CK(cudaMemcpyAsync(E->err_step, &big, sizeof(long long), cudaMemcpyHostToDevice, E->stream));
@@ -456,27 +332,26 @@ int reset_counters(Engine* E, long long t)
     return RDGPU_OK;
 }
 
-// the state of step t sits in buffer t&1 with counts t%3; counts (t+1)%3 must
-// be zero before step t runs
+// the sorted state of step t is in cur/start; the counts must be zero
 int prepare_step_state(Engine* E, long long t)
 {
-    const int nxt = (int)((t + 1) % 3);
-    CK(cudaMemsetAsync(E->cnt[nxt], 0, std::max<long long>(E->ncells_tot, 1) * sizeof(int), E->stream));
+    CK(cudaMemsetAsync(E->counts, 0, std::max<long long>(E->ncells_tot, 1) * sizeof(int), E->stream));
     return reset_counters(E, t);
 }
 
 template <class R> int launch_steps(Engine* E, int n, const double* noise_d)
 {
-    StepArgs<R> a = make_args<R>(E);
+    Args<R> a = make_args<R>(E);
     a.noise = noise_d;
+    const int grid = (int)((E->npart_tot + kStepBlock - 1) / kStepBlock);
     for (int k = 0; k < n; ++k) {
         a.step_off = k;
-        if (E->opt.kernel_variant == 1)
-            step_kernel<R, kBlock><<<E->grid, kBlock, 0, E->stream>>>(a);
+        if (E->value_image)
+            step_kernel<R, true, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a);
         else
-            brick_step_kernel<R, kBrickBlock><<<E->brick_grid, kBrickBlock, 0, E->stream>>>(
-                a, E->bricks_d, (int)E->bricks_h.size());
+            step_kernel<R, false, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a);
         ++E->launches;
+        launch_sort<R>(E);
     }
     advance_kernel<<<1, 32, 0, E->stream>>>(E->step_d, E->err, n);
     ++E->launches;
@@ -500,75 +375,42 @@ template <class R> int capture_graph(Engine* E)
     return RDGPU_OK;
 }
 
-// after an overflow at step tf: regrow the caps of the next layout and resume
-template <class R> int recover_overflow(Engine* E, long long tf)
-{
-    const int bi = (int)(tf & 1), ci = (int)(tf % 3), nci = (int)((tf + 1) % 3);
-    // the claimed counts of the failed next layout are complete: size from them
-    std::vector<int> counts(E->ncells_tot);
-    CK(cudaMemcpy(counts.data(), E->cnt[nci], E->ncells_tot * sizeof(int), cudaMemcpyDeviceToHost));
-    int rc = gather_dense<R>(E, bi, ci);
-    if (rc) return rc;
-    CK(cudaStreamSynchronize(E->stream));
-    for (int s = 0; s < E->nsys; ++s) {
-        SysDev& d = E->sys_h[s];
-        int m = 0;
-        for (int c = 0; c < d.ncells; ++c) m = std::max(m, counts[d.cell_base + c]);
-        int want = ceil_log2(std::max(8, 2 * m));
-        if (want > d.cap_log2) d.cap_log2 = want;
-    }
-    rc = alloc_state(E);
-    if (rc) return rc;
-    rc = bin_dense<R>(E, bi, ci);
-    if (rc) return rc;
-    ++E->regrows;
-    return prepare_step_state(E, tf);
-}
-
 template <class R> int do_steps(Engine* E, long long nsteps, const double* noise_d)
 {
     const long long target = E->step_h + nsteps;
-    for (int round = 0; round < 16; ++round) {
-        long long remaining = target - E->step_h;
-        if (remaining <= 0) return RDGPU_OK;
-        int rc;
-        if (E->graph_steps > 0 && !noise_d && remaining >= E->graph_steps) {
-            rc = capture_graph<R>(E);
-            if (rc) return rc;
-            long long ng = remaining / E->graph_steps;
-            for (long long g = 0; g < ng; ++g) {
-                CK(cudaGraphLaunch(E->graph, E->stream));
-                E->launches += E->graph_steps + 1;
-            }
-            remaining -= ng * E->graph_steps;
-        }
-        while (remaining > 0) {
-            int n = (int)std::min<long long>(remaining, 1000);
-            rc = launch_steps<R>(E, n, noise_d);
-            if (rc) return rc;
-            remaining -= n;
-        }
-        CK(cudaMemcpyAsync(E->pinned_err, E->err, sizeof(int), cudaMemcpyDeviceToHost, E->stream));
-        CK(cudaMemcpyAsync(E->pinned_step, E->err_step, sizeof(long long), cudaMemcpyDeviceToHost, E->stream));
-        CK(cudaStreamSynchronize(E->stream));
-        const int ef = *E->pinned_err;
-        if (ef == 0) {
-            E->step_h = target;
-            return RDGPU_OK;
-        }
-        const long long tf = *E->pinned_step;
-        if (ef & EF_NONFINITE) {
-            prepare_step_state(E, tf);
-            return fail(E, RDGPU_ERR_NONFINITE, "a particle position became non-finite at step " + std::to_string(tf));
-        }
-        if (ef & EF_JUMP) {
-            prepare_step_state(E, tf);
-            return fail(E, RDGPU_ERR_JUMP, "a particle moved more than a box length at step " + std::to_string(tf));
-        }
-        rc = recover_overflow<R>(E, tf);
+    long long remaining = nsteps;
+    if (E->graph_steps > 0 && !noise_d && remaining >= E->graph_steps) {
+        int rc = capture_graph<R>(E);
         if (rc) return rc;
+        const long long ng = remaining / E->graph_steps;
+        const long long per_graph = (long long)E->graph_steps * ((E->npart_tot > 0) ? 4 : 3) + 1;
+        for (long long g = 0; g < ng; ++g) {
+            CK(cudaGraphLaunch(E->graph, E->stream));
+            E->launches += per_graph;
+        }
+        remaining -= ng * E->graph_steps;
     }
-    return fail(E, RDGPU_ERR_OVERFLOW, "repeated cell overflow");
+    while (remaining > 0) {
+        const int n = (int)std::min<long long>(remaining, 1000);
+        int rc = launch_steps<R>(E, n, noise_d);
+        if (rc) return rc;
+        remaining -= n;
+    }
+    CK(cudaMemcpyAsync(E->pinned_err, E->err, sizeof(int), cudaMemcpyDeviceToHost, E->stream));
+    CK(cudaMemcpyAsync(E->pinned_step, E->err_step, sizeof(long long), cudaMemcpyDeviceToHost, E->stream));
+    CK(cudaStreamSynchronize(E->stream));
+    const int ef = *E->pinned_err;
+    if (ef == 0) {
+        E->step_h = target;
+        return RDGPU_OK;
+    }
+    // the failing step's input is the current sorted state (its sort was skipped)
+    const long long tf = *E->pinned_step;
+    int rc = prepare_step_state(E, tf);
+    if (rc) return rc;
+    if (ef & EF_NONFINITE)
+        return fail(E, RDGPU_ERR_NONFINITE, "a particle position became non-finite at step " + std::to_string(tf));
+    return fail(E, RDGPU_ERR_JUMP, "a particle moved more than a box length at step " + std::to_string(tf));
 }
 
 int setup_systems(Engine* E, std::string& why)
@@ -623,7 +465,7 @@ int setup_systems(Engine* E, std::string& why)
         }
         if (nc > (1LL << 26)) { why = "too many cells in one system (box / cutoff too large)"; return -1; }
         v.ncells = (int)nc;
-        v.cap_log2 = E->opt.cell_cap > 0 ? ceil_log2(E->opt.cell_cap) : 3;
+        v.cap_log2 = 0;
         v.seed = b.seed;
         v.lanes_log2 = 0;
     }
@@ -640,24 +482,6 @@ int setup_systems(Engine* E, std::string& why)
     if (cudaMalloc(&E->ext_d, esz) != cudaSuccess) { why = "cudaMalloc failed"; return -2; }
     cudaMemcpy(E->ext_d, ebuf.data(), esz, cudaMemcpyHostToDevice);
     return 0;
-}
-
-// grow-only device scratch sized by the particle count
-int ensure_particle_buffers(Engine* E, long long ntot)
-{
-    const long long N = std::max<long long>(ntot, 1);
-    if (N <= E->cap_particles) return RDGPU_OK;
-    free_particles(E);
-    const long long M = N + N / 4;      // headroom for reactions adding particles
-    CK(cudaMalloc(&E->denseA, M * (E->prec == RDGPU_PREC_F32C ? 16 : 32)));
-    if (E->prec == RDGPU_PREC_F32C) CK(cudaMalloc(&E->denseB, M * 16));
-    CK(cudaMalloc(&E->x0_d, M * 3 * sizeof(double)));
-    CK(cudaMalloc(&E->vec_d, M * 3 * sizeof(double)));
-    CK(cudaMalloc(&E->val_d, M * sizeof(double)));
-    CK(cudaMalloc(&E->ityp_d, M * sizeof(int)));
-    CK(cudaMalloc(&E->u64_d, M * sizeof(unsigned long long)));
-    E->cap_particles = M;
-    return RDGPU_OK;
 }
 
 template <class R> int set_particles_impl(Engine* E, const long long* offsets, long long ntot,
@@ -677,26 +501,27 @@ template <class R> int set_particles_impl(Engine* E, const long long* offsets, l
         long long n = off[s + 1] - off[s];
         if (n < 0 || n > 0x7fffffff) return fail(E, RDGPU_ERR_ARG, "invalid particle count");
     }
+    if (ntot > 0x7fffffff) return fail(E, RDGPU_ERR_ARG, "at most 2^31-1 particles per handle");
     E->part_off.clear();   // no valid state until this call completes
-    bool sizes_changed = false;
-    for (int s = 0; s < E->nsys; ++s) {
-        const int n = (int)(off[s + 1] - off[s]);
-        const int old = E->sys_h[s].npart;
-        if (E->bricks_h.empty() || n > old + old / 4 + 8 || n < old - old / 4 - 8) sizes_changed = true;
-        E->sys_h[s].part_base = off[s];
-        E->sys_h[s].npart = n;
-    }
     int rc = ensure_particle_buffers(E, ntot);
     if (rc) return rc;
+    std::vector<unsigned short> so(std::max<long long>(ntot, 1));
+    for (int s = 0; s < E->nsys; ++s) {
+        E->sys_h[s].part_base = off[s];
+        E->sys_h[s].npart = (int)(off[s + 1] - off[s]);
+        for (long long g = off[s]; g < off[s + 1]; ++g) so[g] = (unsigned short)s;
+    }
     E->npart_tot = ntot;
     CK(cudaMemcpyAsync(E->sys_d, E->sys_h.data(), E->nsys * sizeof(SysDev), cudaMemcpyHostToDevice, E->stream));
     CK(cudaMemsetAsync(E->err, 0, sizeof(int), E->stream));
+    CK(cudaMemsetAsync(E->counts, 0, std::max<long long>(E->ncells_tot, 1) * sizeof(int), E->stream));
     if (ntot > 0) {
-        // inputs: coordinates into the 3N scratch, types into the N scratch
+        CK(cudaMemcpyAsync(E->sys_of, so.data(), ntot * sizeof(unsigned short), cudaMemcpyHostToDevice, E->stream));
         CK(cudaMemcpyAsync(E->vec_d, xyz, ntot * 3 * sizeof(double), cudaMemcpyHostToDevice, E->stream));
         CK(cudaMemcpyAsync(E->ityp_d, types, ntot * sizeof(int), cudaMemcpyHostToDevice, E->stream));
-        ingest_kernel<R><<<grid_for(ntot), 256, 0, E->stream>>>(E->sys_d, E->nsys, ntot, E->vec_d, E->ityp_d,
-                                                                E->desc.n_types, dense<R>(E), E->x0_d, E->err);
+        ingest_kernel<R><<<grid_for(ntot), 256, 0, E->stream>>>(E->sys_d, E->sys_of, ntot, E->vec_d, E->ityp_d,
+                                                                E->desc.n_types, state<R>(E->stgA, E->stgB),
+                                                                E->tcell, E->tslot, E->counts, E->x0_d, E->err);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(E->pinned_err, E->err, sizeof(int), cudaMemcpyDeviceToHost, E->stream));
         CK(cudaStreamSynchronize(E->stream));
@@ -705,25 +530,8 @@ template <class R> int set_particles_impl(Engine* E, const long long* offsets, l
                                           "more than 64 box lengths outside the box");
     }
     E->types_h.assign(types, types + ntot);
-    // lay out (once, or after the caps grew) and bin
-    if (!E->bufA[0]) {
-        rc = alloc_state(E);
-        if (rc) return rc;
-    }
-    rc = bin_dense<R>(E, 0, 0);
-    if (rc) return rc;
-    for (int s = 0; s < E->nsys; ++s) {
-        int L = E->opt.lanes_per_particle;
-        if (L <= 0) L = 1;
-        E->sys_h[s].lanes_log2 = ceil_log2(std::min(std::max(L, 1), 8));
-    }
-    CK(cudaMemcpyAsync(E->sys_d, E->sys_h.data(), E->nsys * sizeof(SysDev), cudaMemcpyHostToDevice, E->stream));
-    if (sizes_changed || E->items_h.empty()) {
-        rc = build_items(E);
-        if (rc) return rc;
-        rc = build_bricks(E);
-        if (rc) return rc;
-    }
+    launch_sort<R>(E);
+    CK(cudaGetLastError());
     E->rdf_frames = 0;
     if (E->rdf_acc && E->rdf_nbins > 0) {
         const int S = E->desc.n_types;
@@ -737,12 +545,10 @@ template <class R> int set_particles_impl(Engine* E, const long long* offsets, l
 
 template <class R> int get_particles_impl(Engine* E, double* xyz, int* types)
 {
-    const long long t = E->step_h;
-    int rc = gather_dense<R>(E, (int)(t & 1), (int)(t % 3));
-    if (rc) return rc;
     const long long N = E->npart_tot;
     if (N == 0) return RDGPU_OK;
-    emit_kernel<R><<<grid_for(N), 256, 0, E->stream>>>(E->sys_d, E->nsys, N, dense<R>(E), E->vec_d, E->ityp_d);
+    emit_kernel<R><<<grid_for(N), 256, 0, E->stream>>>(E->sys_d, E->sys_of, N, state<R>(E->curA, E->curB), E->vec_d,
+                                                       E->ityp_d);
     CK(cudaGetLastError());
     if (xyz) CK(cudaMemcpyAsync(xyz, E->vec_d, N * 3 * sizeof(double), cudaMemcpyDeviceToHost, E->stream));
     if (types) CK(cudaMemcpyAsync(types, E->ityp_d, N * sizeof(int), cudaMemcpyDeviceToHost, E->stream));
@@ -750,16 +556,21 @@ template <class R> int get_particles_impl(Engine* E, double* xyz, int* types)
     return RDGPU_OK;
 }
 
+template <class R, int MODE> void launch_diag(Engine* E, double* f, double* e, int* c, unsigned long long* h)
+{
+    Args<R> a = make_args<R>(E);
+    if (E->value_image)
+        diag_kernel<R, MODE, true><<<grid_for(E->npart_tot), 256, 0, E->stream>>>(a, f, e, c, h);
+    else
+        diag_kernel<R, MODE, false><<<grid_for(E->npart_tot), 256, 0, E->stream>>>(a, f, e, c, h);
+}
+
 template <class R> int forces_impl(Engine* E, double* forces, double* energy)
 {
-    const long long t = E->step_h;
-    StepArgs<R> a = make_args<R>(E);
-    diag_kernel<R, 1><<<grid_for(E->ncells_tot), 256, 0, E->stream>>>(
-        a, E->nsys, E->ncells_tot, (int)(t & 1), (int)(t % 3), E->vec_d, E->val_d, nullptr, nullptr);
+    launch_diag<R, 1>(E, E->vec_d, E->val_d, nullptr, nullptr);
     CK(cudaGetLastError());
     if (forces) CK(cudaMemcpyAsync(forces, E->vec_d, E->npart_tot * 3 * sizeof(double), cudaMemcpyDeviceToHost, E->stream));
     if (energy) {
-        CK(cudaMemsetAsync(E->ityp_d, 0, std::max<long long>(E->npart_tot, 1) * sizeof(int), E->stream));
         typed_sum_kernel<<<1, 256, 256 * 16, E->stream>>>(E->val_d, E->ityp_d, E->npart_tot, 0, E->red_d, E->redc_d);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(energy, E->red_d, sizeof(double), cudaMemcpyDeviceToHost, E->stream));
@@ -770,10 +581,7 @@ template <class R> int forces_impl(Engine* E, double* forces, double* energy)
 
 template <class R> int digest_impl(Engine* E, int* counts, unsigned long long* hashes)
 {
-    const long long t = E->step_h;
-    StepArgs<R> a = make_args<R>(E);
-    diag_kernel<R, 2><<<grid_for(E->ncells_tot), 256, 0, E->stream>>>(
-        a, E->nsys, E->ncells_tot, (int)(t & 1), (int)(t % 3), nullptr, nullptr, E->ityp_d, E->u64_d);
+    launch_diag<R, 2>(E, nullptr, nullptr, E->ityp_d, E->u64_d);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(counts, E->ityp_d, E->npart_tot * sizeof(int), cudaMemcpyDeviceToHost, E->stream));
     CK(cudaMemcpyAsync(hashes, E->u64_d, E->npart_tot * sizeof(unsigned long long), cudaMemcpyDeviceToHost, E->stream));
@@ -822,12 +630,13 @@ template <class R> int rdf_impl(Engine* E, int nbins, double rmax, int accumulat
         E->rdf_frames = 0;
     }
     CK(cudaMemsetAsync(E->rdf_tmp, 0, H * sizeof(unsigned long long), E->stream));
-    const long long t = E->step_h;
     const int use_smem = (H * 4 <= 48 * 1024) ? 1 : 0;
-    rdf_kernel<R><<<grid_for(E->ncells_tot, 128), 128, use_smem ? H * 4 : 0, E->stream>>>(
-        E->sys_d, E->nsys, E->ncells_tot, sbuf<R>(E, (int)(t & 1)), E->cnt[t % 3], S, nbins, E->rdf_e2,
-        rmax / (double)nbins, use_smem, E->rdf_tmp);
-    CK(cudaGetLastError());
+    if (E->npart_tot > 0) {
+        rdf_kernel<R><<<grid_for(E->npart_tot, 128), 128, use_smem ? H * 4 : 0, E->stream>>>(
+            E->sys_d, E->sys_of, E->npart_tot, state<R>(E->curA, E->curB), E->start, S, nbins, E->rdf_e2,
+            rmax / (double)nbins, use_smem, E->rdf_tmp);
+        CK(cudaGetLastError());
+    }
     if (accumulate) {
         add_u64_kernel<<<(H + 255) / 256, 256, 0, E->stream>>>(E->rdf_acc, E->rdf_tmp, H);
         CK(cudaGetLastError());
@@ -843,11 +652,10 @@ template <class R> int rdf_impl(Engine* E, int nbins, double rmax, int accumulat
 
 template <class R> int msd_impl(Engine* E, rdgpu_metrics* m)
 {
-    const long long t = E->step_h;
     const int S = E->desc.n_types;
-    msd_kernel<R><<<grid_for(E->ncells_tot), 256, 0, E->stream>>>(E->sys_d, E->nsys, E->ncells_tot,
-                                                                    sbuf<R>(E, (int)(t & 1)), E->cnt[t % 3],
-                                                                    E->x0_d, E->val_d, E->ityp_d);
+    msd_kernel<R><<<grid_for(E->npart_tot), 256, 0, E->stream>>>(E->sys_d, E->sys_of, E->npart_tot,
+                                                                   state<R>(E->curA, E->curB), E->x0_d, E->val_d,
+                                                                   E->ityp_d);
     CK(cudaGetLastError());
     typed_sum_kernel<<<S, 256, 256 * 16, E->stream>>>(E->val_d, E->ityp_d, E->npart_tot, S, E->red_d, E->redc_d);
     CK(cudaGetLastError());
@@ -868,6 +676,10 @@ int create_impl(const rdgpu_system_desc* desc, int nsys, const rdgpu_box* boxes,
 {
     if (!desc || !out || nsys < 1 || (nsys > 1 && !boxes)) {
         g_create_error = "null argument or no systems";
+        return RDGPU_ERR_ARG;
+    }
+    if (nsys > 65535) {
+        g_create_error = "at most 65535 systems per batch";
         return RDGPU_ERR_ARG;
     }
     std::string why;
@@ -917,11 +729,9 @@ int create_impl(const rdgpu_system_desc* desc, int nsys, const rdgpu_box* boxes,
     if (cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(RDGPU_ERR_CUDA, "cudaStreamCreate failed");
     if (cudaMalloc(&E->sys_d, nsys * sizeof(SysDev)) != cudaSuccess ||
-        cudaMalloc(&E->work_ctr, 3 * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&E->err, sizeof(int)) != cudaSuccess ||
         cudaMalloc(&E->err_step, sizeof(long long)) != cudaSuccess ||
         cudaMalloc(&E->step_d, sizeof(long long)) != cudaSuccess ||
-        cudaMalloc(&E->scratch_i, sizeof(int)) != cudaSuccess ||
         cudaMalloc(&E->red_d, (RDGPU_MAX_TYPES + 1) * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&E->redc_d, (RDGPU_MAX_TYPES + 1) * sizeof(long long)) != cudaSuccess ||
         cudaMallocHost(&E->pinned_err, sizeof(int)) != cudaSuccess ||
@@ -929,28 +739,33 @@ int create_impl(const rdgpu_system_desc* desc, int nsys, const rdgpu_box* boxes,
         return bail(RDGPU_ERR_NOMEM, "device allocation failed");
     int rc = setup_systems(E, why);
     if (rc) return bail(rc == -2 ? RDGPU_ERR_NOMEM : RDGPU_ERR_ARG, why);
-    int sms = 148, occ = 1;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, E->device);
-    if (E->prec == RDGPU_PREC_F32C)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, step_kernel<float, kBlock>, kBlock, 0);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, step_kernel<double, kBlock>, kBlock, 0);
-    E->grid = sms * std::max(occ, 1);
-    int bocc = 1;
-    if (E->prec == RDGPU_PREC_F32C)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bocc, brick_step_kernel<float, kBrickBlock>, kBrickBlock, 0);
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bocc, brick_step_kernel<double, kBrickBlock>, kBrickBlock, 0);
-    E->brick_grid = sms * std::max(bocc, 1);
+    // cells of all systems
+    long long cb = 0;
+    for (int s = 0; s < nsys; ++s) {
+        SysDev& d = E->sys_h[s];
+        d.cell_base = cb;
+        d.slot_base = 0;
+        cb += d.ncells;
+        for (int a = 0; a < 3; ++a)
+            if (d.per[a] && d.n[a] < 3) E->value_image = true;
+    }
+    if (cb >= 0x7fffffffLL) return bail(RDGPU_ERR_ARG, "too many cells in the batch");
+    E->ncells_tot = cb;
+    E->ntiles = (int)((cb + SCAN_TILE - 1) / SCAN_TILE);
+    if (cudaMalloc(&E->start, (cb + 1) * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&E->counts, std::max<long long>(cb, 1) * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&E->tile_sum, std::max(E->ntiles, 1) * sizeof(int)) != cudaSuccess)
+        return bail(RDGPU_ERR_NOMEM, "device allocation failed");
+    cudaMemsetAsync(E->start, 0, (cb + 1) * sizeof(int), E->stream);
+    cudaMemsetAsync(E->counts, 0, std::max<long long>(cb, 1) * sizeof(int), E->stream);
+    cudaMemcpyAsync(E->sys_d, E->sys_h.data(), nsys * sizeof(SysDev), cudaMemcpyHostToDevice, E->stream);
+    if (cudaStreamSynchronize(E->stream) != cudaSuccess) return bail(RDGPU_ERR_CUDA, "initialisation failed");
     *out = E;
     return RDGPU_OK;
 }
 
 }  // namespace
 
-// ===========================================================================
-// C ABI
-// ===========================================================================
 extern "C" {
 
 int rdgpu_create(const rdgpu_system_desc* desc, const rdgpu_options* opt, rdgpu_handle* out)
@@ -970,10 +785,10 @@ int rdgpu_destroy(rdgpu_handle h)
     if (!E) return RDGPU_ERR_ARG;
     cudaSetDevice(E->device);
     if (E->stream) cudaStreamSynchronize(E->stream);
-    free_state(E);
+    if (E->graph) cudaGraphExecDestroy(E->graph);
     free_particles(E);
-    dfree(E->sys_d); dfree(E->items_d); dfree(E->bricks_d); dfree(E->tab_d); dfree(E->ext_d);
-    dfree(E->work_ctr); dfree(E->err); dfree(E->err_step); dfree(E->step_d); dfree(E->scratch_i);
+    dfree(E->sys_d); dfree(E->tab_d); dfree(E->ext_d); dfree(E->start); dfree(E->counts); dfree(E->tile_sum);
+    dfree(E->err); dfree(E->err_step); dfree(E->step_d);
     dfree(E->red_d); dfree(E->redc_d); dfree(E->rdf_acc); dfree(E->rdf_tmp); dfree(E->rdf_e2);
     if (E->pinned_err) cudaFreeHost(E->pinned_err);
     if (E->pinned_step) cudaFreeHost(E->pinned_step);
@@ -1083,9 +898,9 @@ int rdgpu_debug_noise(rdgpu_handle h, int64_t step, double* noise)
     if (!noise) return fail(E, RDGPU_ERR_ARG, "null output");
     if (E->npart_tot == 0) return RDGPU_OK;
     if (E->prec == RDGPU_PREC_F32C)
-        noise_kernel<float><<<grid_for(E->npart_tot), 256, 0, E->stream>>>(E->sys_d, E->nsys, E->npart_tot, step, E->vec_d);
+        noise_kernel<float><<<grid_for(E->npart_tot), 256, 0, E->stream>>>(E->sys_d, E->sys_of, E->npart_tot, step, E->vec_d);
     else
-        noise_kernel<double><<<grid_for(E->npart_tot), 256, 0, E->stream>>>(E->sys_d, E->nsys, E->npart_tot, step, E->vec_d);
+        noise_kernel<double><<<grid_for(E->npart_tot), 256, 0, E->stream>>>(E->sys_d, E->sys_of, E->npart_tot, step, E->vec_d);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(noise, E->vec_d, E->npart_tot * 3 * sizeof(double), cudaMemcpyDeviceToHost, E->stream));
     CK(cudaStreamSynchronize(E->stream));
@@ -1137,8 +952,8 @@ int rdgpu_metrics_get(rdgpu_handle h, rdgpu_metrics* m)
     if (!m) return fail(E, RDGPU_ERR_ARG, "null output");
     memset(m, 0, sizeof(*m));
     m->step = E->step_h;
-    m->cell_cap = 1 << E->sys_h[0].cap_log2;
-    m->overflow_regrows = E->regrows;
+    m->cell_cap = 0;
+    m->overflow_regrows = 0;
     if (E->npart_tot == 0) return RDGPU_OK;
     int rc = rdgpu_forces(h, nullptr, &m->energy);
     if (rc) return rc;

@@ -266,26 +266,26 @@ def test_batch_matches_single_systems(prec):
             assert np.abs(xb[a:b] - xs).max() < 1e-9
 
 
-def test_cell_overflow_regrow_is_exact():
-    """A cap of 2 slots per cell overflows during the run; the engine regrows
-    the cap and redoes the failed step.  FP32 results are bit-identical to a
-    run that never overflowed."""
-    L = 48.0
-    sys_ = System([ParticleType("A", 5e8, 1.0)], pair=[PairPotential(A.P2_HARMONIC, [(0, 0)], 10.0, "repulsive")],
-                  kT=2.437, dt=1e-9, lo=(0, 0, 0), hi=(L, L, L), periodic=(1, 1, 1), cell_size=3.9)
-    g = (np.arange(12) + 0.5) * 4.0       # one particle per 4 nm cell
-    xyz = np.array(np.meshgrid(g, g, g, indexing="ij")).reshape(3, -1).T[:1200]
+@pytest.mark.parametrize("prec", PRECS)
+def test_dense_cluster(oracle, prec):
+    """Hundreds of particles in a few cells (the sorted cell layout has no
+    per-cell capacity): neighbour sets stay bit-exact and forces match."""
+    rng = np.random.default_rng(21)
+    sys_ = System([ParticleType("A", 1e6, 1.0)], pair=[PairPotential(A.P2_HARMONIC, [(0, 0)], 10.0, "repulsive")],
+                  kT=2.437, dt=1e-9, lo=(0, 0, 0), hi=(40, 40, 40), periodic=(1, 1, 1))
+    xyz = np.concatenate([rng.uniform(0, 40, (300, 3)), 20.0 + rng.uniform(-1.5, 1.5, (400, 3))])
     types = np.zeros(len(xyz), np.int32)
-    res = []
-    for cap in (2, 32):
-        with Engine(sys_, precision="f32c", seed=1, cell_cap=cap) as e:
-            e.set_particles(xyz, types)
-            e.step(40)
-            m = e.metrics()
-            res.append((e.get_particles()[0], m))
-    assert res[0][1]["overflow_regrows"] >= 1
-    assert res[1][1]["overflow_regrows"] == 0
-    assert np.array_equal(res[0][0], res[1][0])
+    d, stored, _ = oracle_state(oracle, sys_, xyz, prec)
+    with Engine(sys_, precision=prec) as e:
+        e.set_particles(xyz, types)
+        cnt, h = e.neighbor_digest()
+        F, _ = e.forces()
+        e.step(20)
+    ocnt, oh = oracle.neighbor_digest(d, stored, types, f32=(prec == "f32c"))
+    assert cnt.max() > 300
+    assert np.array_equal(cnt, ocnt) and np.array_equal(h, oh)
+    Fo, _ = oracle.forces_f64(d, stored.astype(np.float64), types)
+    assert np.linalg.norm(F - Fo) <= (1e-12 if prec == "f64" else 1e-5) * np.linalg.norm(Fo)
 
 
 @pytest.mark.parametrize("prec", PRECS)
