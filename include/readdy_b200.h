@@ -237,8 +237,15 @@ int rdgpu_metrics_get(rdgpu_handle h, rdgpu_metrics* m);
 /* The cudaStream_t the handle launches on (as void*). */
 void* rdgpu_stream(rdgpu_handle h);
 
-/* Kernels launched by the last rdgpu_step (for launch accounting). */
+/* Kernels launched by this handle so far (for launch accounting). */
 int64_t rdgpu_launch_count(rdgpu_handle h);
+
+/* Runs nsteps steps one launch at a time (no CUDA graph) with CUDA events on
+   the handle's stream around the fused step kernel and around the counting
+   sort (scan + scatter), and returns their mean duration per step in
+   milliseconds.  The state advances exactly as with rdgpu_step.  No
+   reference counterpart (measurement hook).                                  */
+int rdgpu_step_profile(rdgpu_handle h, int64_t nsteps, double* step_kernel_ms, double* sort_ms);
 
 #ifdef __cplusplus
 }

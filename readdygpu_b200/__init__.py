@@ -15,7 +15,7 @@ LIB_PATH = _os.path.join(_HERE, "libreaddy_b200.so")
 
 if not _os.path.exists(LIB_PATH):
     raise ImportError(
-        f"{LIB_PATH} is missing: build it with `python -m readdygpu_b200.build` "
+        f"{LIB_PATH} is missing: build it with `python readdygpu_b200/build.py` "
         "(there is no CPU fallback)")
 
 lib = _abi.bind(_C.CDLL(LIB_PATH))

@@ -110,6 +110,7 @@ FUNCTIONS = [
     ("rdgpu_metrics_get", C.c_int, [P, C.POINTER(Metrics)]),
     ("rdgpu_stream", C.c_void_p, [P]),
     ("rdgpu_launch_count", C.c_int64, [P]),
+    ("rdgpu_step_profile", C.c_int, [P, C.c_int64, DP, DP]),
 ]
 
 

@@ -1,6 +1,9 @@
 """Builds the in-tree shared libraries.
 
-    python -m readdygpu_b200.build
+    python readdygpu_b200/build.py [--force]
+
+(run by path, not with -m: importing the package would load the library that
+is about to be rebuilt)
 
   readdygpu_b200/libreaddy_b200.so   engine: hand-written CUDA for sm_100a + C ABI
   readdygpu_b200/libreaddy_workloads.so  seeded synthetic benchmark inputs

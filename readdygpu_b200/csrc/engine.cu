@@ -34,6 +34,7 @@ struct rdgpu_engine {
     rdgpu_options opt{};
     int nsys = 0;
     bool value_image = false;            // some periodic axis has fewer than 3 cells
+    bool hrep = false;                   // only single harmonic-repulsion pair terms
     std::vector<rdgpu_box> boxes;
     std::vector<SysDev> sys_h;
     SysDev* sys_d = nullptr;
@@ -339,18 +340,25 @@ int prepare_step_state(Engine* E, long long t)
     return reset_counters(E, t);
 }
 
+template <class R> void launch_step_kernel(Engine* E, Args<R>& a)
+{
+    const int grid = (int)((E->npart_tot + kStepBlock - 1) / kStepBlock);
+    if (E->value_image)
+        step_kernel<R, true, false, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a);
+    else if (E->hrep)
+        step_kernel<R, false, true, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a);
+    else
+        step_kernel<R, false, false, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a);
+    ++E->launches;
+}
+
 template <class R> int launch_steps(Engine* E, int n, const double* noise_d)
 {
     Args<R> a = make_args<R>(E);
     a.noise = noise_d;
-    const int grid = (int)((E->npart_tot + kStepBlock - 1) / kStepBlock);
     for (int k = 0; k < n; ++k) {
         a.step_off = k;
-        if (E->value_image)
-            step_kernel<R, true, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a);
-        else
-            step_kernel<R, false, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a);
-        ++E->launches;
+        launch_step_kernel<R>(E, a);
         launch_sort<R>(E);
     }
     advance_kernel<<<1, 32, 0, E->stream>>>(E->step_d, E->err, n);
@@ -482,6 +490,42 @@ int setup_systems(Engine* E, std::string& why)
     if (cudaMalloc(&E->ext_d, esz) != cudaSuccess) { why = "cudaMalloc failed"; return -2; }
     cudaMemcpy(E->ext_d, ebuf.data(), esz, cudaMemcpyHostToDevice);
     return 0;
+}
+
+template <class R> int profile_impl(Engine* E, long long nsteps, double* kms, double* sms)
+{
+    cudaEvent_t e0, e1, e2;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventCreate(&e2));
+    Args<R> a = make_args<R>(E);
+    double tk = 0.0, ts = 0.0;
+    for (long long k = 0; k < nsteps; ++k) {
+        a.step_off = 0;
+        CK(cudaEventRecord(e0, E->stream));
+        launch_step_kernel<R>(E, a);
+        CK(cudaEventRecord(e1, E->stream));
+        launch_sort<R>(E);
+        CK(cudaEventRecord(e2, E->stream));
+        advance_kernel<<<1, 32, 0, E->stream>>>(E->step_d, E->err, 1);
+        ++E->launches;
+        CK(cudaEventSynchronize(e2));
+        float m1 = 0.f, m2 = 0.f;
+        cudaEventElapsedTime(&m1, e0, e1);
+        cudaEventElapsedTime(&m2, e1, e2);
+        tk += m1;
+        ts += m2;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    CK(cudaMemcpyAsync(E->pinned_err, E->err, sizeof(int), cudaMemcpyDeviceToHost, E->stream));
+    CK(cudaStreamSynchronize(E->stream));
+    if (*E->pinned_err) return fail(E, RDGPU_ERR_JUMP, "a step failed during profiling");
+    E->step_h += nsteps;
+    if (kms) *kms = nsteps > 0 ? tk / nsteps : 0.0;
+    if (sms) *sms = nsteps > 0 ? ts / nsteps : 0.0;
+    return RDGPU_OK;
 }
 
 template <class R> int set_particles_impl(Engine* E, const long long* offsets, long long ntot,
@@ -739,6 +783,21 @@ int create_impl(const rdgpu_system_desc* desc, int nsys, const rdgpu_box* boxes,
         return bail(RDGPU_ERR_NOMEM, "device allocation failed");
     int rc = setup_systems(E, why);
     if (rc) return bail(rc == -2 ? RDGPU_ERR_NOMEM : RDGPU_ERR_ARG, why);
+    // the harmonic-repulsion-only fast path applies when every pair potential is
+    // a harmonic repulsion and no type pair carries more than one of them
+    {
+        bool h = true;
+        for (int p = 0; p < desc->n_pair; ++p)
+            if (!(desc->pair[p].kind == RDGPU_P2_HARMONIC && desc->pair[p].subtype == RDGPU_SUB_REPULSIVE)) h = false;
+        const int M = RDGPU_MAX_TYPES;
+        for (int i = 0; i < desc->n_types && h; ++i)
+            for (int j = 0; j < desc->n_types && h; ++j) {
+                int n = 0;
+                for (int p = 0; p < desc->n_pair; ++p) n += (desc->pair[p].pairs[i * M + j] || desc->pair[p].pairs[j * M + i]);
+                if (n > 1) h = false;
+            }
+        E->hrep = h;
+    }
     // cells of all systems
     long long cb = 0;
     for (int s = 0; s < nsys; ++s) {
@@ -964,6 +1023,15 @@ void* rdgpu_stream(rdgpu_handle h)
 {
     Engine* E = (Engine*)h;
     return E ? (void*)E->stream : nullptr;
+}
+
+int rdgpu_step_profile(rdgpu_handle h, int64_t nsteps, double* step_kernel_ms, double* sort_ms)
+{
+    Engine* E = (Engine*)h;
+    GUARD(E);
+    NEED_PARTICLES(E);
+    if (nsteps < 1 || E->npart_tot == 0) return fail(E, RDGPU_ERR_ARG, "nsteps >= 1 and particles needed");
+    return DISPATCH(E, profile_impl, E, (long long)nsteps, step_kernel_ms, sort_ms);
 }
 
 int64_t rdgpu_launch_count(rdgpu_handle h)

@@ -132,11 +132,19 @@ __device__ __forceinline__ void cell_coords(const SysDev& s, const R x[3], int c
 // the range, which for >= 3 cells gives the same displacement xi - (xj + kL)
 // for every pair inside the cutoff.
 // ---------------------------------------------------------------------------
-template <class R, int MODE, bool VALUE_IMAGE>
-__device__ __forceinline__ void range_pairs(const State<R>& st, int j0, int j1, long long self, const R xi[3], int ti,
-                                            R sx, R sy, R sz, const R* __restrict__ rc2, const Box<R>& bx,
-                                            const SysDev& s, const TypeTab<R>* __restrict__ tab, Acc<R>& acc,
-                                            int& ncount, unsigned long long& hash)
+// Harmonic-repulsion-only fast path: every type pair has at most the one
+// term k (r - r0)/r for r < r0 (P2_Harmonic.java:167-178 with rc = r0), with
+// k and r0 in shared memory; the general path walks the term table.
+template <class R> struct FastTab {
+    R k[MAXT * MAXT];
+    R r0[MAXT * MAXT];
+};
+
+template <class R, int MODE, bool VALUE_IMAGE, bool SHIFT, bool HREP>
+__device__ __forceinline__ void range_pairs(const State<R>& st, int j0, int j1, int self, const R xi[3], int ti,
+                                            R sx, R sy, R sz, const R* __restrict__ rc2, const FastTab<R>* __restrict__ ft,
+                                            const Box<R>& bx, const SysDev& s, const TypeTab<R>* __restrict__ tab,
+                                            Acc<R>& acc, int& ncount, unsigned long long& hash)
 {
     for (int j = j0; j < j1; ++j) {
         R xj[3];
@@ -147,10 +155,14 @@ __device__ __forceinline__ void range_pairs(const State<R>& st, int j0, int j1, 
             dx = mimg(xi[0], xj[0], bx.L[0], bx.half[0], s.per[0]);
             dy = mimg(xi[1], xj[1], bx.L[1], bx.half[1], s.per[1]);
             dz = mimg(xi[2], xj[2], bx.L[2], bx.half[2], s.per[2]);
-        } else {
+        } else if (SHIFT) {
             dx = sub_rn(xi[0], add_rn(xj[0], sx));
             dy = sub_rn(xi[1], add_rn(xj[1], sy));
             dz = sub_rn(xi[2], add_rn(xj[2], sz));
+        } else {
+            dx = sub_rn(xi[0], xj[0]);
+            dy = sub_rn(xi[1], xj[1]);
+            dz = sub_rn(xi[2], xj[2]);
         }
         const R r2 = dist2(dx, dy, dz);
         const int pidx = ti * MAXT + (wj & 0xff);
@@ -158,6 +170,16 @@ __device__ __forceinline__ void range_pairs(const State<R>& st, int j0, int j1, 
             if (MODE == 2) {
                 ncount++;
                 hash += splitmix64((unsigned long long)load_id(st, j));
+                continue;
+            }
+            if (HREP && MODE == 0) {
+                // force only: pre = k (r - r0) / r; r == 0 has no direction
+                if (r2 > R(0)) {
+                    R pre;
+                    if constexpr (sizeof(R) == 4) pre = ft->k[pidx] * (1.0f - ft->r0[pidx] * rsqrtf(r2));
+                    else { const R r = sqrt(r2); pre = ft->k[pidx] * (r - ft->r0[pidx]) / r; }
+                    acc.add(pre, dx, dy, dz);
+                }
                 continue;
             }
             const R r = sqrt(r2);
@@ -172,16 +194,42 @@ __device__ __forceinline__ void range_pairs(const State<R>& st, int j0, int j1, 
     }
 }
 
-template <class R, int MODE, bool VALUE_IMAGE>
+// squared gap between coordinate x (cell-local offset f in [0, c)) and the
+// neighbour cell at offset d: 0 for d == 0, f^2 below, (c - f)^2 above
+template <class R>
+__device__ __forceinline__ R gap2(int d, R f, R c)
+{
+    const R g = d < 0 ? f : (d > 0 ? c - f : R(0));
+    return g * g;
+}
+
+// Pair sum over the 27-cell neighbourhood.  Cells whose nearest point is
+// farther than the particle's largest cutoff (with a relative margin of 1e-4,
+// far above rounding) are skipped: they cannot hold a neighbour, so the
+// neighbour set is unchanged.
+template <class R, int MODE, bool VALUE_IMAGE, bool HREP>
 __device__ __forceinline__ void neighbourhood(const State<R>& st, const int* __restrict__ start, const SysDev& s,
-                                              const int c[3], long long self, const R xi[3], int ti,
-                                              const R* __restrict__ rc2, const TypeTab<R>* __restrict__ tab,
-                                              Acc<R>& acc, int& ncount, unsigned long long& hash)
+                                              const int c[3], int self, const R xi[3], int ti,
+                                              const R* __restrict__ rc2, const FastTab<R>* __restrict__ ft,
+                                              const TypeTab<R>* __restrict__ tab, Acc<R>& acc, int& ncount,
+                                              unsigned long long& hash, R rmax2)
 {
     Box<R> bx;
     bx.load(s);
     const int n0 = s.n[0], n1 = s.n[1], n2 = s.n[2];
+    R cw[3], f[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if constexpr (sizeof(R) == 4) cw[a] = R(1) / s.invcf[a]; else cw[a] = R(1) / s.invc[a];
+        f[a] = xi[a] - (R)c[a] * cw[a];
+        // a periodic axis with fewer than 3 cells reaches each cell from
+        // either side: no pruning along it (zero gaps)
+        if (VALUE_IMAGE && s.per[a] && s.n[a] < 3) { f[a] = R(0); cw[a] = R(0); }
+    }
+    const R lim = rmax2 * R(1.0001);
     for (int dz = -1; dz <= 1; ++dz) {
+        const R gz = gap2(dz, f[2], cw[2]);
+        if (gz >= lim) continue;
         int z = c[2] + dz;
         R sz = R(0);
         if (z < 0 || z >= n2) {
@@ -191,6 +239,8 @@ __device__ __forceinline__ void neighbourhood(const State<R>& st, const int* __r
             z = z < 0 ? z + n2 : z - n2;
         }
         for (int dy = -1; dy <= 1; ++dy) {
+            const R gyz = gz + gap2(dy, f[1], cw[1]);
+            if (gyz >= lim) continue;
             int y = c[1] + dy;
             R sy = R(0);
             if (y < 0 || y >= n1) {
@@ -199,27 +249,51 @@ __device__ __forceinline__ void neighbourhood(const State<R>& st, const int* __r
                 sy = y < 0 ? -bx.L[1] : bx.L[1];
                 y = y < 0 ? y + n1 : y - n1;
             }
-            const long long row = s.cell_base + ((long long)z * n1 + y) * n0;
-            int xa = c[0] - 1, xb = c[0] + 1;
-            if (!s.per[0] || (VALUE_IMAGE && n0 < 3)) {
+            const int row = (int)s.cell_base + (z * n1 + y) * n0;
+            const bool shifted = (sy != R(0)) || (sz != R(0));
+            // x cells of the row within reach
+            int xa = (gyz + f[0] * f[0] < lim) ? c[0] - 1 : c[0];
+            int xb = (gyz + (cw[0] - f[0]) * (cw[0] - f[0]) < lim) ? c[0] + 1 : c[0];
+            if (VALUE_IMAGE) {
+                if (!s.per[0] || n0 < 3) { xa = max(xa, 0); xb = min(xb, n0 - 1); }
+                else {
+                    // ranges with the x wrap: the image is chosen per candidate
+                    if (xa < 0) {
+                        range_pairs<R, MODE, true, false, HREP>(st, start[row + n0 - 1], start[row + n0], self, xi, ti,
+                                                                R(0), R(0), R(0), rc2, ft, bx, s, tab, acc, ncount, hash);
+                        xa = 0;
+                    }
+                    if (xb >= n0) {
+                        range_pairs<R, MODE, true, false, HREP>(st, start[row], start[row + 1], self, xi, ti, R(0),
+                                                                R(0), R(0), rc2, ft, bx, s, tab, acc, ncount, hash);
+                        xb = n0 - 1;
+                    }
+                }
+                range_pairs<R, MODE, true, false, HREP>(st, start[row + xa], start[row + xb + 1], self, xi, ti, R(0),
+                                                        R(0), R(0), rc2, ft, bx, s, tab, acc, ncount, hash);
+                continue;
+            }
+            if (!s.per[0]) {
                 xa = max(xa, 0);
                 xb = min(xb, n0 - 1);
-                range_pairs<R, MODE, VALUE_IMAGE>(st, start[row + xa], start[row + xb + 1], self, xi, ti, R(0), sy, sz,
-                                                  rc2, bx, s, tab, acc, ncount, hash);
             } else {
                 if (xa < 0) {
-                    range_pairs<R, MODE, VALUE_IMAGE>(st, start[row + n0 - 1], start[row + n0], self, xi, ti, -bx.L[0],
-                                                      sy, sz, rc2, bx, s, tab, acc, ncount, hash);
+                    range_pairs<R, MODE, false, true, HREP>(st, start[row + n0 - 1], start[row + n0], self, xi, ti,
+                                                            -bx.L[0], sy, sz, rc2, ft, bx, s, tab, acc, ncount, hash);
                     xa = 0;
                 }
-                const bool wrapb = xb >= n0;
-                if (wrapb) xb = n0 - 1;
-                range_pairs<R, MODE, VALUE_IMAGE>(st, start[row + xa], start[row + xb + 1], self, xi, ti, R(0), sy, sz,
-                                                  rc2, bx, s, tab, acc, ncount, hash);
-                if (wrapb)
-                    range_pairs<R, MODE, VALUE_IMAGE>(st, start[row], start[row + 1], self, xi, ti, bx.L[0], sy, sz,
-                                                      rc2, bx, s, tab, acc, ncount, hash);
+                if (xb >= n0) {
+                    range_pairs<R, MODE, false, true, HREP>(st, start[row], start[row + 1], self, xi, ti, bx.L[0], sy,
+                                                            sz, rc2, ft, bx, s, tab, acc, ncount, hash);
+                    xb = n0 - 1;
+                }
             }
+            if (shifted)
+                range_pairs<R, MODE, false, true, HREP>(st, start[row + xa], start[row + xb + 1], self, xi, ti, R(0),
+                                                        sy, sz, rc2, ft, bx, s, tab, acc, ncount, hash);
+            else
+                range_pairs<R, MODE, false, false, HREP>(st, start[row + xa], start[row + xb + 1], self, xi, ti, R(0),
+                                                         R(0), R(0), rc2, ft, bx, s, tab, acc, ncount, hash);
         }
     }
 }
@@ -290,15 +364,28 @@ __device__ __forceinline__ int em_update(double x[3], double* /*c*/, int& w, con
 // ---------------------------------------------------------------------------
 // The step kernel: one thread per particle of the sorted arrays
 // ---------------------------------------------------------------------------
-template <class R, bool VALUE_IMAGE, int BLOCK>
-__global__ void __launch_bounds__(BLOCK, 4) step_kernel(Args<R> a)
+template <class R, bool VALUE_IMAGE, bool HREP, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) step_kernel(Args<R> a)
 {
     __shared__ R s_rc2[MAXT * MAXT];
+    __shared__ R s_rmax2[MAXT];
+    __shared__ FastTab<R> s_ft;
     if (*((volatile int*)a.err)) return;   // an earlier step failed: keep its input intact
-    for (int k = threadIdx.x; k < MAXT * MAXT; k += BLOCK) s_rc2[k] = a.tab->rc2[k];
+    for (int k = threadIdx.x; k < MAXT * MAXT; k += BLOCK) {
+        s_rc2[k] = a.tab->rc2[k];
+        if (HREP) {
+            s_ft.k[k] = a.tab->nterm[k] ? a.tab->term[k * MAX_TERMS].k : R(0);
+            s_ft.r0[k] = a.tab->nterm[k] ? a.tab->term[k * MAX_TERMS].r0 : R(0);
+        }
+    }
+    for (int k = threadIdx.x; k < MAXT; k += BLOCK) {
+        R m = R(0);
+        for (int j = 0; j < MAXT; ++j) m = max(m, a.tab->rc2[k * MAXT + j]);
+        s_rmax2[k] = m;
+    }
     __syncthreads();
     const long long t = (a.step_ptr ? *a.step_ptr : 0LL) + a.step_off;
-    const long long i = blockIdx.x * (long long)BLOCK + threadIdx.x;
+    const int i = blockIdx.x * BLOCK + threadIdx.x;
     if (i >= a.ntot) return;
     const int si = a.sys_of[i];
     const SysDev& s = a.sys[si];
@@ -321,7 +408,8 @@ __global__ void __launch_bounds__(BLOCK, 4) step_kernel(Args<R> a)
     acc.zero();
     int nc = 0;
     unsigned long long hh = 0;
-    neighbourhood<R, 0, VALUE_IMAGE>(a.cur, a.start, s, cc, i, xi, ti, s_rc2, a.tab, acc, nc, hh);
+    neighbourhood<R, 0, VALUE_IMAGE, HREP>(a.cur, a.start, s, cc, i, xi, ti, s_rc2, &s_ft, a.tab, acc, nc, hh,
+                                           s_rmax2[ti]);
     R F[3];
     acc.force(F);
     if (a.n_ext > 0) {
@@ -382,34 +470,49 @@ __global__ void __launch_bounds__(SCAN_BLOCK) scan_tiles_kernel(const int* __res
 }
 
 // start[c] = exclusive prefix of counts; counts cleared for the next step;
-// start[ncells] = total
+// start[ncells] = total.  The tile goes through shared memory so that every
+// global access is coalesced.
 __global__ void __launch_bounds__(SCAN_BLOCK) scan_apply_kernel(int* __restrict__ counts, long long ncells,
                                                                 const int* __restrict__ tile_sum, int ntiles,
                                                                 int* __restrict__ start, const int* err)
 {
     constexpr int PER = SCAN_TILE / SCAN_BLOCK;
+    __shared__ int s_t[SCAN_TILE + SCAN_TILE / 32];   // padded against bank conflicts
     __shared__ int s_w[SCAN_BLOCK / 32];
     __shared__ int s_base;
     if (*((volatile const int*)err)) return;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const long long base_c = (long long)blockIdx.x * SCAN_TILE;
     // base of this tile: sum of the preceding tile sums
     int b = 0;
     for (int k = tid; k < (int)blockIdx.x; k += SCAN_BLOCK) b += tile_sum[k];
     for (int o = 16; o > 0; o >>= 1) b += __shfl_xor_sync(FULL, b, o);
     if (lane == 0) s_w[wid] = b;
+    // coalesced load of the tile; the counts are cleared for the next step
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int e = k * SCAN_BLOCK + tid;
+        const long long c = base_c + e;
+        int v = 0;
+        if (c < ncells) {
+            v = counts[c];
+            counts[c] = 0;
+        }
+        s_t[e + (e >> 5)] = v;
+    }
     __syncthreads();
     if (tid == 0) {
         int tot = 0;
         for (int w = 0; w < SCAN_BLOCK / 32; ++w) tot += s_w[w];
         s_base = tot;
     }
-    __syncthreads();
-    const long long c0 = (long long)blockIdx.x * SCAN_TILE + (long long)tid * PER;
+    // each thread scans PER contiguous elements
     int v[PER];
     int sum = 0;
 #pragma unroll
     for (int k = 0; k < PER; ++k) {
-        v[k] = (c0 + k < ncells) ? counts[c0 + k] : 0;
+        const int e = tid * PER + k;
+        v[k] = s_t[e + (e >> 5)];
         sum += v[k];
     }
     const int incl = warp_incl_scan(sum, lane);
@@ -425,13 +528,18 @@ __global__ void __launch_bounds__(SCAN_BLOCK) scan_apply_kernel(int* __restrict_
     int run = s_base + s_w[wid] + incl - sum;
 #pragma unroll
     for (int k = 0; k < PER; ++k) {
-        if (c0 + k < ncells) {
-            start[c0 + k] = run;
-            counts[c0 + k] = 0;
-        }
+        const int e = tid * PER + k;
+        s_t[e + (e >> 5)] = run;
         run += v[k];
     }
     if (blockIdx.x == ntiles - 1 && tid == SCAN_BLOCK - 1) start[ncells] = run;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < PER; ++k) {
+        const int e = k * SCAN_BLOCK + tid;
+        const long long c = base_c + e;
+        if (c < ncells) start[c] = s_t[e + (e >> 5)];
+    }
 }
 
 template <class R>
@@ -565,7 +673,13 @@ template <class R, int MODE, bool VALUE_IMAGE>
 __global__ void diag_kernel(Args<R> a, double* forces, double* energy, int* ncount, unsigned long long* hashes)
 {
     __shared__ R s_rc2[MAXT * MAXT];
+    __shared__ R s_rmax2[MAXT];
     for (int k = threadIdx.x; k < MAXT * MAXT; k += blockDim.x) s_rc2[k] = a.tab->rc2[k];
+    for (int k = threadIdx.x; k < MAXT; k += blockDim.x) {
+        R m = R(0);
+        for (int j = 0; j < MAXT; ++j) m = max(m, a.tab->rc2[k * MAXT + j]);
+        s_rmax2[k] = m;
+    }
     __syncthreads();
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.ntot;
          i += (long long)gridDim.x * blockDim.x) {
@@ -582,7 +696,8 @@ __global__ void diag_kernel(Args<R> a, double* forces, double* energy, int* ncou
         acc.zero();
         int nc = 0;
         unsigned long long hh = 0;
-        neighbourhood<R, MODE, VALUE_IMAGE>(a.cur, a.start, s, cc, i, xi, ti, s_rc2, a.tab, acc, nc, hh);
+        neighbourhood<R, MODE, VALUE_IMAGE, false>(a.cur, a.start, s, cc, (int)i, xi, ti, s_rc2, nullptr, a.tab,
+                                                   acc, nc, hh, s_rmax2[ti]);
         if (MODE == 2) {
             ncount[g] = nc;
             hashes[g] = hh;

@@ -98,6 +98,12 @@ class Engine:
     def launch_count(self):
         return _lib().rdgpu_launch_count(self._h)
 
+    def step_profile(self, nsteps):
+        """Mean ms per step of the fused step kernel and of the counting sort."""
+        ks, ss = C.c_double(), C.c_double()
+        self._check(_lib().rdgpu_step_profile(self._h, int(nsteps), C.byref(ks), C.byref(ss)))
+        return ks.value, ss.value
+
     # -- state -----------------------------------------------------------
     def set_particles(self, xyz, types, offsets=None):
         xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)

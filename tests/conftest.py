@@ -18,7 +18,7 @@ def _ensure_built():
         subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
     need = [os.path.join(ROOT, "readdygpu_b200", f) for f in ("libreaddy_b200.so", "libreaddy_workloads.so")]
     if not all(os.path.exists(p) for p in need):
-        subprocess.check_call([sys.executable, "-m", "readdygpu_b200.build"], cwd=ROOT)
+        subprocess.check_call([sys.executable, os.path.join(ROOT, "readdygpu_b200", "build.py")], cwd=ROOT)
 
 
 _ensure_built()
