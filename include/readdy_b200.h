@@ -232,6 +232,34 @@ int rdgpu_rdf_normalized(rdgpu_handle h, double* g);
 
 int rdgpu_metrics_get(rdgpu_handle h, rdgpu_metrics* m);
 
+/* ---- RDF counts without device allocation ------------------------------ */
+
+/* Limits of rdgpu_rdf_counts_noalloc (its scratch is a fixed static array). */
+#define RDGPU_NOALLOC_MAX_PARTICLES  65536
+#define RDGPU_NOALLOC_MAX_CELLS      131072
+#define RDGPU_NOALLOC_MAX_BINS       4096
+
+/* RDF pair counts of one periodic/non-periodic box for callers that cannot
+   allocate device memory: a host runtime that owns the device memory pool
+   (a JVM handing out direct buffers, a plug-in that must not change the
+   device footprint after start-up).  No counterpart in the reference.
+   xyz_dev (3n doubles, absolute coordinates) and types_dev (n ints) are
+   device pointers the caller owns; counts_dev (n_types^2 * nbins uint64) is
+   the device output, overwritten with this call's counts -- the same counts
+   rdgpu_rdf(accumulate = 0) gives for these particles in an FP64 handle with
+   the same box.  Scratch: a static device array of about 3.7 MB held by every
+   GPU that loads the library; the first call on a device resolves its
+   address (make that call before any stream capture).  Calls on the same
+   device share the scratch: calls that overlap on the GPU race.  Runs on
+   `stream` (a cudaStream_t, NULL = default) and synchronises it before
+   returning.  Rejects n > RDGPU_NOALLOC_MAX_PARTICLES, nbins >
+   RDGPU_NOALLOC_MAX_BINS and boxes needing more than RDGPU_NOALLOC_MAX_CELLS
+   cells with RDGPU_ERR_ARG; rdgpu_last_error(NULL) gives the reason.         */
+int rdgpu_rdf_counts_noalloc(const double* xyz_dev, const int32_t* types_dev, int64_t n,
+                             int32_t n_types, const double lo[3], const double hi[3],
+                             const int32_t periodic[3], int32_t nbins, double rmax,
+                             uint64_t* counts_dev, void* stream);
+
 /* ---- device-resident access for benchmarks ----------------------------- */
 
 /* The cudaStream_t the handle launches on (as void*). */

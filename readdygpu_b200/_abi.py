@@ -111,6 +111,8 @@ FUNCTIONS = [
     ("rdgpu_stream", C.c_void_p, [P]),
     ("rdgpu_launch_count", C.c_int64, [P]),
     ("rdgpu_step_profile", C.c_int, [P, C.c_int64, DP, DP]),
+    ("rdgpu_rdf_counts_noalloc", C.c_int, [P, P, C.c_int64, C.c_int32, DP, DP, I32P, C.c_int32, C.c_double,
+                                           P, P]),
 ]
 
 

@@ -36,11 +36,11 @@ def _stale(out, deps):
 
 def build_engine(force=False):
     out = os.path.join(HERE, "libreaddy_b200.so")
-    deps = [os.path.join(CSRC, f) for f in ("engine.cu", "engine_kernels.cuh", "engine_device.cuh")]
+    deps = [os.path.join(CSRC, f) for f in ("engine.cu", "engine_kernels.cuh", "engine_device.cuh", "rdf_noalloc.cu")]
     deps.append(os.path.join(ROOT, "include", "readdy_b200.h"))
     if force or _stale(out, deps):
         _run([NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-                              os.path.join(CSRC, "engine.cu"), "-o", out])
+                              os.path.join(CSRC, "engine.cu"), os.path.join(CSRC, "rdf_noalloc.cu"), "-o", out])
     return out
 
 

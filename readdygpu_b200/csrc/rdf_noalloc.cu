@@ -47,7 +47,6 @@ static __device__ __align__(256) unsigned char g_na_scratch[sizeof(NaScratch)];
 
 std::mutex g_na_mutex;
 void* g_na_ptr[64] = {nullptr};          // resolved scratch address per device
-thread_local std::string g_na_error;
 
 struct NaBox {
     double L[3], half[3], lo[3];
@@ -165,7 +164,7 @@ __global__ void na_rdf(const NaScratch* __restrict__ s, long long n, int S, int 
     if (!s->flags) {
         const double rmax2 = s->e2[nbins];
         const double rmax = w * nbins;
-        int rng[3], lo3[3], cntax[3];
+        int lo3[3], cntax[3];
         for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
              i += (long long)gridDim.x * blockDim.x) {
             const NaRec p = s->rec[i];
@@ -174,7 +173,6 @@ __global__ void na_rdf(const NaScratch* __restrict__ s, long long n, int S, int 
             for (int a = 0; a < 3; ++a) {
                 int r = (int)ceil(rmax * b.invc[a]);
                 if (r < 1) r = 1;
-                rng[a] = r;
                 if (b.per[a]) {
                     if (2 * r + 1 >= b.n[a]) { lo3[a] = 0; cntax[a] = b.n[a]; }
                     else { lo3[a] = cc[a] - r; cntax[a] = 2 * r + 1; }
@@ -222,15 +220,18 @@ __global__ void na_rdf(const NaScratch* __restrict__ s, long long n, int S, int 
     }
 }
 
-int na_fail(int code, const std::string& msg)
-{
-    g_na_error = msg;
-    return code;
-}
-
 }  // namespace
 
-const char* rdgpu_noalloc_last_error_text() { return g_na_error.c_str(); }
+// the text rdgpu_last_error(NULL) returns (engine.cu)
+std::string& rdgpu_global_error();
+
+namespace {
+int na_fail(int code, const std::string& msg)
+{
+    rdgpu_global_error() = msg;
+    return code;
+}
+}  // namespace
 
 extern "C" int rdgpu_rdf_counts_noalloc(const double* xyz_dev, const int32_t* types_dev, int64_t n,
                                         int32_t n_types, const double lo[3], const double hi[3],
@@ -258,7 +259,7 @@ extern "C" int rdgpu_rdf_counts_noalloc(const double* xyz_dev, const int32_t* ty
         b.per[a] = periodic[a] ? 1 : 0;
         int k = (int)std::floor(L / rmax);
         if (k < 1) k = 1;
-        if (k > 64) k = 64;
+        if (k > 50) k = 50;          // 50^3 cells fit RDGPU_NOALLOC_MAX_CELLS
         b.n[a] = k;
         b.invc[a] = (double)k / L;
         ncells *= k;
