@@ -299,6 +299,160 @@ __device__ __forceinline__ void neighbourhood(const State<R>& st, const int* __r
 }
 
 // ---------------------------------------------------------------------------
+// Flattened force walk for systems with >= 3 cells on every periodic axis.
+//
+// The per-row loops of neighbourhood() make a warp iterate, for every one of
+// the 9 rows, as often as its longest lane needs, and run the accepted-pair
+// block in nearly every iteration for the few lanes that accept.  Here each
+// thread walks its 9 row ranges as ONE sequence of candidates (the warp
+// iterates max over lanes of the candidate total), and accepted pairs go to a
+// short per-thread list in shared memory that is evaluated in bulk.  Row
+// bounds are loaded up front, all 18 loads in flight together, and kept in
+// shared memory.  The periodic x wrap of boundary cells is a second, rare
+// pass.  Rows, images, pruning and the pair set are those of neighbourhood();
+// forces of FP32 states are bit-identical (fixed-point accumulation).
+// ---------------------------------------------------------------------------
+template <class R> struct PairRec;
+template <> struct __align__(16) PairRec<float> { float dx, dy, dz; int pidx; };
+template <> struct __align__(16) PairRec<double> { double dx, dy, dz; long long pidx; };
+
+template <class R, bool HREP, int BLOCK>
+__device__ __forceinline__ void flush_pairs(const PairRec<R>* __restrict__ l, int cnt,
+                                            const FastTab<R>* __restrict__ ft,
+                                            const TypeTab<R>* __restrict__ tab, Acc<R>& acc)
+{
+    for (int m = 0; m < cnt; ++m) {
+        const PairRec<R> p = l[m * BLOCK];
+        const int pidx = (int)p.pidx;
+        const R r2 = dist2(p.dx, p.dy, p.dz);
+        if (HREP) {
+            // pre = k (r - r0) / r; r == 0 has no direction
+            if (r2 > R(0)) {
+                R pre;
+                if constexpr (sizeof(R) == 4) pre = ft->k[pidx] * (1.0f - ft->r0[pidx] * rsqrtf(r2));
+                else { const R r = sqrt(r2); pre = ft->k[pidx] * (r - ft->r0[pidx]) / r; }
+                acc.add(pre, p.dx, p.dy, p.dz);
+            }
+        } else {
+            const R r = sqrt(r2);
+            const int nt = tab->nterm[pidx];
+            for (int q = 0; q < nt; ++q) {
+                R pre, e;
+                pair_term(tab->term[pidx * MAX_TERMS + q], r, pre, e);
+                acc.add(pre, p.dx, p.dy, p.dz);
+            }
+        }
+    }
+}
+
+// shift code of one axis: 0 none, 1 minus L, 2 plus L
+template <class R> __device__ __forceinline__ R shift_of(unsigned code, R L)
+{
+    return (code & 1u) ? -L : ((code & 2u) ? L : R(0));
+}
+
+template <class R, bool HREP, int BLOCK, int CAP>
+__device__ __forceinline__ void neighbourhood_flat(const State<R>& st, const int* __restrict__ start,
+                                                   const SysDev& s, const int c[3], int self, const R xi[3], int ti,
+                                                   const R* __restrict__ rc2, const FastTab<R>* __restrict__ ft,
+                                                   const TypeTab<R>* __restrict__ tab, Acc<R>& acc, R rmax2,
+                                                   int* __restrict__ s_j0, int* __restrict__ s_j1,
+                                                   PairRec<R>* __restrict__ s_list)
+{
+    const int tid = threadIdx.x;
+    Box<R> bx;
+    bx.load(s);
+    const int n0 = s.n[0], n1 = s.n[1], n2 = s.n[2];
+    R cw[3], f[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        if constexpr (sizeof(R) == 4) cw[q] = R(1) / s.invcf[q]; else cw[q] = R(1) / s.invc[q];
+        f[q] = xi[q] - (R)c[q] * cw[q];
+    }
+    const R lim = rmax2 * R(1.0001);
+    const R fx2 = f[0] * f[0], gx2 = (cw[0] - f[0]) * (cw[0] - f[0]);
+    // rows r = 3 (dz + 1) + (dy + 1): bounds to shared memory, image shift
+    // codes of y and z packed 2 bits per row, x-wrap rows as a bit mask
+    unsigned ycode = 0, zcode = 0, wrap = 0;
+    int rowpos[9];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+        const int dz = r / 3 - 1, dy = r % 3 - 1;
+        int z = c[2] + dz, y = c[1] + dy;
+        bool v = true;
+        unsigned zc = 0, yc = 0;
+        if (z < 0) { if (s.per[2]) { z += n2; zc = 1; } else v = false; }
+        else if (z >= n2) { if (s.per[2]) { z -= n2; zc = 2; } else v = false; }
+        if (y < 0) { if (s.per[1]) { y += n1; yc = 1; } else v = false; }
+        else if (y >= n1) { if (s.per[1]) { y -= n1; yc = 2; } else v = false; }
+        const R gyz = gap2(dz, f[2], cw[2]) + gap2(dy, f[1], cw[1]);
+        v = v && gyz < lim;
+        const int row = (int)s.cell_base + (z * n1 + y) * n0;
+        int xa = (gyz + fx2 < lim) ? c[0] - 1 : c[0];
+        int xb = (gyz + gx2 < lim) ? c[0] + 1 : c[0];
+        if (v && s.per[0] && (xa < 0 || xb >= n0)) wrap |= 1u << r;
+        xa = max(xa, 0);
+        xb = min(xb, n0 - 1);
+        ycode |= yc << (2 * r);
+        zcode |= zc << (2 * r);
+        rowpos[r] = row;
+        s_j0[r * BLOCK + tid] = v ? __ldg(start + row + xa) : 0;
+        s_j1[r * BLOCK + tid] = v ? __ldg(start + row + xb + 1) : 0;
+    }
+    int cnt = 0;
+    R sx = R(0);
+    for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) {
+            if (!wrap) break;
+            // the wrapped-around boundary cell of each wrap row, shifted by -L
+            // (cell n0 - 1 seen from cell 0) or +L (cell 0 seen from n0 - 1)
+            const bool lo = c[0] == 0;
+            sx = lo ? -bx.L[0] : bx.L[0];
+#pragma unroll
+            for (int r = 0; r < 9; ++r) {
+                const bool w = (wrap >> r) & 1u;
+                const int cx = rowpos[r] + (lo ? n0 - 1 : 0);
+                s_j0[r * BLOCK + tid] = w ? __ldg(start + cx) : 0;
+                s_j1[r * BLOCK + tid] = w ? __ldg(start + cx + 1) : 0;
+            }
+        }
+        int r = -1, j = 0, e = 0;
+        R sy = R(0), sz = R(0);
+        for (;;) {
+            if (j >= e) {
+                do {
+                    if (++r == 9) break;
+                    j = s_j0[r * BLOCK + tid];
+                    e = s_j1[r * BLOCK + tid];
+                } while (j >= e);
+                if (r == 9) break;
+                sy = shift_of<R>(ycode >> (2 * r), bx.L[1]);
+                sz = shift_of<R>(zcode >> (2 * r), bx.L[2]);
+            }
+            R xj[3];
+            int wj;
+            load_pos(st, j, xj, wj);
+            const R dx = sub_rn(xi[0], add_rn(xj[0], sx));
+            const R dy = sub_rn(xi[1], add_rn(xj[1], sy));
+            const R dz = sub_rn(xi[2], add_rn(xj[2], sz));
+            const R r2 = dist2(dx, dy, dz);
+            const int pidx = ti * MAXT + (wj & 0xff);
+            if (r2 < rc2[pidx] && j != self) {
+                PairRec<R> p;
+                p.dx = dx; p.dy = dy; p.dz = dz; p.pidx = pidx;
+                s_list[cnt * BLOCK + tid] = p;
+                if (++cnt == CAP) {
+                    flush_pairs<R, HREP, BLOCK>(s_list + tid, cnt, ft, tab, acc);
+                    cnt = 0;
+                }
+            }
+            ++j;
+        }
+    }
+    flush_pairs<R, HREP, BLOCK>(s_list + tid, cnt, ft, tab, acc);
+}
+
+// ---------------------------------------------------------------------------
 // Euler-Maruyama update + wrap (CudaSimulation.cu:1852-1858 with the Java
 // mobility D dt/(kB T), ParticleParametersFactory.java:152-155)
 // ---------------------------------------------------------------------------
@@ -370,6 +524,10 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) step_kernel(Arg
     __shared__ R s_rc2[MAXT * MAXT];
     __shared__ R s_rmax2[MAXT];
     __shared__ FastTab<R> s_ft;
+    constexpr int CAP = 4;
+    constexpr bool FLAT = !VALUE_IMAGE && sizeof(R) == 8;
+    __shared__ int s_j0[FLAT ? 9 * BLOCK : 1], s_j1[FLAT ? 9 * BLOCK : 1];
+    __shared__ PairRec<R> s_list[FLAT ? CAP * BLOCK : 1];
     if (*((volatile int*)a.err)) return;   // an earlier step failed: keep its input intact
     for (int k = threadIdx.x; k < MAXT * MAXT; k += BLOCK) {
         s_rc2[k] = a.tab->rc2[k];
@@ -408,8 +566,14 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) step_kernel(Arg
     acc.zero();
     int nc = 0;
     unsigned long long hh = 0;
-    neighbourhood<R, 0, VALUE_IMAGE, HREP>(a.cur, a.start, s, cc, i, xi, ti, s_rc2, &s_ft, a.tab, acc, nc, hh,
-                                           s_rmax2[ti]);
+    // FP64 states take the flattened walk (faster there); FP32 states the
+    // per-row walk, which measured slightly faster for them
+    if (VALUE_IMAGE || sizeof(R) == 4)
+        neighbourhood<R, 0, VALUE_IMAGE, HREP>(a.cur, a.start, s, cc, i, xi, ti, s_rc2, &s_ft, a.tab, acc, nc, hh,
+                                               s_rmax2[ti]);
+    else
+        neighbourhood_flat<R, HREP, BLOCK, CAP>(a.cur, a.start, s, cc, i, xi, ti, s_rc2, &s_ft, a.tab, acc,
+                                                s_rmax2[ti], s_j0, s_j1, s_list);
     R F[3];
     acc.force(F);
     if (a.n_ext > 0) {
