@@ -48,6 +48,9 @@ def parse():
     p.add_argument("--precision", default="f32c", choices=["f32c", "f64"])
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--neighbour", default="auto", choices=["auto", "cells", "list"])
+    p.add_argument("--skin", type=float, default=0.0)
 
     return p.parse_args()
 
@@ -61,14 +64,14 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def traffic_per_particle(prec, config):
+def traffic_per_particle(prec, config, mode):
     """DRAM bytes per particle-step of the step kernel from the committed ncu
     summary (profiles/step_kernel_traffic.json), scaled to this launch."""
     path = os.path.join(ROOT, "profiles", "step_kernel_traffic.json")
     try:
         with open(path) as f:
             d = json.load(f)
-        return d[f"{prec}_config{config}"]["bytes_per_particle_step"]
+        return d[f"{prec}_config{config}_{mode}"]["bytes_per_particle_step"]
     except Exception:
         return None
 
@@ -168,6 +171,47 @@ def cpu_baseline(w, budget_s=12.0, threads=None):
                       f"C oracle, {threads} OpenMP threads, {dt:.1f} s"}
 
 
+def plain_f64(w, local, steps=200, sample=32):
+    """The plain FP64 single-system GPU path (the drop-in): each sampled system
+    of the batch alone in its own FP64 handle with default options (autotuned
+    before timing), stepped `steps` steps after as many warm-up steps; the
+    particle-steps/s of running them one after another, device-timed."""
+    import numpy as np
+    import torch
+    import readdygpu_b200 as R
+    if w.boxes is None:
+        picks = [None]
+    else:
+        picks = sorted(set(np.linspace(0, len(w.boxes) - 1, sample).round().astype(int).tolist()))
+    ps, ms, npart = 0.0, 0.0, 0
+    for k in picks:
+        if k is None:
+            eng = R.Engine(w.system, precision="f64", device=local, seed=3)
+            xyz, ty, off = w.xyz, w.types, None
+        else:
+            eng = R.Engine(w.system, precision="f64", device=local, boxes=[w.boxes[k]])
+            a_, b_ = int(w.offsets[k]), int(w.offsets[k + 1])
+            xyz, ty, off = w.xyz[a_:b_], w.types[a_:b_], np.array([0, b_ - a_], np.int64)
+        eng.set_particles(xyz, ty, offsets=off)
+        eng.autotune()
+        eng.step(steps)
+        st = torch.cuda.ExternalStream(eng.stream, device=local)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        eng.step(steps)
+        e1.record(st)
+        e1.synchronize()
+        ms += e0.elapsed_time(e1)
+        ps += len(ty) * steps
+        npart += len(ty)
+        eng.close()
+    return {"value": ps / (ms / 1e3), "unit": "particle-steps/s", "systems": len(picks), "particles": npart,
+            "steps": steps,
+            "sample": f"{len(picks)} of the workload's systems spread over its size range, each alone in an FP64 "
+                      f"handle, {steps} timed steps each"}
+
+
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -202,10 +246,13 @@ def run_ours(args):
     if w.boxes is not None:
         # each rank owns its own replicate ensemble: shift the seeds
         kw["boxes"] = [(lo, hi, per, sd + 7919 * rank) for (lo, hi, per, sd) in w.boxes]
-    eng = R.Engine(w.system, precision=args.precision, device=local, seed=11 + rank, **kw)
+    eng = R.Engine(w.system, precision=args.precision, device=local, seed=11 + rank,
+                   neighbour_mode=args.neighbour, skin=args.skin, **kw)
     eng.set_particles(w.xyz, w.types, offsets=w.offsets)
     stream = torch.cuda.ExternalStream(eng.stream, device=local)
+    eng.autotune()          # outside the timed region
     eng.step(args.warmup)
+    nb = eng.metrics()
 
     def barrier():
         torch.cuda.synchronize()
@@ -238,7 +285,7 @@ def run_ours(args):
     alg = ALG_BYTES[args.precision] * w.n
     peak, peak_kind = measured_peak_hbm()
     achieved = alg / per_launch_s / 1e9
-    tpp = traffic_per_particle(args.precision, args.config)
+    tpp = traffic_per_particle(args.precision, args.config, nb["neighbour_mode"])
 
     # ---- end to end through the C ABI with host buffers ------------------
     e2e = None
@@ -269,6 +316,9 @@ def run_ours(args):
     cb = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(w)
+    plain = None
+    if rank == 0 and not args.no_plain:
+        plain = plain_f64(w, local)
     if rank == 0:
         line = {"metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": ws,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
@@ -277,14 +327,18 @@ def run_ours(args):
                 "config": {"workload": w.name, "particles": w.n,
                            "systems": len(w.boxes) if w.boxes else 1, "precision": args.precision,
                            "parallelism": f"replicas{ws}",
+                           "neighbour": {"mode": nb["neighbour_mode"], "skin_nm": nb["skin"],
+                                         "requested": args.neighbour},
                            "l2": "inputs larger than L2 (state read+written per step exceeds 126 MB)"
                            if alg > 126e6 else "state fits in L2"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_kind": peak_kind,
                              "traffic": (tpp * w.n if tpp else None),
-                             "kernel": "step_kernel", "kernel_ms": kernel_ms, "sort_ms": sort_ms,
+                             "kernel": "list_step_kernel" if nb["neighbour_mode"] == "list" else "step_kernel",
+                             "kernel_ms": kernel_ms, "sort_ms": sort_ms,
                              "alg_bytes_per_particle_step": ALG_BYTES[args.precision]},
-                "e2e": e2e, "cpu_baseline": cb, "gpu_launches": launches, "clocks": clk.summary()}
+                "e2e": e2e, "cpu_baseline": cb, "gpu_launches": launches, "clocks": clk.summary(),
+                "plain_f64": plain, "vs_plain_f64": (value / ws / plain["value"]) if plain else None}
         print(json.dumps(line), flush=True)
     eng.close()
     if ws > 1:

@@ -124,16 +124,25 @@ typedef struct {
     uint64_t seed;
 } rdgpu_box;
 
+/* Neighbour search of the step.  CELLS walks the 27-cell neighbourhood of
+   every particle in every step.  LIST evaluates a pair list of radius
+   rc_max + skin that is rebuilt (with a re-sort by cell) whenever a particle
+   has moved more than about skin/2 since the last build; the pair set and the
+   FP32 forces are identical to CELLS.  AUTO starts with CELLS and, at the
+   first rdgpu_step of >= 4 x graph_steps steps, times CELLS and LIST at
+   skins of 0.1 .. 0.5 x rc_max on the handle's particles and keeps the
+   fastest.                                                                     */
+#define RDGPU_NB_AUTO  0
+#define RDGPU_NB_CELLS 1
+#define RDGPU_NB_LIST  2
+
 typedef struct {
     int32_t  precision;           /* RDGPU_PREC_*                                      */
     int32_t  device;              /* CUDA device ordinal                               */
-    int32_t  cell_cap;            /* slots per cell, power of two; 0 = automatic       */
-    int32_t  lanes_per_particle;  /* 1,2,4,8; 0 = automatic (autotuner table)          */
-    int32_t  cells_per_lane;      /* warp-list kernel: cells per lane; brick kernel:
-                                     brick edge in cells; 0 = automatic                */
-    int32_t  block_size;          /* threads per block of the step kernel; 0 = auto    */
+    int32_t  neighbour_mode;      /* RDGPU_NB_*                                        */
     int32_t  graph_steps;         /* steps captured per CUDA graph; 0 = 100, <0 = off  */
-    int32_t  kernel_variant;      /* 0: brick-staged step kernel, 1: warp-list kernel  */
+    double   skin;                /* pair-list skin [nm] for RDGPU_NB_LIST; 0 = 0.25 x
+                                     the largest pair cutoff                           */
     uint64_t seed;                /* Philox seed of a single-system handle             */
 } rdgpu_options;
 
@@ -142,8 +151,11 @@ typedef struct {
     double   msd[RDGPU_MAX_TYPES];      /* mean squared displacement per type [nm^2] */
     int64_t  count[RDGPU_MAX_TYPES];    /* particles per type                        */
     int64_t  step;                      /* steps done since rdgpu_set_particles      */
-    int32_t  cell_cap;                  /* current slots per cell                    */
-    int32_t  overflow_regrows;          /* times the cap was grown and a step redone */
+    int32_t  neighbour_mode;            /* RDGPU_NB_CELLS or RDGPU_NB_LIST in effect */
+    int32_t  list_builds;               /* pair-list builds so far                   */
+    double   skin;                      /* pair-list skin in effect [nm], 0: cells   */
+    int32_t  list_capacity;             /* pair-list slots per particle              */
+    int32_t  reserved;
 } rdgpu_metrics;
 
 typedef struct rdgpu_engine* rdgpu_handle;
@@ -269,11 +281,19 @@ void* rdgpu_stream(rdgpu_handle h);
 int64_t rdgpu_launch_count(rdgpu_handle h);
 
 /* Runs nsteps steps one launch at a time (no CUDA graph) with CUDA events on
-   the handle's stream around the fused step kernel and around the counting
-   sort (scan + scatter), and returns their mean duration per step in
-   milliseconds.  The state advances exactly as with rdgpu_step.  No
-   reference counterpart (measurement hook).                                  */
+   the handle's stream around the step kernel and around what follows it in
+   the step: the counting sort (scan + scatter) of the cell walk, or the
+   re-sort and list build of the pair list (no-ops in steps that need no
+   rebuild).  Returns their mean duration per step in milliseconds.  The
+   state advances exactly as with rdgpu_step.  No reference counterpart
+   (measurement hook).                                                        */
 int rdgpu_step_profile(rdgpu_handle h, int64_t nsteps, double* step_kernel_ms, double* sort_ms);
+
+/* Runs the neighbour-search autotuner of an RDGPU_NB_AUTO handle now, on its
+   current particles, instead of at its first long rdgpu_step; a no-op for
+   other handles and once tuned.  The state and step count are unchanged.  No
+   reference counterpart.                                                     */
+int rdgpu_autotune(rdgpu_handle h);
 
 #ifdef __cplusplus
 }

@@ -70,17 +70,19 @@ class Box(C.Structure):
                 ("periodic", C.c_int32 * 3), ("seed", C.c_uint64)]
 
 
+NB_AUTO, NB_CELLS, NB_LIST = 0, 1, 2
+
+
 class Options(C.Structure):
-    _fields_ = [("precision", C.c_int32), ("device", C.c_int32), ("cell_cap", C.c_int32),
-                ("lanes_per_particle", C.c_int32), ("cells_per_lane", C.c_int32),
-                ("block_size", C.c_int32), ("graph_steps", C.c_int32),
-                ("kernel_variant", C.c_int32), ("seed", C.c_uint64)]
+    _fields_ = [("precision", C.c_int32), ("device", C.c_int32), ("neighbour_mode", C.c_int32),
+                ("graph_steps", C.c_int32), ("skin", C.c_double), ("seed", C.c_uint64)]
 
 
 class Metrics(C.Structure):
     _fields_ = [("energy", C.c_double), ("msd", C.c_double * MAX_TYPES),
                 ("count", C.c_int64 * MAX_TYPES), ("step", C.c_int64),
-                ("cell_cap", C.c_int32), ("overflow_regrows", C.c_int32)]
+                ("neighbour_mode", C.c_int32), ("list_builds", C.c_int32), ("skin", C.c_double),
+                ("list_capacity", C.c_int32), ("reserved", C.c_int32)]
 
 
 # C-ABI functions and their signatures: (name, restype, argtypes)
@@ -111,6 +113,7 @@ FUNCTIONS = [
     ("rdgpu_stream", C.c_void_p, [P]),
     ("rdgpu_launch_count", C.c_int64, [P]),
     ("rdgpu_step_profile", C.c_int, [P, C.c_int64, DP, DP]),
+    ("rdgpu_autotune", C.c_int, [P]),
     ("rdgpu_rdf_counts_noalloc", C.c_int, [P, P, C.c_int64, C.c_int32, DP, DP, I32P, C.c_int32, C.c_double,
                                            P, P]),
 ]

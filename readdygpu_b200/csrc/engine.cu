@@ -51,10 +51,9 @@ struct rdgpu_engine {
     long long npart_tot = 0, cap_particles = 0;
     std::vector<long long> part_off;     // n_sys + 1
     std::vector<int> types_h;            // by global index
-    void* curA = nullptr;                // FP32: pos, FP64: records
-    void* curB = nullptr;                // FP32: aux
-    void* stgA = nullptr;
-    void* stgB = nullptr;
+    void* bufA[2] = {nullptr, nullptr};  // two state buffers; FP32: pos, FP64: records
+    void* bufB[2] = {nullptr, nullptr};  // FP32: aux
+    int cur = 0;                         // the buffer that holds the current state
     int* tcell = nullptr;
     int* tslot = nullptr;
     unsigned short* sys_of = nullptr;
@@ -79,8 +78,26 @@ struct rdgpu_engine {
     int rdf_nbins = 0;
     double rdf_rmax = 0.0;
     long long rdf_frames = 0;
-    // CUDA graph of graph_steps steps
+    // neighbour search
+    int nb_req = RDGPU_NB_AUTO;          // requested mode
+    int nb_mode = RDGPU_NB_CELLS;        // mode in effect
+    double skin_req = 0.0;               // requested pair-list skin (0: automatic)
+    double skin = 0.0;                   // pair-list skin in effect
+    double max_rc = 0.0;                 // largest pair cutoff
+    double cell_cut = 0.0;               // lower bound of the cell edge of the current grid
+    bool tuned = false;
+    ListCtl* ctl = nullptr;
+    ListCtl* pinned_ctl = nullptr;
+    int nbuild_h = 0;
+    int* nbr = nullptr;                  // pair lists, list_cap x list_stride
+    float4* xref = nullptr;              // positions at the build and list lengths
+    cudaStream_t stream2 = nullptr;      // captures the re-sort into conditional graph nodes
+    bool capturing = false;
+    long long list_stride = 0;
+    int list_cap = 0;
+    // CUDA graphs of graph_steps steps: cell walk, pair list
     cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t lgraph = nullptr;
     int graph_steps = 100;
     long long launches = 0;
     std::string last_error;
@@ -236,9 +253,26 @@ template <class R> void build_ext(const rdgpu_system_desc& d, const rdgpu_box& b
 // ---------------------------------------------------------------------------
 // buffers
 // ---------------------------------------------------------------------------
+void drop_graphs(Engine* E)
+{
+    if (E->graph) { cudaGraphExecDestroy(E->graph); E->graph = nullptr; }
+    if (E->lgraph) { cudaGraphExecDestroy(E->lgraph); E->lgraph = nullptr; }
+}
+
+// the current state moved to buffer c; the cell-walk graph captured the old one
+void set_cur(Engine* E, int c)
+{
+    if (c != E->cur && E->graph) { cudaGraphExecDestroy(E->graph); E->graph = nullptr; }
+    E->cur = c;
+}
+
 void free_particles(Engine* E)
 {
-    dfree(E->curA); dfree(E->curB); dfree(E->stgA); dfree(E->stgB); dfree(E->tcell); dfree(E->tslot);
+    for (int b = 0; b < 2; ++b) { dfree(E->bufA[b]); dfree(E->bufB[b]); }
+    dfree(E->tcell); dfree(E->tslot);
+    dfree(E->nbr); dfree(E->xref);
+    E->list_stride = 0;
+    E->list_cap = 0;
     dfree(E->sys_of); dfree(E->x0_d); dfree(E->vec_d); dfree(E->val_d); dfree(E->ityp_d); dfree(E->u64_d);
     E->cap_particles = 0;
 }
@@ -248,16 +282,15 @@ int ensure_particle_buffers(Engine* E, long long ntot)
 {
     const long long N = std::max<long long>(ntot, 1);
     if (N <= E->cap_particles) return RDGPU_OK;
-    if (E->graph) { cudaGraphExecDestroy(E->graph); E->graph = nullptr; }
+    drop_graphs(E);
     free_particles(E);
     const long long M = N + N / 4;      // headroom for reactions adding particles
     const size_t rec = E->prec == RDGPU_PREC_F32C ? 16 : 32;
-    CK(cudaMalloc(&E->curA, M * rec));
-    CK(cudaMalloc(&E->stgA, M * rec));
-    if (E->prec == RDGPU_PREC_F32C) {
-        CK(cudaMalloc(&E->curB, M * 16));
-        CK(cudaMalloc(&E->stgB, M * 16));
+    for (int b = 0; b < 2; ++b) {
+        CK(cudaMalloc(&E->bufA[b], M * rec));
+        if (E->prec == RDGPU_PREC_F32C) CK(cudaMalloc(&E->bufB[b], M * 16));
     }
+    E->cur = 0;
     CK(cudaMalloc(&E->tcell, M * sizeof(int)));
     CK(cudaMalloc(&E->tslot, M * sizeof(int)));
     CK(cudaMalloc(&E->sys_of, M * sizeof(unsigned short)));
@@ -278,6 +311,9 @@ template <class R> State<R> state(void* A, void* B)
     return s;
 }
 
+template <class R> State<R> cur_state(Engine* E) { return state<R>(E->bufA[E->cur], E->bufB[E->cur]); }
+template <class R> State<R> stg_state(Engine* E) { return state<R>(E->bufA[E->cur ^ 1], E->bufB[E->cur ^ 1]); }
+
 template <class R> Args<R> make_args(Engine* E)
 {
     Args<R> a;
@@ -289,8 +325,8 @@ template <class R> Args<R> make_args(Engine* E)
     a.n_ext = E->n_ext;
     a.tab = (const TypeTab<R>*)E->tab_d;
     a.ext = (const ExtTerm<R>*)E->ext_d;
-    a.cur = state<R>(E->curA, E->curB);
-    a.stg = state<R>(E->stgA, E->stgB);
+    a.cur = cur_state<R>(E);
+    a.stg = stg_state<R>(E);
     a.start = E->start;
     a.counts = E->counts;
     a.tcell = E->tcell;
@@ -312,13 +348,13 @@ int grid_for(long long n, int block = 256)
 // scan + scatter of the staging arrays (tcell/tslot/counts filled)
 template <class R> void launch_sort(Engine* E)
 {
-    scan_tiles_kernel<<<E->ntiles, SCAN_BLOCK, 0, E->stream>>>(E->counts, E->ncells_tot, E->tile_sum, E->err);
+    scan_tiles_kernel<<<E->ntiles, SCAN_BLOCK, 0, E->stream>>>(E->counts, E->ncells_tot, E->tile_sum, E->err,
+                                                               nullptr);
     scan_apply_kernel<<<E->ntiles, SCAN_BLOCK, 0, E->stream>>>(E->counts, E->ncells_tot, E->tile_sum, E->ntiles,
-                                                               E->start, E->err);
+                                                               E->start, E->err, nullptr);
     if (E->npart_tot > 0)
         scatter_kernel<R><<<grid_for(E->npart_tot), 256, 0, E->stream>>>(
-            state<R>(E->stgA, E->stgB), state<R>(E->curA, E->curB), E->tcell, E->tslot, E->start, E->npart_tot,
-            E->err);
+            stg_state<R>(E), cur_state<R>(E), E->tcell, E->tslot, E->start, E->npart_tot, E->err);
     E->launches += (E->npart_tot > 0) ? 3 : 2;
 }
 
@@ -383,7 +419,7 @@ template <class R> int capture_graph(Engine* E)
     return RDGPU_OK;
 }
 
-template <class R> int do_steps(Engine* E, long long nsteps, const double* noise_d)
+template <class R> int do_steps_cells(Engine* E, long long nsteps, const double* noise_d)
 {
     const long long target = E->step_h + nsteps;
     long long remaining = nsteps;
@@ -421,6 +457,466 @@ template <class R> int do_steps(Engine* E, long long nsteps, const double* noise
     return fail(E, RDGPU_ERR_JUMP, "a particle moved more than a box length at step " + std::to_string(tf));
 }
 
+// box edge as the engine stores it
+double edge(const Engine* E, int s, int a)
+{
+    return E->prec == RDGPU_PREC_F32C ? (double)E->sys_h[s].Lf[a] : E->sys_h[s].L[a];
+}
+
+int cells_along(double Lp, double cut)
+{
+    if (!(cut > 0.0)) return 1;
+    double q = std::floor(Lp / (cut * (1.0 + 1e-5)));
+    return (int)std::max(1.0, std::min(q, 2048.0));
+}
+
+// (Re)builds the cell grids of all systems with cell edges >= cut; the
+// particles must be re-sorted afterwards.
+int configure_cells(Engine* E, double cut, std::string& why)
+{
+    long long cb = 0;
+    bool vi = false;
+    for (int s = 0; s < E->nsys; ++s) {
+        SysDev& v = E->sys_h[s];
+        long long nc = 1;
+        for (int a = 0; a < 3; ++a) {
+            const double Lp = edge(E, s, a);
+            const int n = cells_along(Lp, cut);
+            v.n[a] = n;
+            v.invcf[a] = (float)((double)n / (double)v.Lf[a]);
+            v.invc[a] = (double)n / Lp;
+            nc *= n;
+            if (v.per[a] && n < 3) vi = true;
+        }
+        if (nc > (1LL << 26)) { why = "too many cells in one system (box / cutoff too large)"; return RDGPU_ERR_ARG; }
+        v.ncells = (int)nc;
+        v.cell_base = cb;
+        v.slot_base = 0;
+        cb += nc;
+    }
+    if (cb >= 0x7fffffffLL) { why = "too many cells in the batch"; return RDGPU_ERR_ARG; }
+    drop_graphs(E);
+    const int ntiles = (int)((cb + SCAN_TILE - 1) / SCAN_TILE);
+    if (cb > E->ncells_tot || !E->start) {
+        dfree(E->start); dfree(E->counts); dfree(E->tile_sum);
+        if (cudaMalloc(&E->start, (cb + 1) * sizeof(int)) != cudaSuccess ||
+            cudaMalloc(&E->counts, std::max<long long>(cb, 1) * sizeof(int)) != cudaSuccess ||
+            cudaMalloc(&E->tile_sum, std::max(ntiles, 1) * sizeof(int)) != cudaSuccess) {
+            why = "device allocation failed";
+            return RDGPU_ERR_NOMEM;
+        }
+    }
+    E->ncells_tot = cb;
+    E->ntiles = ntiles;
+    E->value_image = vi;
+    E->cell_cut = cut;
+    cudaMemsetAsync(E->start, 0, (cb + 1) * sizeof(int), E->stream);
+    cudaMemsetAsync(E->counts, 0, std::max<long long>(cb, 1) * sizeof(int), E->stream);
+    cudaMemcpyAsync(E->sys_d, E->sys_h.data(), E->nsys * sizeof(SysDev), cudaMemcpyHostToDevice, E->stream);
+    if (cudaStreamSynchronize(E->stream) != cudaSuccess) { why = "cell grid upload failed"; return RDGPU_ERR_CUDA; }
+    return RDGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// pair-list mode (list_step_kernel and the re-sort chain; see the kernels)
+// ---------------------------------------------------------------------------
+template <class R> ListArgs<R> make_list_args(Engine* E, bool with_list)
+{
+    ListArgs<R> v;
+    memset(&v, 0, sizeof(v));
+    v.b0 = state<R>(E->bufA[0], E->bufB[0]);
+    v.b1 = state<R>(E->bufA[1], E->bufB[1]);
+    v.ctl = E->ctl;
+    v.nbr = with_list ? E->nbr : nullptr;
+    v.xref = E->xref;
+    v.stride = E->list_stride;
+    v.cap = E->list_cap;
+    // list radius and rebuild threshold.  A pair closer than its cutoff at a
+    // later step was closer than rc_max + 2 th at the build, th being the
+    // largest displacement since; th is kept below skin/2 by a margin for the
+    // FP32 rounding of positions (a few ulp of the largest box edge) and of
+    // the squared distances.
+    const double rl = E->max_rc + E->skin;
+    v.rl2 = (R)(rl * rl * (1.0 + 1e-6));
+    double lmax = 0.0;
+    for (int s = 0; s < E->nsys; ++s)
+        for (int a = 0; a < 3; ++a) lmax = std::max(lmax, E->sys_h[s].L[a]);
+    const double th = 0.5 * E->skin * (1.0 - 2e-3) - 4.0 * lmax * std::ldexp(1.0, -20);
+    v.thr2 = (float)(th > 0 ? th * th : 0.0);
+    return v;
+}
+
+// the skin is usable: positive rebuild threshold and >= 3 cells of edge
+// >= rc_max + skin on every periodic axis of every system
+bool list_eligible(Engine* E, double skin)
+{
+    if (!(skin > 0.0) || !(E->max_rc > 0.0)) return false;
+    double lmax = 0.0;
+    for (int s = 0; s < E->nsys; ++s)
+        for (int a = 0; a < 3; ++a) lmax = std::max(lmax, E->sys_h[s].L[a]);
+    if (0.5 * skin * (1.0 - 2e-3) - 4.0 * lmax * std::ldexp(1.0, -20) < 0.25 * skin) return false;
+    const double cut = std::max(E->desc.cell_size, E->max_rc + skin);
+    for (int s = 0; s < E->nsys; ++s)
+        for (int a = 0; a < 3; ++a)
+            if (E->sys_h[s].per[a] && cells_along(edge(E, s, a), cut) < 3) return false;
+    return true;
+}
+
+int ensure_list(Engine* E, int cap)
+{
+    const long long stride = std::max<long long>(E->cap_particles, 1);
+    if (cap <= E->list_cap && stride == E->list_stride && E->nbr) return RDGPU_OK;
+    cap = std::max(cap, E->list_cap);
+    if (E->lgraph) { cudaGraphExecDestroy(E->lgraph); E->lgraph = nullptr; }
+    dfree(E->nbr); dfree(E->xref);
+    E->list_cap = 0;
+    E->list_stride = 0;
+    CK(cudaMalloc(&E->nbr, (size_t)cap * stride * sizeof(int)));
+    CK(cudaMalloc(&E->xref, stride * sizeof(float4)));
+    E->list_cap = cap;
+    E->list_stride = stride;
+    return RDGPU_OK;
+}
+
+// list capacity from the densest system, x2 for fluctuations and clusters
+int list_cap_estimate(Engine* E)
+{
+    const double rl = E->max_rc + E->skin;
+    double best = 0.0;
+    for (int s = 0; s < E->nsys; ++s) {
+        double vol = 1.0;
+        for (int a = 0; a < 3; ++a) vol *= edge(E, s, a);
+        const double rho = (double)E->sys_h[s].npart / vol;
+        best = std::max(best, rho * 4.0 / 3.0 * 3.14159265358979 * rl * rl * rl);
+    }
+    return (int)std::min(4096.0, std::ceil(2.0 * best) + 16.0);
+}
+
+template <class R> void launch_chain(Engine* E, const Args<R>& a, const ListArgs<R>& v, long long off,
+                                     cudaStream_t st)
+{
+    const long long N = E->npart_tot;
+    list_count_kernel<R><<<grid_for(N), 256, 0, st>>>(a, v, off);
+    scan_tiles_kernel<<<E->ntiles, SCAN_BLOCK, 0, st>>>(E->counts, E->ncells_tot, E->tile_sum, E->err,
+                                                        &E->ctl->need);
+    scan_apply_kernel<<<E->ntiles, SCAN_BLOCK, 0, st>>>(E->counts, E->ncells_tot, E->tile_sum, E->ntiles,
+                                                        E->start, E->err, &E->ctl->need);
+    list_scatter_kernel<R><<<grid_for(N), 256, 0, st>>>(a, v, off);
+    if (v.nbr)
+        list_build_kernel<R, 128><<<(int)((N + 127) / 128), 128, 0, st>>>(a, v, off);
+    list_finish_kernel<<<1, 32, 0, st>>>(E->ctl, E->err);
+}
+
+// Inside a stream capture: the re-sort of a step becomes a conditional graph
+// node whose body (the chain above) runs only when the step raised the
+// rebuild flag, so steps without a rebuild launch two kernels, not eight.
+template <class R> int add_conditional_chain(Engine* E, const Args<R>& a, const ListArgs<R>& v, long long off)
+{
+    cudaStreamCaptureStatus st;
+    unsigned long long id;
+    cudaGraph_t g;
+    const cudaGraphNode_t* deps;
+    size_t nd;
+    CK(cudaStreamGetCaptureInfo(E->stream, &st, &id, &g, &deps, &nd));
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    list_cond_kernel<<<1, 32, 0, E->stream>>>(h, E->ctl, E->err);
+    CK(cudaGetLastError());
+    CK(cudaStreamGetCaptureInfo(E->stream, &st, &id, &g, &deps, &nd));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, nd, &cp));
+    CK(cudaStreamUpdateCaptureDependencies(E->stream, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CK(cudaStreamBeginCaptureToGraph(E->stream2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    launch_chain<R>(E, a, v, off, E->stream2);
+    cudaGraph_t out = nullptr;
+    CK(cudaStreamEndCapture(E->stream2, &out));
+    return RDGPU_OK;
+}
+
+template <class R> void launch_list_step_kernel(Engine* E, const Args<R>& a, const ListArgs<R>& v)
+{
+    const int grid = (int)((E->npart_tot + kStepBlock - 1) / kStepBlock);
+    if (E->hrep)
+        list_step_kernel<R, true, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a, v);
+    else
+        list_step_kernel<R, false, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a, v);
+    ++E->launches;
+}
+
+template <class R> int launch_list_steps(Engine* E, int n, const double* noise_d)
+{
+    Args<R> a = make_args<R>(E);
+    a.noise = noise_d;
+    const ListArgs<R> v = make_list_args<R>(E, true);
+    for (int k = 0; k < n; ++k) {
+        a.step_off = k;
+        launch_list_step_kernel<R>(E, a, v);
+        if (E->capturing) {
+            int rc = add_conditional_chain<R>(E, a, v, k + 1);
+            if (rc) return rc;
+            ++E->launches;
+        } else {
+            launch_chain<R>(E, a, v, k + 1, E->stream);
+            E->launches += v.nbr ? 6 : 5;
+        }
+    }
+    advance_kernel<<<1, 32, 0, E->stream>>>(E->step_d, E->err, n);
+    ++E->launches;
+    CK(cudaGetLastError());
+    return RDGPU_OK;
+}
+
+// device control block and counters for the input of step step_h in buffer cur
+int write_ctl(Engine* E, int need)
+{
+    ListCtl c;
+    c.need = need;
+    c.nreb = (int)((E->cur ^ (int)(E->step_h & 1)) & 1);
+    c.maxcnt = 0;
+    c.nbuild = E->nbuild_h;
+    CK(cudaMemcpyAsync(E->ctl, &c, sizeof(c), cudaMemcpyHostToDevice, E->stream));
+    return reset_counters(E, E->step_h);
+}
+
+int read_back(Engine* E)
+{
+    CK(cudaMemcpyAsync(E->pinned_err, E->err, sizeof(int), cudaMemcpyDeviceToHost, E->stream));
+    CK(cudaMemcpyAsync(E->pinned_step, E->err_step, sizeof(long long), cudaMemcpyDeviceToHost, E->stream));
+    CK(cudaMemcpyAsync(E->pinned_ctl, E->ctl, sizeof(ListCtl), cudaMemcpyDeviceToHost, E->stream));
+    CK(cudaStreamSynchronize(E->stream));
+    E->nbuild_h = E->pinned_ctl->nbuild;
+    return RDGPU_OK;
+}
+
+// Re-sorts the current state (the input of step step_h) by cell into the
+// other buffer and, with_list, builds the pair lists; an overflowing build
+// grows the lists and is redone.
+template <class R> int resort(Engine* E, bool with_list)
+{
+    if (E->npart_tot == 0) return RDGPU_OK;
+    for (int attempt = 0; attempt < 16; ++attempt) {
+        int rc = write_ctl(E, 1);
+        if (rc) return rc;
+        Args<R> a = make_args<R>(E);
+        const ListArgs<R> v = make_list_args<R>(E, with_list);
+        launch_chain<R>(E, a, v, 0, E->stream);
+        E->launches += v.nbr ? 6 : 5;
+        CK(cudaGetLastError());
+        rc = read_back(E);
+        if (rc) return rc;
+        const int ef = *E->pinned_err;
+        if (ef == 0) {
+            set_cur(E, E->cur ^ 1);
+            return reset_counters(E, E->step_h);
+        }
+        if (ef != EF_LISTOVF) return fail(E, RDGPU_ERR_CUDA, "re-sort failed");
+        // the scan cleared the counts; the current state is untouched
+        rc = ensure_list(E, E->pinned_ctl->maxcnt + E->pinned_ctl->maxcnt / 4 + 8);
+        if (rc) return rc;
+    }
+    return fail(E, RDGPU_ERR_CUDA, "pair-list build did not converge");
+}
+
+// switch to the pair list with the given skin (the particles, if any, are
+// re-sorted on the list's cell grid and the lists built)
+template <class R> int enter_list(Engine* E, double skin)
+{
+    std::string why;
+    const double cut = std::max(E->desc.cell_size, E->max_rc + skin);
+    if (E->cell_cut != cut) {
+        int rc = configure_cells(E, cut, why);
+        if (rc) return fail(E, rc, why);
+    }
+    if (E->skin != skin && E->lgraph) { cudaGraphExecDestroy(E->lgraph); E->lgraph = nullptr; }
+    E->skin = skin;
+    E->nb_mode = RDGPU_NB_LIST;
+    if (E->part_off.empty() || E->npart_tot == 0) return RDGPU_OK;
+    int rc = ensure_list(E, list_cap_estimate(E));
+    if (rc) return rc;
+    return resort<R>(E, true);
+}
+
+// switch to the cell walk (particles re-sorted on its grid)
+template <class R> int enter_cells(Engine* E)
+{
+    std::string why;
+    const double cut = std::max(E->desc.cell_size, E->max_rc);
+    const bool regrid = E->cell_cut != cut;
+    if (regrid) {
+        int rc = configure_cells(E, cut, why);
+        if (rc) return fail(E, rc, why);
+    }
+    const bool was_list = E->nb_mode == RDGPU_NB_LIST;
+    E->nb_mode = RDGPU_NB_CELLS;
+    if (E->part_off.empty() || E->npart_tot == 0) return RDGPU_OK;
+    if (regrid || was_list) return resort<R>(E, false);
+    return RDGPU_OK;
+}
+
+template <class R> int capture_list_graph(Engine* E)
+{
+    if (E->lgraph) return RDGPU_OK;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(E->stream, cudaStreamCaptureModeThreadLocal));
+    long long l0 = E->launches;
+    E->capturing = true;
+    int rc = launch_list_steps<R>(E, E->graph_steps, nullptr);
+    E->capturing = false;
+    cudaError_t ce = cudaStreamEndCapture(E->stream, &g);
+    E->launches = l0;
+    if (rc) return rc;
+    CK(ce);
+    CK(cudaGraphInstantiate(&E->lgraph, g, 0));
+    cudaGraphDestroy(g);
+    return RDGPU_OK;
+}
+
+template <class R> int do_steps_list(Engine* E, long long nsteps, const double* noise_d)
+{
+    const long long target = E->step_h + nsteps;
+    while (E->step_h < target) {
+        long long remaining = target - E->step_h;
+        int rc = write_ctl(E, 0);
+        if (rc) return rc;
+        const long long per_graph = (long long)E->graph_steps * 2 + 1;
+        const int nb0 = E->nbuild_h;
+        if (E->graph_steps > 0 && !noise_d && remaining >= E->graph_steps) {
+            rc = capture_list_graph<R>(E);
+            if (rc) return rc;
+            const long long ng = remaining / E->graph_steps;
+            for (long long g = 0; g < ng; ++g) {
+                CK(cudaGraphLaunch(E->lgraph, E->stream));
+                E->launches += per_graph;
+            }
+            remaining -= ng * E->graph_steps;
+            // the re-sorts that ran inside the graphs (six kernels each)
+            rc = read_back(E);
+            if (rc) return rc;
+            E->launches += 6LL * std::max(0, E->nbuild_h - nb0);
+        }
+        // the rest, after the graphs (the step counter and parity carry over on the device)
+        while (remaining > 0) {
+            const int n = (int)std::min<long long>(remaining, 1000);
+            rc = launch_list_steps<R>(E, n, noise_d);
+            if (rc) return rc;
+            remaining -= n;
+        }
+        rc = read_back(E);
+        if (rc) return rc;
+        const int ef = *E->pinned_err;
+        const int nreb = E->pinned_ctl->nreb;
+        if (ef == 0) {
+            E->step_h = target;
+            set_cur(E, (int)((target + nreb) & 1));
+            return RDGPU_OK;
+        }
+        // the input of step tf is intact in buffer (tf + nreb) & 1
+        const long long tf = *E->pinned_step;
+        E->step_h = tf;
+        set_cur(E, (int)((tf + nreb) & 1));
+        if (ef == EF_LISTOVF) {
+            rc = ensure_list(E, E->pinned_ctl->maxcnt + E->pinned_ctl->maxcnt / 4 + 8);
+            if (rc) return rc;
+            rc = resort<R>(E, true);
+            if (rc) return rc;
+            continue;
+        }
+        rc = prepare_step_state(E, tf);
+        if (rc) return rc;
+        if (ef & EF_NONFINITE)
+            return fail(E, RDGPU_ERR_NONFINITE, "a particle position became non-finite at step " + std::to_string(tf));
+        return fail(E, RDGPU_ERR_JUMP, "a particle moved more than a box length at step " + std::to_string(tf));
+    }
+    return RDGPU_OK;
+}
+
+template <class R> int do_steps_mode(Engine* E, long long nsteps, const double* noise_d)
+{
+    return E->nb_mode == RDGPU_NB_LIST ? do_steps_list<R>(E, nsteps, noise_d) : do_steps_cells<R>(E, nsteps, noise_d);
+}
+
+// The autotuner: times the cell walk and the pair list at a few skins on the
+// handle's own particles (graph_steps steps each after as many warm-up
+// steps, from a snapshot of the state that is restored afterwards) and keeps
+// the fastest.  The trajectory does not depend on the choice: the noise is
+// keyed by the step, and the FP32 forces are identical in both modes.
+template <class R> int tune(Engine* E)
+{
+    E->tuned = true;
+    const long long N = E->npart_tot;
+    if (N == 0 || E->graph_steps <= 0) return RDGPU_OK;
+    const size_t recA = sizeof(R) == 4 ? 16 : 32;
+    void* snapA = nullptr;
+    void* snapB = nullptr;
+    CK(cudaMalloc(&snapA, N * recA));
+    if (sizeof(R) == 4) CK(cudaMalloc(&snapB, N * 16));
+    const long long step0 = E->step_h;
+    auto snap = [&](bool save) -> int {
+        void* a = E->bufA[E->cur];
+        void* b = E->bufB[E->cur];
+        CK(cudaMemcpyAsync(save ? snapA : a, save ? a : snapA, N * recA, cudaMemcpyDeviceToDevice, E->stream));
+        if (sizeof(R) == 4) CK(cudaMemcpyAsync(save ? snapB : b, save ? b : snapB, N * 16, cudaMemcpyDeviceToDevice, E->stream));
+        CK(cudaStreamSynchronize(E->stream));
+        return RDGPU_OK;
+    };
+    int rc = snap(true);
+    std::vector<double> skins = {0.0};
+    for (double f : {0.1, 0.2, 0.35, 0.5})
+        if (list_eligible(E, f * E->max_rc)) skins.push_back(f * E->max_rc);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best_ms = 1e300, best_skin = 0.0;
+    for (size_t c = 0; c < skins.size() && rc == RDGPU_OK; ++c) {
+        // restore the snapshot as the input of step step0, sorted for the candidate
+        rc = snap(false);
+        if (rc) break;
+        E->step_h = step0;
+        rc = prepare_step_state(E, step0);
+        if (rc) break;
+        // the snapshot is sorted for the grid it was taken on; re-sort on the candidate's
+        rc = skins[c] > 0.0 ? enter_list<R>(E, skins[c]) : (E->nb_mode = RDGPU_NB_LIST, enter_cells<R>(E));
+        if (rc) break;
+        // a trial that fails (the dynamics itself, e.g. a particle leaving the
+        // box) disqualifies the candidate; the real run reports the failure
+        if (do_steps_mode<R>(E, E->graph_steps, nullptr) != RDGPU_OK) continue;
+        cudaEventRecord(e0, E->stream);
+        const int trial = do_steps_mode<R>(E, E->graph_steps, nullptr);
+        cudaEventRecord(e1, E->stream);
+        cudaEventSynchronize(e1);
+        if (trial != RDGPU_OK) continue;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) { best_ms = ms; best_skin = skins[c]; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const int rs = snap(false);
+    if (rc == RDGPU_OK) rc = rs;
+    cudaFree(snapA);
+    if (snapB) cudaFree(snapB);
+    if (rc) return rc;
+    E->step_h = step0;
+    rc = prepare_step_state(E, step0);
+    if (rc) return rc;
+    return best_skin > 0.0 ? enter_list<R>(E, best_skin) : (E->nb_mode = RDGPU_NB_LIST, enter_cells<R>(E));
+}
+
+template <class R> int do_steps(Engine* E, long long nsteps, const double* noise_d)
+{
+    if (E->nb_req == RDGPU_NB_AUTO && !E->tuned && !noise_d && nsteps >= 4LL * std::max(E->graph_steps, 1)) {
+        int rc = tune<R>(E);
+        if (rc) return rc;
+    }
+    return do_steps_mode<R>(E, nsteps, noise_d);
+}
+
 int setup_systems(Engine* E, std::string& why)
 {
     const rdgpu_system_desc& d = E->desc;
@@ -438,14 +934,13 @@ int setup_systems(Engine* E, std::string& why)
         build_tab<double>(d, *(TypeTab<double>*)tabbuf.data(), max_rc, why, bad);
     }
     if (bad) return -1;
-    double cut = d.cell_size > 0.0 ? d.cell_size : max_rc;
+    E->max_rc = max_rc;
     if (d.cell_size > 0.0 && d.cell_size < max_rc) { why = "cell_size is smaller than the largest pair cutoff"; return -1; }
     E->sys_h.assign(E->nsys, SysDev{});
     for (int s = 0; s < E->nsys; ++s) {
         const rdgpu_box& b = E->boxes[s];
         SysDev& v = E->sys_h[s];
         memset(&v, 0, sizeof(v));
-        long long nc = 1;
         for (int a = 0; a < 3; ++a) {
             double L = b.hi[a] - b.lo[a];
             if (!(L > 0)) { why = "box bounds must satisfy hi > lo"; return -1; }
@@ -455,24 +950,13 @@ int setup_systems(Engine* E, std::string& why)
                 why = "periodic box edge shorter than twice the pair cutoff (minimum image)";
                 return -1;
             }
-            int n = 1;
-            if (cut > 0.0) {
-                double q = std::floor(Lp / (cut * (1.0 + 1e-5)));
-                n = (int)std::max(1.0, std::min(q, 2048.0));
-            }
-            v.n[a] = n;
             v.per[a] = b.periodic[a] ? 1 : 0;
             v.Lf[a] = Lf;
             v.halff[a] = 0.5f * Lf;
-            v.invcf[a] = (float)((double)n / (double)Lf);
             v.L[a] = L;
             v.half[a] = 0.5 * L;
-            v.invc[a] = (double)n / Lp;
             v.lo[a] = b.lo[a];
-            nc *= n;
         }
-        if (nc > (1LL << 26)) { why = "too many cells in one system (box / cutoff too large)"; return -1; }
-        v.ncells = (int)nc;
         v.cap_log2 = 0;
         v.seed = b.seed;
         v.lanes_log2 = 0;
@@ -492,8 +976,50 @@ int setup_systems(Engine* E, std::string& why)
     return 0;
 }
 
+template <class R> int profile_list(Engine* E, long long nsteps, double* kms, double* sms)
+{
+    int rc = write_ctl(E, 0);
+    if (rc) return rc;
+    cudaEvent_t e0, e1, e2;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventCreate(&e2));
+    Args<R> a = make_args<R>(E);
+    const ListArgs<R> v = make_list_args<R>(E, true);
+    double tk = 0.0, ts = 0.0;
+    for (long long k = 0; k < nsteps; ++k) {
+        a.step_off = 0;
+        CK(cudaEventRecord(e0, E->stream));
+        launch_list_step_kernel<R>(E, a, v);
+        CK(cudaEventRecord(e1, E->stream));
+        launch_chain<R>(E, a, v, 1, E->stream);
+        E->launches += 6;
+        CK(cudaEventRecord(e2, E->stream));
+        advance_kernel<<<1, 32, 0, E->stream>>>(E->step_d, E->err, 1);
+        ++E->launches;
+        CK(cudaEventSynchronize(e2));
+        float m1 = 0.f, m2 = 0.f;
+        cudaEventElapsedTime(&m1, e0, e1);
+        cudaEventElapsedTime(&m2, e1, e2);
+        tk += m1;
+        ts += m2;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    rc = read_back(E);
+    if (rc) return rc;
+    if (*E->pinned_err) return fail(E, RDGPU_ERR_JUMP, "a step failed during profiling");
+    E->step_h += nsteps;
+    set_cur(E, (int)((E->step_h + E->pinned_ctl->nreb) & 1));
+    if (kms) *kms = tk / nsteps;
+    if (sms) *sms = ts / nsteps;
+    return RDGPU_OK;
+}
+
 template <class R> int profile_impl(Engine* E, long long nsteps, double* kms, double* sms)
 {
+    if (E->nb_mode == RDGPU_NB_LIST) return profile_list<R>(E, nsteps, kms, sms);
     cudaEvent_t e0, e1, e2;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -547,6 +1073,7 @@ template <class R> int set_particles_impl(Engine* E, const long long* offsets, l
     }
     if (ntot > 0x7fffffff) return fail(E, RDGPU_ERR_ARG, "at most 2^31-1 particles per handle");
     E->part_off.clear();   // no valid state until this call completes
+    if (ntot != E->npart_tot) drop_graphs(E);   // launch shapes depend on the particle count
     int rc = ensure_particle_buffers(E, ntot);
     if (rc) return rc;
     std::vector<unsigned short> so(std::max<long long>(ntot, 1));
@@ -564,7 +1091,7 @@ template <class R> int set_particles_impl(Engine* E, const long long* offsets, l
         CK(cudaMemcpyAsync(E->vec_d, xyz, ntot * 3 * sizeof(double), cudaMemcpyHostToDevice, E->stream));
         CK(cudaMemcpyAsync(E->ityp_d, types, ntot * sizeof(int), cudaMemcpyHostToDevice, E->stream));
         ingest_kernel<R><<<grid_for(ntot), 256, 0, E->stream>>>(E->sys_d, E->sys_of, ntot, E->vec_d, E->ityp_d,
-                                                                E->desc.n_types, state<R>(E->stgA, E->stgB),
+                                                                E->desc.n_types, stg_state<R>(E),
                                                                 E->tcell, E->tslot, E->counts, E->x0_d, E->err);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(E->pinned_err, E->err, sizeof(int), cudaMemcpyDeviceToHost, E->stream));
@@ -584,6 +1111,11 @@ template <class R> int set_particles_impl(Engine* E, const long long* offsets, l
     rc = prepare_step_state(E, 0);
     if (rc) return rc;
     E->part_off = off;
+    if (E->nb_mode == RDGPU_NB_LIST && ntot > 0) {
+        rc = ensure_list(E, list_cap_estimate(E));
+        if (!rc) rc = resort<R>(E, true);
+        if (rc) { E->part_off.clear(); return rc; }
+    }
     return RDGPU_OK;
 }
 
@@ -591,7 +1123,7 @@ template <class R> int get_particles_impl(Engine* E, double* xyz, int* types)
 {
     const long long N = E->npart_tot;
     if (N == 0) return RDGPU_OK;
-    emit_kernel<R><<<grid_for(N), 256, 0, E->stream>>>(E->sys_d, E->sys_of, N, state<R>(E->curA, E->curB), E->vec_d,
+    emit_kernel<R><<<grid_for(N), 256, 0, E->stream>>>(E->sys_d, E->sys_of, N, cur_state<R>(E), E->vec_d,
                                                        E->ityp_d);
     CK(cudaGetLastError());
     if (xyz) CK(cudaMemcpyAsync(xyz, E->vec_d, N * 3 * sizeof(double), cudaMemcpyDeviceToHost, E->stream));
@@ -609,8 +1141,17 @@ template <class R, int MODE> void launch_diag(Engine* E, double* f, double* e, i
         diag_kernel<R, MODE, false><<<grid_for(E->npart_tot), 256, 0, E->stream>>>(a, f, e, c, h);
 }
 
+// the diagnostics walk the cells: in pair-list mode re-sort first (the
+// particles have moved since the last build)
+template <class R> int fresh_cells(Engine* E)
+{
+    return E->nb_mode == RDGPU_NB_LIST ? resort<R>(E, true) : RDGPU_OK;
+}
+
 template <class R> int forces_impl(Engine* E, double* forces, double* energy)
 {
+    int rc = fresh_cells<R>(E);
+    if (rc) return rc;
     launch_diag<R, 1>(E, E->vec_d, E->val_d, nullptr, nullptr);
     CK(cudaGetLastError());
     if (forces) CK(cudaMemcpyAsync(forces, E->vec_d, E->npart_tot * 3 * sizeof(double), cudaMemcpyDeviceToHost, E->stream));
@@ -625,6 +1166,8 @@ template <class R> int forces_impl(Engine* E, double* forces, double* energy)
 
 template <class R> int digest_impl(Engine* E, int* counts, unsigned long long* hashes)
 {
+    int rc = fresh_cells<R>(E);
+    if (rc) return rc;
     launch_diag<R, 2>(E, nullptr, nullptr, E->ityp_d, E->u64_d);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(counts, E->ityp_d, E->npart_tot * sizeof(int), cudaMemcpyDeviceToHost, E->stream));
@@ -658,6 +1201,8 @@ template <class R> int rdf_impl(Engine* E, int nbins, double rmax, int accumulat
 {
     const int S = E->desc.n_types;
     const int H = S * S * nbins;
+    int rc = fresh_cells<R>(E);
+    if (rc) return rc;
     if (E->rdf_nbins != nbins || E->rdf_rmax != rmax) {
         dfree(E->rdf_acc); dfree(E->rdf_tmp); dfree(E->rdf_e2);
         CK(cudaMalloc(&E->rdf_acc, H * sizeof(unsigned long long)));
@@ -677,7 +1222,7 @@ template <class R> int rdf_impl(Engine* E, int nbins, double rmax, int accumulat
     const int use_smem = (H * 4 <= 48 * 1024) ? 1 : 0;
     if (E->npart_tot > 0) {
         rdf_kernel<R><<<grid_for(E->npart_tot, 128), 128, use_smem ? H * 4 : 0, E->stream>>>(
-            E->sys_d, E->sys_of, E->npart_tot, state<R>(E->curA, E->curB), E->start, S, nbins, E->rdf_e2,
+            E->sys_d, E->sys_of, E->npart_tot, cur_state<R>(E), E->start, S, nbins, E->rdf_e2,
             rmax / (double)nbins, use_smem, E->rdf_tmp);
         CK(cudaGetLastError());
     }
@@ -698,7 +1243,7 @@ template <class R> int msd_impl(Engine* E, rdgpu_metrics* m)
 {
     const int S = E->desc.n_types;
     msd_kernel<R><<<grid_for(E->npart_tot), 256, 0, E->stream>>>(E->sys_d, E->sys_of, E->npart_tot,
-                                                                   state<R>(E->curA, E->curB), E->x0_d, E->val_d,
+                                                                   cur_state<R>(E), E->x0_d, E->val_d,
                                                                    E->ityp_d);
     CK(cudaGetLastError());
     typed_sum_kernel<<<S, 256, 256 * 16, E->stream>>>(E->val_d, E->ityp_d, E->npart_tot, S, E->red_d, E->redc_d);
@@ -765,12 +1310,20 @@ int create_impl(const rdgpu_system_desc* desc, int nsys, const rdgpu_box* boxes,
         E->boxes.assign(boxes, boxes + nsys);
     }
     E->graph_steps = o.graph_steps == 0 ? 100 : (o.graph_steps < 0 ? 0 : o.graph_steps);
+    if (o.neighbour_mode < RDGPU_NB_AUTO || o.neighbour_mode > RDGPU_NB_LIST || !(o.skin >= 0.0)) {
+        g_create_error = "invalid neighbour_mode or skin";
+        delete E;
+        return RDGPU_ERR_ARG;
+    }
+    E->nb_req = o.neighbour_mode;
+    E->skin_req = o.skin;
     auto bail = [&](int code, const std::string& msg) {
         g_create_error = msg;
         rdgpu_destroy(E);
         return code;
     };
-    if (cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) != cudaSuccess)
+    if (cudaStreamCreateWithFlags(&E->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&E->stream2, cudaStreamNonBlocking) != cudaSuccess)
         return bail(RDGPU_ERR_CUDA, "cudaStreamCreate failed");
     if (cudaMalloc(&E->sys_d, nsys * sizeof(SysDev)) != cudaSuccess ||
         cudaMalloc(&E->err, sizeof(int)) != cudaSuccess ||
@@ -798,27 +1351,22 @@ int create_impl(const rdgpu_system_desc* desc, int nsys, const rdgpu_box* boxes,
             }
         E->hrep = h;
     }
-    // cells of all systems
-    long long cb = 0;
-    for (int s = 0; s < nsys; ++s) {
-        SysDev& d = E->sys_h[s];
-        d.cell_base = cb;
-        d.slot_base = 0;
-        cb += d.ncells;
-        for (int a = 0; a < 3; ++a)
-            if (d.per[a] && d.n[a] < 3) E->value_image = true;
-    }
-    if (cb >= 0x7fffffffLL) return bail(RDGPU_ERR_ARG, "too many cells in the batch");
-    E->ncells_tot = cb;
-    E->ntiles = (int)((cb + SCAN_TILE - 1) / SCAN_TILE);
-    if (cudaMalloc(&E->start, (cb + 1) * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&E->counts, std::max<long long>(cb, 1) * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&E->tile_sum, std::max(E->ntiles, 1) * sizeof(int)) != cudaSuccess)
+    // cells of all systems, for the cell walk
+    rc = configure_cells(E, std::max(desc->cell_size, E->max_rc), why);
+    if (rc) return bail(rc, why);
+    if (cudaMalloc(&E->ctl, sizeof(ListCtl)) != cudaSuccess ||
+        cudaMallocHost(&E->pinned_ctl, sizeof(ListCtl)) != cudaSuccess)
         return bail(RDGPU_ERR_NOMEM, "device allocation failed");
-    cudaMemsetAsync(E->start, 0, (cb + 1) * sizeof(int), E->stream);
-    cudaMemsetAsync(E->counts, 0, std::max<long long>(cb, 1) * sizeof(int), E->stream);
-    cudaMemcpyAsync(E->sys_d, E->sys_h.data(), nsys * sizeof(SysDev), cudaMemcpyHostToDevice, E->stream);
+    cudaMemsetAsync(E->ctl, 0, sizeof(ListCtl), E->stream);
     if (cudaStreamSynchronize(E->stream) != cudaSuccess) return bail(RDGPU_ERR_CUDA, "initialisation failed");
+    if (E->nb_req == RDGPU_NB_LIST) {
+        // a requested pair list that the boxes cannot hold falls back to the cell walk
+        const double skin = E->skin_req > 0.0 ? E->skin_req : 0.25 * E->max_rc;
+        if (list_eligible(E, skin)) {
+            rc = E->prec == RDGPU_PREC_F32C ? enter_list<float>(E, skin) : enter_list<double>(E, skin);
+            if (rc) return bail(rc, E->last_error);
+        }
+    }
     *out = E;
     return RDGPU_OK;
 }
@@ -844,14 +1392,16 @@ int rdgpu_destroy(rdgpu_handle h)
     if (!E) return RDGPU_ERR_ARG;
     cudaSetDevice(E->device);
     if (E->stream) cudaStreamSynchronize(E->stream);
-    if (E->graph) cudaGraphExecDestroy(E->graph);
+    drop_graphs(E);
     free_particles(E);
     dfree(E->sys_d); dfree(E->tab_d); dfree(E->ext_d); dfree(E->start); dfree(E->counts); dfree(E->tile_sum);
-    dfree(E->err); dfree(E->err_step); dfree(E->step_d);
+    dfree(E->err); dfree(E->err_step); dfree(E->step_d); dfree(E->ctl);
+    if (E->pinned_ctl) cudaFreeHost(E->pinned_ctl);
     dfree(E->red_d); dfree(E->redc_d); dfree(E->rdf_acc); dfree(E->rdf_tmp); dfree(E->rdf_e2);
     if (E->pinned_err) cudaFreeHost(E->pinned_err);
     if (E->pinned_step) cudaFreeHost(E->pinned_step);
     if (E->stream) cudaStreamDestroy(E->stream);
+    if (E->stream2) cudaStreamDestroy(E->stream2);
     delete E;
     return RDGPU_OK;
 }
@@ -1011,8 +1561,10 @@ int rdgpu_metrics_get(rdgpu_handle h, rdgpu_metrics* m)
     if (!m) return fail(E, RDGPU_ERR_ARG, "null output");
     memset(m, 0, sizeof(*m));
     m->step = E->step_h;
-    m->cell_cap = 0;
-    m->overflow_regrows = 0;
+    m->neighbour_mode = E->nb_mode;
+    m->list_builds = E->nbuild_h;
+    m->skin = E->nb_mode == RDGPU_NB_LIST ? E->skin : 0.0;
+    m->list_capacity = E->nb_mode == RDGPU_NB_LIST ? E->list_cap : 0;
     if (E->npart_tot == 0) return RDGPU_OK;
     int rc = rdgpu_forces(h, nullptr, &m->energy);
     if (rc) return rc;
@@ -1032,6 +1584,15 @@ int rdgpu_step_profile(rdgpu_handle h, int64_t nsteps, double* step_kernel_ms, d
     NEED_PARTICLES(E);
     if (nsteps < 1 || E->npart_tot == 0) return fail(E, RDGPU_ERR_ARG, "nsteps >= 1 and particles needed");
     return DISPATCH(E, profile_impl, E, (long long)nsteps, step_kernel_ms, sort_ms);
+}
+
+int rdgpu_autotune(rdgpu_handle h)
+{
+    Engine* E = (Engine*)h;
+    GUARD(E);
+    NEED_PARTICLES(E);
+    if (E->nb_req != RDGPU_NB_AUTO || E->tuned || E->npart_tot == 0) return RDGPU_OK;
+    return DISPATCH(E, tune, E);
 }
 
 int64_t rdgpu_launch_count(rdgpu_handle h)

@@ -613,10 +613,12 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) step_kernel(Arg
 // counting sort: tile sums, exclusive prefix, scatter
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(SCAN_BLOCK) scan_tiles_kernel(const int* __restrict__ counts, long long ncells,
-                                                                int* __restrict__ tile_sum, const int* err)
+                                                                int* __restrict__ tile_sum, const int* err,
+                                                                const int* gate)
 {
     __shared__ int red[SCAN_BLOCK / 32];
     if (*((volatile const int*)err)) return;
+    if (gate && !*((volatile const int*)gate)) return;
     const long long base = (long long)blockIdx.x * SCAN_TILE;
     int sum = 0;
     for (int k = threadIdx.x; k < SCAN_TILE; k += SCAN_BLOCK) {
@@ -638,13 +640,15 @@ __global__ void __launch_bounds__(SCAN_BLOCK) scan_tiles_kernel(const int* __res
 // global access is coalesced.
 __global__ void __launch_bounds__(SCAN_BLOCK) scan_apply_kernel(int* __restrict__ counts, long long ncells,
                                                                 const int* __restrict__ tile_sum, int ntiles,
-                                                                int* __restrict__ start, const int* err)
+                                                                int* __restrict__ start, const int* err,
+                                                                const int* gate)
 {
     constexpr int PER = SCAN_TILE / SCAN_BLOCK;
     __shared__ int s_t[SCAN_TILE + SCAN_TILE / 32];   // padded against bank conflicts
     __shared__ int s_w[SCAN_BLOCK / 32];
     __shared__ int s_base;
     if (*((volatile const int*)err)) return;
+    if (gate && !*((volatile const int*)gate)) return;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const long long base_c = (long long)blockIdx.x * SCAN_TILE;
     // base of this tile: sum of the preceding tile sums
@@ -1044,6 +1048,344 @@ __global__ void typed_sum_kernel(const double* v, const int* types, long long n,
         out[want] = red[0];
         counts[want] = cr[0];
     }
+}
+
+// ---------------------------------------------------------------------------
+// Pair-list mode.
+//
+// The cell walk of step_kernel finds the candidates of every particle again in
+// every step.  In pair-list mode a list of the pairs closer than
+// rl = rc_max + skin is built from the sorted cell layout, and each step
+// evaluates only the listed pairs.  The list stays complete -- every pair
+// closer than its cutoff at a later step is in it -- while no particle has
+// moved more than skin/2 since the build.  The step kernel checks that bound
+// for every particle and raises a flag; the kernels that follow it in the
+// same step (gated on the flag, no-ops otherwise) re-sort the particles by
+// cell and rebuild the list before the next step.  Pair displacements are the
+// minimum image with the same IEEE operations as the cell walk, so the
+// accepted pairs and the FP32 fixed-point forces are identical to the cell
+// walk's.
+//
+// Between builds a particle keeps its sorted index; each step writes the
+// other of two state buffers at the same index, and so does the re-sort.  The
+// buffer that holds the input of step t is (t + nreb) & 1, where the parity
+// bit nreb flips at every re-sort.
+// ---------------------------------------------------------------------------
+constexpr int EF_LISTOVF = 16;
+
+struct ListCtl {
+    int need;        // 1: re-sort and rebuild after this step
+    int nreb;        // parity bit, flipped by every re-sort
+    int maxcnt;      // longest list met by an overflowing build
+    int nbuild;      // builds so far
+};
+
+template <class R> struct ListArgs {
+    State<R> b0, b1;     // the two state buffers
+    ListCtl* ctl;
+    int* nbr;            // nbr[k * stride + i]: k-th partner of sorted particle i; null: sort only
+    float4* xref;        // position of particle i at the build; w: bits of its list length
+    long long stride;
+    int cap;             // list capacity per particle
+    R rl2;               // squared list radius
+    float thr2;          // squared displacement since the build that triggers a rebuild
+};
+
+template <class R>
+__device__ __forceinline__ int list_sel(const Args<R>& a, const ListArgs<R>& v, long long off)
+{
+    const long long t = *((volatile const long long*)a.step_ptr) + off;
+    return (int)((t + (long long)*((volatile const int*)&v.ctl->nreb)) & 1LL);
+}
+
+template <class R>
+__device__ __forceinline__ bool list_gate(const Args<R>& a, const ListArgs<R>& v)
+{
+    return *((volatile const int*)a.err) == 0 && *((volatile const int*)&v.ctl->need) != 0;
+}
+
+__device__ __forceinline__ void store_state(const State<float>& st, long long i, const float x[3], int w,
+                                            const float c[3], int id)
+{
+    st.pos[i] = make_float4(x[0], x[1], x[2], __int_as_float(w));
+    st.aux[i] = make_float4(c[0], c[1], c[2], __int_as_float(id));
+}
+__device__ __forceinline__ void store_state(const State<double>& st, long long i, const double x[3], int w,
+                                            const double* /*c*/, int id)
+{
+    Rec64 r;
+    r.x = x[0]; r.y = x[1]; r.z = x[2]; r.w = w; r.id = id;
+    st.rec[i] = r;
+}
+
+// one BD step of every particle over its pair list
+template <class R, bool HREP, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) list_step_kernel(Args<R> a, ListArgs<R> v)
+{
+    __shared__ R s_rc2[MAXT * MAXT];
+    __shared__ FastTab<R> s_ft;
+    if (*((volatile int*)a.err)) return;   // an earlier step failed: keep its input intact
+    for (int k = threadIdx.x; k < MAXT * MAXT; k += BLOCK) {
+        s_rc2[k] = a.tab->rc2[k];
+        if (HREP) {
+            s_ft.k[k] = a.tab->nterm[k] ? a.tab->term[k * MAX_TERMS].k : R(0);
+            s_ft.r0[k] = a.tab->nterm[k] ? a.tab->term[k * MAX_TERMS].r0 : R(0);
+        }
+    }
+    __syncthreads();
+    const long long t = *((volatile const long long*)a.step_ptr) + a.step_off;
+    const int sel = list_sel(a, v, a.step_off);
+    const State<R> cur = sel ? v.b1 : v.b0;
+    const State<R> nxt = sel ? v.b0 : v.b1;
+    const int i = blockIdx.x * BLOCK + threadIdx.x;
+    if (i >= a.ntot) return;
+    const int si = a.sys_of[i];
+    const SysDev& s = a.sys[si];
+    R xi[3];
+    int wi;
+    load_pos(cur, i, xi, wi);
+    const int ti = wi & 0xff;
+    R c[3] = {R(0), R(0), R(0)};
+    int id;
+    if constexpr (sizeof(R) == 4) {
+        const float4 q = __ldg(cur.aux + i);
+        c[0] = q.x; c[1] = q.y; c[2] = q.z;
+        id = __float_as_int(q.w);
+    } else {
+        id = __ldg(&cur.rec[i].id);
+    }
+    Box<R> bx;
+    bx.load(s);
+    const int p0 = s.per[0], p1 = s.per[1], p2 = s.per[2];
+    Acc<R> acc;
+    acc.zero();
+    const float4 xr = __ldg(v.xref + i);
+    const int cnt = __float_as_int(xr.w);
+    const int* nb = v.nbr + i;
+    // the partners in chunks of LCHUNK: all their indices, then all their
+    // positions are requested before the first pair is evaluated
+    constexpr int LCHUNK = 4;
+    for (int k0 = 0; k0 < cnt; k0 += LCHUNK) {
+        int jj[LCHUNK];
+#pragma unroll
+        for (int u = 0; u < LCHUNK; ++u) jj[u] = (k0 + u < cnt) ? __ldg(nb + (long long)(k0 + u) * v.stride) : -1;
+        R xj[LCHUNK][3];
+        int wj[LCHUNK];
+#pragma unroll
+        for (int u = 0; u < LCHUNK; ++u) {
+            if (jj[u] >= 0) load_pos(cur, jj[u], xj[u], wj[u]);
+            else { xj[u][0] = xj[u][1] = xj[u][2] = R(0); wj[u] = 0; }
+        }
+#pragma unroll
+        for (int u = 0; u < LCHUNK; ++u) {
+            if (jj[u] < 0) continue;
+            const R dx = mimg(xi[0], xj[u][0], bx.L[0], bx.half[0], p0);
+            const R dy = mimg(xi[1], xj[u][1], bx.L[1], bx.half[1], p1);
+            const R dz = mimg(xi[2], xj[u][2], bx.L[2], bx.half[2], p2);
+            const R r2 = dist2(dx, dy, dz);
+            const int pidx = ti * MAXT + (wj[u] & 0xff);
+            if (r2 < s_rc2[pidx]) {
+                if (HREP) {
+                    // pre = k (r - r0) / r; r == 0 has no direction
+                    if (r2 > R(0)) {
+                        R pre;
+                        if constexpr (sizeof(R) == 4) pre = s_ft.k[pidx] * (1.0f - s_ft.r0[pidx] * rsqrtf(r2));
+                        else { const R r = sqrt(r2); pre = s_ft.k[pidx] * (r - s_ft.r0[pidx]) / r; }
+                        acc.add(pre, dx, dy, dz);
+                    }
+                } else {
+                    const R r = sqrt(r2);
+                    const int nt = a.tab->nterm[pidx];
+                    for (int m = 0; m < nt; ++m) {
+                        R pre, e;
+                        pair_term(a.tab->term[pidx * MAX_TERMS + m], r, pre, e);
+                        acc.add(pre, dx, dy, dz);
+                    }
+                }
+            }
+        }
+    }
+    R F[3];
+    acc.force(F);
+    if (a.n_ext > 0) {
+        const ExtTerm<R>* ep = a.ext + (long long)si * a.n_ext;
+        R ee = R(0);
+        for (int e = 0; e < a.n_ext; ++e)
+            if ((ep[e].tmask >> ti) & 1u) ext_force(ep[e], a.tab->prad[ti], xi, F, ee);
+    }
+    R xn[3];
+    if (a.noise) {
+        const double* nz = a.noise + 3 * (s.part_base + id);
+        xn[0] = (R)nz[0]; xn[1] = (R)nz[1]; xn[2] = (R)nz[2];
+    } else {
+        bd_normals(s.seed, t, (long long)id, xn);
+    }
+    const int ef = em_update(xi, c, wi, F, xn, a.tab->a[ti], a.tab->b[ti], s);
+    // displacement since the build, minimum image
+    const float d0 = mimg((float)xi[0], xr.x, s.Lf[0], s.halff[0], p0);
+    const float d1 = mimg((float)xi[1], xr.y, s.Lf[1], s.halff[1], p1);
+    const float d2 = mimg((float)xi[2], xr.z, s.Lf[2], s.halff[2], p2);
+    if (d0 * d0 + d1 * d1 + d2 * d2 > v.thr2) *((volatile int*)&v.ctl->need) = 1;
+    store_state(nxt, i, xi, wi, c, id);
+    if (ef) {
+        atomicOr(a.err, ef);
+        atomicMin((unsigned long long*)a.err_step, (unsigned long long)t);
+    }
+}
+
+// re-sort, part 1: cell and slot of every particle of the current state
+template <class R>
+__global__ void list_count_kernel(Args<R> a, ListArgs<R> v, long long off)
+{
+    if (!list_gate(a, v)) return;
+    const State<R> src = list_sel(a, v, off) ? v.b1 : v.b0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.ntot;
+         i += (long long)gridDim.x * blockDim.x) {
+        const SysDev& s = a.sys[a.sys_of[i]];
+        R x[3];
+        int w;
+        load_pos(src, i, x, w);
+        int c[3];
+        cell_coords(s, x, c);
+        const long long cell = s.cell_base + ((long long)c[2] * s.n[1] + c[1]) * s.n[0] + c[0];
+        a.tslot[i] = atomicAdd(a.counts + cell, 1);
+        a.tcell[i] = (int)cell;
+    }
+}
+
+// re-sort, part 3 (after the scan): scatter into the other buffer
+template <class R>
+__global__ void list_scatter_kernel(Args<R> a, ListArgs<R> v, long long off)
+{
+    if (!list_gate(a, v)) return;
+    const int sel = list_sel(a, v, off);
+    const State<R> src = sel ? v.b1 : v.b0;
+    const State<R> dst = sel ? v.b0 : v.b1;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < a.ntot;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long d = a.start[a.tcell[i]] + a.tslot[i];
+        if constexpr (sizeof(R) == 4) {
+            dst.pos[d] = src.pos[i];
+            dst.aux[d] = src.aux[i];
+        } else {
+            dst.rec[d] = src.rec[i];
+        }
+    }
+}
+
+// appends the pairs of one candidate range closer than rl
+template <class R>
+__device__ __forceinline__ void list_range(const State<R>& st, int j0, int j1, int self, const R xi[3], R sx, R sy,
+                                           R sz, R rl2, int* __restrict__ nb, long long stride, int cap, int& cnt)
+{
+    for (int j = j0; j < j1; ++j) {
+        R xj[3];
+        int wj;
+        load_pos(st, j, xj, wj);
+        const R dx = sub_rn(xi[0], add_rn(xj[0], sx));
+        const R dy = sub_rn(xi[1], add_rn(xj[1], sy));
+        const R dz = sub_rn(xi[2], add_rn(xj[2], sz));
+        if (dist2(dx, dy, dz) < rl2 && j != self) {
+            if (cnt < cap) nb[(long long)cnt * stride] = j;
+            ++cnt;
+        }
+    }
+}
+
+// re-sort, part 4: the pair list of every particle of the re-sorted state,
+// from its 27-cell neighbourhood (every periodic axis has >= 3 cells here)
+template <class R, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) list_build_kernel(Args<R> a, ListArgs<R> v, long long off)
+{
+    if (!list_gate(a, v)) return;
+    const int sel = list_sel(a, v, off);
+    const State<R> st = sel ? v.b0 : v.b1;     // the scatter's destination
+    const int i = blockIdx.x * BLOCK + threadIdx.x;
+    if (i >= a.ntot) return;
+    const SysDev& s = a.sys[a.sys_of[i]];
+    R xi[3];
+    int wi;
+    load_pos(st, i, xi, wi);
+    int c[3];
+    cell_coords(s, xi, c);
+    Box<R> bx;
+    bx.load(s);
+    const int n0 = s.n[0], n1 = s.n[1], n2 = s.n[2];
+    R cw[3], f[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        if constexpr (sizeof(R) == 4) cw[q] = R(1) / s.invcf[q]; else cw[q] = R(1) / s.invc[q];
+        f[q] = xi[q] - (R)c[q] * cw[q];
+    }
+    const R rl2 = v.rl2;
+    const R lim = rl2 * R(1.0001);
+    int* nb = v.nbr + i;
+    int cnt = 0;
+    for (int dz = -1; dz <= 1; ++dz) {
+        const R gz = gap2(dz, f[2], cw[2]);
+        if (gz >= lim) continue;
+        int z = c[2] + dz;
+        R sz = R(0);
+        if (z < 0 || z >= n2) {
+            if (!s.per[2]) continue;
+            sz = z < 0 ? -bx.L[2] : bx.L[2];
+            z = z < 0 ? z + n2 : z - n2;
+        }
+        for (int dy = -1; dy <= 1; ++dy) {
+            const R gyz = gz + gap2(dy, f[1], cw[1]);
+            if (gyz >= lim) continue;
+            int y = c[1] + dy;
+            R sy = R(0);
+            if (y < 0 || y >= n1) {
+                if (!s.per[1]) continue;
+                sy = y < 0 ? -bx.L[1] : bx.L[1];
+                y = y < 0 ? y + n1 : y - n1;
+            }
+            const int row = (int)s.cell_base + (z * n1 + y) * n0;
+            int xa = (gyz + f[0] * f[0] < lim) ? c[0] - 1 : c[0];
+            int xb = (gyz + (cw[0] - f[0]) * (cw[0] - f[0]) < lim) ? c[0] + 1 : c[0];
+            if (!s.per[0]) {
+                xa = max(xa, 0);
+                xb = min(xb, n0 - 1);
+            } else {
+                if (xa < 0) {
+                    list_range<R>(st, a.start[row + n0 - 1], a.start[row + n0], i, xi, -bx.L[0], sy, sz, rl2, nb,
+                                  v.stride, v.cap, cnt);
+                    xa = 0;
+                }
+                if (xb >= n0) {
+                    list_range<R>(st, a.start[row], a.start[row + 1], i, xi, bx.L[0], sy, sz, rl2, nb, v.stride,
+                                  v.cap, cnt);
+                    xb = n0 - 1;
+                }
+            }
+            list_range<R>(st, a.start[row + xa], a.start[row + xb + 1], i, xi, R(0), sy, sz, rl2, nb, v.stride,
+                          v.cap, cnt);
+        }
+    }
+    v.xref[i] = make_float4((float)xi[0], (float)xi[1], (float)xi[2], __int_as_float(min(cnt, v.cap)));
+    if (cnt > v.cap) {
+        atomicMax(&v.ctl->maxcnt, cnt);
+        atomicOr(a.err, EF_LISTOVF);
+        atomicMin((unsigned long long*)a.err_step, (unsigned long long)(*a.step_ptr + off));
+    }
+}
+
+// sets the condition of the graph node that holds the re-sort of this step
+__global__ void list_cond_kernel(cudaGraphConditionalHandle h, const ListCtl* ctl, const int* err)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0)
+        cudaGraphSetConditional(h, (*((volatile const int*)err) == 0 && *((volatile const int*)&ctl->need)) ? 1u : 0u);
+}
+
+// re-sort, part 5: flip the buffer parity, clear the flag
+__global__ void list_finish_kernel(ListCtl* ctl, const int* err)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (*((volatile const int*)err) || !*((volatile const int*)&ctl->need)) return;
+    ctl->nreb ^= 1;
+    ctl->nbuild += 1;
+    ctl->need = 0;
 }
 
 }  // namespace rdgpu

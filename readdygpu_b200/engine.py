@@ -33,18 +33,18 @@ class Engine:
     """One handle: a single system, or a batch of systems sharing types and
     potentials (boxes=[(lo, hi, periodic, seed), ...])."""
 
-    def __init__(self, system, precision="f64", device=0, seed=0, boxes=None, cell_cap=0,
-                 lanes_per_particle=0, cells_per_lane=0, graph_steps=0, kernel_variant=0):
+    NB_MODES = {"auto": A.NB_AUTO, "cells": A.NB_CELLS, "list": A.NB_LIST}
+
+    def __init__(self, system, precision="f64", device=0, seed=0, boxes=None, neighbour_mode="auto",
+                 skin=0.0, graph_steps=0):
         self.system = system
         self._desc = system.to_desc()
         opt = A.Options()
         opt.precision = {"f64": A.PREC_F64, "f32c": A.PREC_F32C}[precision]
         opt.device = device
-        opt.cell_cap = cell_cap
-        opt.lanes_per_particle = lanes_per_particle
-        opt.cells_per_lane = cells_per_lane
+        opt.neighbour_mode = self.NB_MODES[neighbour_mode]
+        opt.skin = skin
         opt.graph_steps = graph_steps
-        opt.kernel_variant = kernel_variant
         opt.seed = seed
         self.precision = precision
         h = C.c_void_p()
@@ -97,6 +97,10 @@ class Engine:
 
     def launch_count(self):
         return _lib().rdgpu_launch_count(self._h)
+
+    def autotune(self):
+        """Run the neighbour-search autotuner now (neighbour_mode="auto")."""
+        self._check(_lib().rdgpu_autotune(self._h))
 
     def step_profile(self, nsteps):
         """Mean ms per step of the fused step kernel and of the counting sort."""
@@ -171,4 +175,5 @@ class Engine:
         self._check(_lib().rdgpu_metrics_get(self._h, C.byref(m)))
         S = self.system.n_types
         return {"energy": m.energy, "msd": list(m.msd[:S]), "count": list(m.count[:S]),
-                "step": m.step, "cell_cap": m.cell_cap, "overflow_regrows": m.overflow_regrows}
+                "step": m.step, "neighbour_mode": {A.NB_CELLS: "cells", A.NB_LIST: "list"}.get(m.neighbour_mode),
+                "list_builds": m.list_builds, "skin": m.skin, "list_capacity": m.list_capacity}
