@@ -290,8 +290,9 @@ int64_t rdgpu_launch_count(rdgpu_handle h);
 int rdgpu_step_profile(rdgpu_handle h, int64_t nsteps, double* step_kernel_ms, double* sort_ms);
 
 /* Runs the neighbour-search autotuner of an RDGPU_NB_AUTO handle now, on its
-   current particles, instead of at its first long rdgpu_step; a no-op for
-   other handles and once tuned.  The state and step count are unchanged.  No
+   current particles, instead of at its first long rdgpu_step (once per
+   handle), then captures the CUDA graph of the mode in effect, so that the
+   next rdgpu_step pays neither.  The state and step count are unchanged.  No
    reference counterpart.                                                     */
 int rdgpu_autotune(rdgpu_handle h);
 

@@ -908,6 +908,13 @@ template <class R> int tune(Engine* E)
     return best_skin > 0.0 ? enter_list<R>(E, best_skin) : (E->nb_mode = RDGPU_NB_LIST, enter_cells<R>(E));
 }
 
+// captures the step graph of the mode in effect (nothing runs)
+template <class R> int prepare_graph(Engine* E)
+{
+    if (E->graph_steps <= 0) return RDGPU_OK;
+    return E->nb_mode == RDGPU_NB_LIST ? capture_list_graph<R>(E) : capture_graph<R>(E);
+}
+
 template <class R> int do_steps(Engine* E, long long nsteps, const double* noise_d)
 {
     if (E->nb_req == RDGPU_NB_AUTO && !E->tuned && !noise_d && nsteps >= 4LL * std::max(E->graph_steps, 1)) {
@@ -1591,8 +1598,12 @@ int rdgpu_autotune(rdgpu_handle h)
     Engine* E = (Engine*)h;
     GUARD(E);
     NEED_PARTICLES(E);
-    if (E->nb_req != RDGPU_NB_AUTO || E->tuned || E->npart_tot == 0) return RDGPU_OK;
-    return DISPATCH(E, tune, E);
+    if (E->npart_tot == 0) return RDGPU_OK;
+    if (E->nb_req == RDGPU_NB_AUTO && !E->tuned) {
+        int rc = DISPATCH(E, tune, E);
+        if (rc) return rc;
+    }
+    return DISPATCH(E, prepare_graph, E);
 }
 
 int64_t rdgpu_launch_count(rdgpu_handle h)
