@@ -95,6 +95,8 @@ struct rdgpu_engine {
     bool capturing = false;
     long long list_stride = 0;
     int list_cap = 0;
+    std::vector<double> rc_h;            // pair cutoff per type pair (0: no potential)
+    void* rl2_d = nullptr;               // squared list radius per type pair, in the state precision
     // CUDA graphs of graph_steps steps: cell walk, pair list
     cudaGraphExec_t graph = nullptr;
     cudaGraphExec_t lgraph = nullptr;
@@ -536,8 +538,9 @@ template <class R> ListArgs<R> make_list_args(Engine* E, bool with_list)
     // largest displacement since; th is kept below skin/2 by a margin for the
     // FP32 rounding of positions (a few ulp of the largest box edge) and of
     // the squared distances.
+    v.rl2t = (const R*)E->rl2_d;
     const double rl = E->max_rc + E->skin;
-    v.rl2 = (R)(rl * rl * (1.0 + 1e-6));
+    v.rl2max = (R)(rl * rl * (1.0 + 1e-6));
     double lmax = 0.0;
     for (int s = 0; s < E->nsys; ++s)
         for (int a = 0; a < 3; ++a) lmax = std::max(lmax, E->sys_h[s].L[a]);
@@ -736,6 +739,20 @@ template <class R> int enter_list(Engine* E, double skin)
     if (E->skin != skin && E->lgraph) { cudaGraphExecDestroy(E->lgraph); E->lgraph = nullptr; }
     E->skin = skin;
     E->nb_mode = RDGPU_NB_LIST;
+    {
+        // list radius per type pair: its own cutoff + skin (the same margin as rl2max)
+        std::vector<double> t(MAXT * MAXT, 0.0);
+        for (int q = 0; q < MAXT * MAXT; ++q)
+            if (E->rc_h[q] > 0.0) t[q] = (E->rc_h[q] + skin) * (E->rc_h[q] + skin) * (1.0 + 1e-6);
+        const size_t rs = E->prec == RDGPU_PREC_F32C ? sizeof(float) : sizeof(double);
+        if (!E->rl2_d) CK(cudaMalloc(&E->rl2_d, MAXT * MAXT * rs));
+        if (E->prec == RDGPU_PREC_F32C) {
+            std::vector<float> f(t.begin(), t.end());
+            CK(cudaMemcpy(E->rl2_d, f.data(), MAXT * MAXT * rs, cudaMemcpyHostToDevice));
+        } else {
+            CK(cudaMemcpy(E->rl2_d, t.data(), MAXT * MAXT * rs, cudaMemcpyHostToDevice));
+        }
+    }
     if (E->part_off.empty() || E->npart_tot == 0) return RDGPU_OK;
     int rc = ensure_list(E, list_cap_estimate(E));
     if (rc) return rc;
@@ -942,6 +959,12 @@ int setup_systems(Engine* E, std::string& why)
     }
     if (bad) return -1;
     E->max_rc = max_rc;
+    E->rc_h.assign(MAXT * MAXT, 0.0);
+    for (int q = 0; q < MAXT * MAXT; ++q) {
+        const double r2 = E->prec == RDGPU_PREC_F32C ? (double)((TypeTab<float>*)tabbuf.data())->rc2[q]
+                                                     : ((TypeTab<double>*)tabbuf.data())->rc2[q];
+        E->rc_h[q] = std::sqrt(r2) * (1.0 + 1e-7);   // at least the cutoff the kernels test against
+    }
     if (d.cell_size > 0.0 && d.cell_size < max_rc) { why = "cell_size is smaller than the largest pair cutoff"; return -1; }
     E->sys_h.assign(E->nsys, SysDev{});
     for (int s = 0; s < E->nsys; ++s) {
@@ -1402,7 +1425,7 @@ int rdgpu_destroy(rdgpu_handle h)
     drop_graphs(E);
     free_particles(E);
     dfree(E->sys_d); dfree(E->tab_d); dfree(E->ext_d); dfree(E->start); dfree(E->counts); dfree(E->tile_sum);
-    dfree(E->err); dfree(E->err_step); dfree(E->step_d); dfree(E->ctl);
+    dfree(E->err); dfree(E->err_step); dfree(E->step_d); dfree(E->ctl); dfree(E->rl2_d);
     if (E->pinned_ctl) cudaFreeHost(E->pinned_ctl);
     dfree(E->red_d); dfree(E->redc_d); dfree(E->rdf_acc); dfree(E->rdf_tmp); dfree(E->rdf_e2);
     if (E->pinned_err) cudaFreeHost(E->pinned_err);

@@ -211,6 +211,17 @@ __device__ __forceinline__ R mimg(R xi, R xj, R L, R half, int per)
     return d;
 }
 
+// The same displacement as mimg, with the image chosen first and one
+// subtraction path: xj + (-L) == xj - L exactly, and xj + 0 == xj up to the
+// sign of a zero (which no force or distance sees).
+template <class R>
+__device__ __forceinline__ R mimg_sel(R xi, R xj, R L, R half, int per)
+{
+    const R d0 = sub_rn(xi, xj);
+    const R s = (per && d0 > half) ? L : ((per && d0 < -half) ? -L : R(0));
+    return sub_rn(xi, add_rn(xj, s));
+}
+
 // r^2 = (dx*dx + dy*dy) + dz*dz, rounded after every operation
 template <class R>
 __device__ __forceinline__ R dist2(R dx, R dy, R dz)

@@ -69,9 +69,11 @@ template <> struct Acc<float> {
     __device__ __forceinline__ void zero() { fx = fy = fz = 0; e = 0.f; }
     __device__ __forceinline__ void add(float pre, float dx, float dy, float dz)
     {
-        fx += __float2ll_rn(-pre * dx * FX_SCALE);
-        fy += __float2ll_rn(-pre * dy * FX_SCALE);
-        fz += __float2ll_rn(-pre * dz * FX_SCALE);
+        // scaling by 2^32 is exact, so (-pre 2^32) d == ((-pre) d) 2^32
+        const float q = -pre * FX_SCALE;
+        fx += __float2ll_rn(q * dx);
+        fy += __float2ll_rn(q * dy);
+        fz += __float2ll_rn(q * dz);
     }
     __device__ __forceinline__ void force(float F[3]) const
     {
@@ -1087,7 +1089,8 @@ template <class R> struct ListArgs {
     float4* xref;        // position of particle i at the build; w: bits of its list length
     long long stride;
     int cap;             // list capacity per particle
-    R rl2;               // squared list radius
+    const R* rl2t;       // squared list radius (rc + skin) per type pair; 0: no potential, never listed
+    R rl2max;            // the largest of them
     float thr2;          // squared displacement since the build that triggers a rebuild
 };
 
@@ -1179,9 +1182,9 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) list_step_kerne
 #pragma unroll
         for (int u = 0; u < LCHUNK; ++u) {
             if (jj[u] < 0) continue;
-            const R dx = mimg(xi[0], xj[u][0], bx.L[0], bx.half[0], p0);
-            const R dy = mimg(xi[1], xj[u][1], bx.L[1], bx.half[1], p1);
-            const R dz = mimg(xi[2], xj[u][2], bx.L[2], bx.half[2], p2);
+            const R dx = mimg_sel(xi[0], xj[u][0], bx.L[0], bx.half[0], p0);
+            const R dy = mimg_sel(xi[1], xj[u][1], bx.L[1], bx.half[1], p1);
+            const R dz = mimg_sel(xi[2], xj[u][2], bx.L[2], bx.half[2], p2);
             const R r2 = dist2(dx, dy, dz);
             const int pidx = ti * MAXT + (wj[u] & 0xff);
             if (r2 < s_rc2[pidx]) {
@@ -1273,10 +1276,11 @@ __global__ void list_scatter_kernel(Args<R> a, ListArgs<R> v, long long off)
     }
 }
 
-// appends the pairs of one candidate range closer than rl
+// appends the pairs of one candidate range closer than their list radius
 template <class R>
 __device__ __forceinline__ void list_range(const State<R>& st, int j0, int j1, int self, const R xi[3], R sx, R sy,
-                                           R sz, R rl2, int* __restrict__ nb, long long stride, int cap, int& cnt)
+                                           R sz, const R* __restrict__ rl2, int* __restrict__ nb, long long stride,
+                                           int cap, int& cnt)
 {
     for (int j = j0; j < j1; ++j) {
         R xj[3];
@@ -1285,7 +1289,7 @@ __device__ __forceinline__ void list_range(const State<R>& st, int j0, int j1, i
         const R dx = sub_rn(xi[0], add_rn(xj[0], sx));
         const R dy = sub_rn(xi[1], add_rn(xj[1], sy));
         const R dz = sub_rn(xi[2], add_rn(xj[2], sz));
-        if (dist2(dx, dy, dz) < rl2 && j != self) {
+        if (dist2(dx, dy, dz) < rl2[wj & 0xff] && j != self) {
             if (cnt < cap) nb[(long long)cnt * stride] = j;
             ++cnt;
         }
@@ -1293,11 +1297,16 @@ __device__ __forceinline__ void list_range(const State<R>& st, int j0, int j1, i
 }
 
 // re-sort, part 4: the pair list of every particle of the re-sorted state,
-// from its 27-cell neighbourhood (every periodic axis has >= 3 cells here)
+// from its 27-cell neighbourhood (every periodic axis has >= 3 cells here).
+// A flattened walk (one candidate sequence per thread, as neighbourhood_flat)
+// measured slower here than the per-row loops: the candidate test is short.
 template <class R, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) list_build_kernel(Args<R> a, ListArgs<R> v, long long off)
 {
+    __shared__ R s_rl2[MAXT * MAXT];
     if (!list_gate(a, v)) return;
+    for (int k = threadIdx.x; k < MAXT * MAXT; k += BLOCK) s_rl2[k] = v.rl2t[k];
+    __syncthreads();
     const int sel = list_sel(a, v, off);
     const State<R> st = sel ? v.b0 : v.b1;     // the scatter's destination
     const int i = blockIdx.x * BLOCK + threadIdx.x;
@@ -1306,6 +1315,7 @@ __global__ void __launch_bounds__(BLOCK) list_build_kernel(Args<R> a, ListArgs<R
     R xi[3];
     int wi;
     load_pos(st, i, xi, wi);
+    const R* rl2 = s_rl2 + (wi & 0xff) * MAXT;
     int c[3];
     cell_coords(s, xi, c);
     Box<R> bx;
@@ -1317,8 +1327,7 @@ __global__ void __launch_bounds__(BLOCK) list_build_kernel(Args<R> a, ListArgs<R
         if constexpr (sizeof(R) == 4) cw[q] = R(1) / s.invcf[q]; else cw[q] = R(1) / s.invc[q];
         f[q] = xi[q] - (R)c[q] * cw[q];
     }
-    const R rl2 = v.rl2;
-    const R lim = rl2 * R(1.0001);
+    const R lim = v.rl2max * R(1.0001);
     int* nb = v.nbr + i;
     int cnt = 0;
     for (int dz = -1; dz <= 1; ++dz) {
