@@ -68,6 +68,8 @@ struct rdgpu_engine {
     long long* step_d = nullptr;
     double* red_d = nullptr;
     long long* redc_d = nullptr;
+    double* part_d = nullptr;            // partial sums of the typed reductions
+    long long* pcnt_d = nullptr;
     int* pinned_err = nullptr;
     long long* pinned_step = nullptr;
     long long step_h = 0;
@@ -238,6 +240,11 @@ template <class R> void build_ext(const rdgpu_system_desc& d, const rdgpu_box& b
             e.bhi[a] = (R)(hi - b.lo[a]);
         }
         e.rad = (R)q.radius;
+        {
+            const double r2 = q.radius * q.radius;
+            e.rad2h = (R)r2;
+            e.rad2l = (R)(r2 - (double)e.rad2h);
+        }
         e.h = (R)q.height;
         e.consider = q.consider_radius;
         e.tmask = 0;
@@ -1178,6 +1185,17 @@ template <class R> int fresh_cells(Engine* E)
     return E->nb_mode == RDGPU_NB_LIST ? resort<R>(E, true) : RDGPU_OK;
 }
 
+// sums of v by type into red_d/redc_d: wants 0..nwant-1, type S meaning all
+constexpr int kSumParts = 148 * 4;
+void launch_typed_sums(Engine* E, const double* v, const int* types, int S, int nwant)
+{
+    const long long n = E->npart_tot;
+    const long long chunk = std::max<long long>(1, (n + kSumParts - 1) / kSumParts);
+    typed_partial_kernel<<<dim3(kSumParts, nwant), TSUM_BLOCK, 0, E->stream>>>(v, types, n, S, chunk, E->part_d,
+                                                                              E->pcnt_d);
+    typed_final_kernel<<<nwant, TSUM_BLOCK, 0, E->stream>>>(E->part_d, E->pcnt_d, kSumParts, E->red_d, E->redc_d);
+}
+
 template <class R> int forces_impl(Engine* E, double* forces, double* energy)
 {
     int rc = fresh_cells<R>(E);
@@ -1186,7 +1204,7 @@ template <class R> int forces_impl(Engine* E, double* forces, double* energy)
     CK(cudaGetLastError());
     if (forces) CK(cudaMemcpyAsync(forces, E->vec_d, E->npart_tot * 3 * sizeof(double), cudaMemcpyDeviceToHost, E->stream));
     if (energy) {
-        typed_sum_kernel<<<1, 256, 256 * 16, E->stream>>>(E->val_d, E->ityp_d, E->npart_tot, 0, E->red_d, E->redc_d);
+        launch_typed_sums(E, E->val_d, E->ityp_d, 0, 1);
         CK(cudaGetLastError());
         CK(cudaMemcpyAsync(energy, E->red_d, sizeof(double), cudaMemcpyDeviceToHost, E->stream));
     }
@@ -1276,7 +1294,7 @@ template <class R> int msd_impl(Engine* E, rdgpu_metrics* m)
                                                                    cur_state<R>(E), E->x0_d, E->val_d,
                                                                    E->ityp_d);
     CK(cudaGetLastError());
-    typed_sum_kernel<<<S, 256, 256 * 16, E->stream>>>(E->val_d, E->ityp_d, E->npart_tot, S, E->red_d, E->redc_d);
+    launch_typed_sums(E, E->val_d, E->ityp_d, S, S);
     CK(cudaGetLastError());
     std::vector<double> sums(S);
     std::vector<long long> cnts(S);
@@ -1361,6 +1379,8 @@ int create_impl(const rdgpu_system_desc* desc, int nsys, const rdgpu_box* boxes,
         cudaMalloc(&E->step_d, sizeof(long long)) != cudaSuccess ||
         cudaMalloc(&E->red_d, (RDGPU_MAX_TYPES + 1) * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&E->redc_d, (RDGPU_MAX_TYPES + 1) * sizeof(long long)) != cudaSuccess ||
+        cudaMalloc(&E->part_d, (RDGPU_MAX_TYPES + 1) * kSumParts * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&E->pcnt_d, (RDGPU_MAX_TYPES + 1) * kSumParts * sizeof(long long)) != cudaSuccess ||
         cudaMallocHost(&E->pinned_err, sizeof(int)) != cudaSuccess ||
         cudaMallocHost(&E->pinned_step, sizeof(long long)) != cudaSuccess)
         return bail(RDGPU_ERR_NOMEM, "device allocation failed");
@@ -1427,7 +1447,7 @@ int rdgpu_destroy(rdgpu_handle h)
     dfree(E->sys_d); dfree(E->tab_d); dfree(E->ext_d); dfree(E->start); dfree(E->counts); dfree(E->tile_sum);
     dfree(E->err); dfree(E->err_step); dfree(E->step_d); dfree(E->ctl); dfree(E->rl2_d);
     if (E->pinned_ctl) cudaFreeHost(E->pinned_ctl);
-    dfree(E->red_d); dfree(E->redc_d); dfree(E->rdf_acc); dfree(E->rdf_tmp); dfree(E->rdf_e2);
+    dfree(E->red_d); dfree(E->redc_d); dfree(E->part_d); dfree(E->pcnt_d); dfree(E->rdf_acc); dfree(E->rdf_tmp); dfree(E->rdf_e2);
     if (E->pinned_err) cudaFreeHost(E->pinned_err);
     if (E->pinned_step) cudaFreeHost(E->pinned_step);
     if (E->stream) cudaStreamDestroy(E->stream);

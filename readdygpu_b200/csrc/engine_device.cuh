@@ -69,6 +69,7 @@ template <class R> struct ExtTerm {
     R blo[3], bhi[3];
     int consider;
     unsigned tmask;
+    R rad2h, rad2l;   // rad^2 as an unevaluated sum hi + lo (FP32 sphere distance)
 };
 
 template <class R> struct TypeTab {
@@ -333,18 +334,39 @@ __device__ __forceinline__ void ext_force(const ExtTerm<R>& p, R prad, const R x
     } else if (p.kind == 3) {
         R pr = p.consider ? prad : R(0);
         R d0 = x[0] - p.c[0], d1 = x[1] - p.c[1], d2 = x[2] - p.c[2];
-        R d = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
-        R r, r0;
+        R d, dr;   // distance to the centre, and d - rad
+        if constexpr (sizeof(R) == 4) {
+            // d - rad without the cancellation of FP32 d near the shell:
+            // d^2 - rad^2 from the exact products (fma residues) and the
+            // two-part rad^2, divided by d + rad
+            // (the _rn intrinsics keep the compiler from fusing the
+            // products into the sums, which the two-sums rely on)
+            const float h0 = __fmul_rn(d0, d0), h1 = __fmul_rn(d1, d1), h2 = __fmul_rn(d2, d2);
+            const float l = fmaf(d0, d0, -h0) + fmaf(d1, d1, -h1) + fmaf(d2, d2, -h2);
+            const float s01 = __fadd_rn(h0, h1);
+            const float b01 = __fsub_rn(s01, h0);
+            const float e01 = __fadd_rn(__fsub_rn(h0, __fsub_rn(s01, b01)), __fsub_rn(h1, b01));   // two-sum residue
+            const float s = __fadd_rn(s01, h2);
+            const float bs = __fsub_rn(s, s01);
+            const float es = __fadd_rn(__fsub_rn(s01, __fsub_rn(s, bs)), __fsub_rn(h2, bs));
+            d = sqrtf(s);
+            const float num = __fsub_rn(s, p.rad2h) + ((e01 + es + l) - p.rad2l);
+            dr = num / (d + p.rad);
+        } else {
+            d = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+            dr = d - p.rad;
+        }
+        R r, rr;   // r and r - r0 of the Java potential
         bool act;
-        if (p.sub == 1) { r = d + pr; r0 = p.rad; act = r > r0; }
-        else if (p.sub == 2) { r = d; r0 = p.rad + pr; act = r < r0; }
-        else { r = d; r0 = p.rad; act = r != r0; }
+        if (p.sub == 1) { r = d + pr; rr = dr + pr; act = rr > R(0); }
+        else if (p.sub == 2) { r = d; rr = dr - pr; act = rr < R(0); }
+        else { r = d; rr = dr; act = rr != R(0); }
         if (act) {
-            R pre = (r != R(0)) ? k * (r - r0) / r : R(0);
+            R pre = (r != R(0)) ? k * rr / r : R(0);
             g[0] += pre * (p.c[0] - x[0]);
             g[1] += pre * (p.c[1] - x[1]);
             g[2] += pre * (p.c[2] - x[2]);
-            e += R(0.5) * k * (r - r0) * (r - r0);
+            e += R(0.5) * k * rr * rr;
         }
     } else {
         R pr = p.consider ? prad : R(0);

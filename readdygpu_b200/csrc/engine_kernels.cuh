@@ -1024,22 +1024,58 @@ __global__ void msd_kernel(const SysDev* __restrict__ sys, const unsigned short*
     }
 }
 
-// deterministic per-type sums in index order: block b sums the entries of
-// type b (b == S: all entries)
-__global__ void typed_sum_kernel(const double* v, const int* types, long long n, int S, double* out, long long* counts)
+// Deterministic per-type sums, in two passes with fixed partitions and fixed
+// reduction trees (the result does not depend on scheduling):
+// typed_partial_kernel: block (x, y) sums the entries of type y (y == S: all
+// entries) in index chunk x; typed_final_kernel: block y sums its partials.
+constexpr int TSUM_BLOCK = 256;
+__global__ void __launch_bounds__(TSUM_BLOCK) typed_partial_kernel(const double* __restrict__ v,
+                                                                   const int* __restrict__ types, long long n, int S,
+                                                                   long long chunk, double* __restrict__ part,
+                                                                   long long* __restrict__ pcnt)
 {
-    extern __shared__ double red[];
+    __shared__ double red[TSUM_BLOCK];
+    __shared__ long long cr[TSUM_BLOCK];
+    const int want = blockIdx.y;
+    const long long a = (long long)blockIdx.x * chunk;
+    const long long b = min(n, a + chunk);
+    double acc = 0.0;
+    long long c = 0;
+    for (long long i = a + threadIdx.x; i < b; i += TSUM_BLOCK)
+        if (want == S || types[i] == want) { acc += v[i]; ++c; }
+    red[threadIdx.x] = acc;
+    cr[threadIdx.x] = c;
+    __syncthreads();
+    for (int o = TSUM_BLOCK / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) {
+            red[threadIdx.x] += red[threadIdx.x + o];
+            cr[threadIdx.x] += cr[threadIdx.x + o];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        part[(long long)want * gridDim.x + blockIdx.x] = red[0];
+        pcnt[(long long)want * gridDim.x + blockIdx.x] = cr[0];
+    }
+}
+
+__global__ void __launch_bounds__(TSUM_BLOCK) typed_final_kernel(const double* __restrict__ part,
+                                                                 const long long* __restrict__ pcnt, int P,
+                                                                 double* __restrict__ out, long long* __restrict__ counts)
+{
+    __shared__ double red[TSUM_BLOCK];
+    __shared__ long long cr[TSUM_BLOCK];
     const int want = blockIdx.x;
     double acc = 0.0;
     long long c = 0;
-    for (long long i = threadIdx.x; i < n; i += blockDim.x) {
-        if (want == S || types[i] == want) { acc += v[i]; ++c; }
+    for (int k = threadIdx.x; k < P; k += TSUM_BLOCK) {
+        acc += part[(long long)want * P + k];
+        c += pcnt[(long long)want * P + k];
     }
     red[threadIdx.x] = acc;
-    long long* cr = reinterpret_cast<long long*>(red + blockDim.x);
     cr[threadIdx.x] = c;
     __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    for (int o = TSUM_BLOCK / 2; o > 0; o >>= 1) {
         if (threadIdx.x < o) {
             red[threadIdx.x] += red[threadIdx.x + o];
             cr[threadIdx.x] += cr[threadIdx.x + o];
