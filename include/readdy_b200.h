@@ -197,6 +197,20 @@ int rdgpu_get_particles(rdgpu_handle h, double* xyz, int32_t* types);
 
 int rdgpu_num_particles(rdgpu_handle h, int64_t* n_total);
 
+/* Applies one frame's reaction edits on the device, in the layout of ReaDDy's
+   cReactions field: count entries of (readdyId, newType, x, y, z, gpuIndex).
+   gpuIndex != -1 deletes that particle; newType != -1 appends a particle of
+   that type at (x, y, z), absolute.  Survivors keep their order, appended
+   particles follow, and particle indices become 0 .. n-1 in that order.
+   Survivors keep their state (FP32 compensation, image counters, MSD
+   origin); appended particles start their MSD at their position; the step
+   count and the RDF accumulator continue.  Invalid entries (index out of
+   range or repeated, type out of range, non-integer type or index) leave the
+   state unchanged and return RDGPU_ERR_ARG.  Single-system handles only.
+   Replaces the host-side edit, compaction and re-upload of the reference
+   (ReaDDyGPU.cpp:303-461), which moved every particle through host memory.   */
+int rdgpu_apply_edits(rdgpu_handle h, const float* edits, int64_t count);
+
 /* ---- dynamics ---------------------------------------------------------- */
 
 /* Advance every system by nsteps Brownian-dynamics steps (Philox noise keyed

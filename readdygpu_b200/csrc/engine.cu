@@ -62,6 +62,12 @@ struct rdgpu_engine {
     double* val_d = nullptr;             // N doubles scratch
     int* ityp_d = nullptr;               // N ints scratch
     unsigned long long* u64_d = nullptr; // N scratch
+    int* ed_flag = nullptr;              // reaction edits: deleted flag, keep flag, new id by old id
+    int* ed_keep = nullptr;
+    int* ed_newid = nullptr;
+    int* ed_tile = nullptr;              // tile sums of the id scan
+    void* ed_buf = nullptr;              // deleted indices and appended particles of one frame
+    size_t ed_buf_bytes = 0;
     // control
     int* err = nullptr;
     long long* err_step = nullptr;
@@ -283,6 +289,7 @@ void free_particles(Engine* E)
     E->list_stride = 0;
     E->list_cap = 0;
     dfree(E->sys_of); dfree(E->x0_d); dfree(E->vec_d); dfree(E->val_d); dfree(E->ityp_d); dfree(E->u64_d);
+    dfree(E->ed_flag); dfree(E->ed_keep); dfree(E->ed_newid); dfree(E->ed_tile);
     E->cap_particles = 0;
 }
 
@@ -308,6 +315,10 @@ int ensure_particle_buffers(Engine* E, long long ntot)
     CK(cudaMalloc(&E->val_d, M * sizeof(double)));
     CK(cudaMalloc(&E->ityp_d, M * sizeof(int)));
     CK(cudaMalloc(&E->u64_d, M * sizeof(unsigned long long)));
+    CK(cudaMalloc(&E->ed_flag, (M + 1) * sizeof(int)));
+    CK(cudaMalloc(&E->ed_keep, (M + 1) * sizeof(int)));
+    CK(cudaMalloc(&E->ed_newid, (M + 1) * sizeof(int)));
+    CK(cudaMalloc(&E->ed_tile, ((M + SCAN_TILE - 1) / SCAN_TILE + 1) * sizeof(int)));
     E->cap_particles = M;
     return RDGPU_OK;
 }
@@ -1156,6 +1167,147 @@ template <class R> int set_particles_impl(Engine* E, const long long* offsets, l
     return RDGPU_OK;
 }
 
+// grows the per-particle buffers to hold n particles, keeping the current
+// state and the MSD origins of the first npart_tot particles
+template <class R> int grow_preserving(Engine* E, long long n)
+{
+    if (n <= E->cap_particles) return RDGPU_OK;
+    const long long nold = E->npart_tot;
+    const size_t recA = sizeof(R) == 4 ? 16 : 32;
+    void* keepA = E->bufA[E->cur];
+    void* keepB = E->bufB[E->cur];
+    double* keepX0 = E->x0_d;
+    E->bufA[E->cur] = nullptr;
+    E->bufB[E->cur] = nullptr;
+    E->x0_d = nullptr;
+    int rc = ensure_particle_buffers(E, n);    // new buffers, current state in buffer 0
+    if (rc == RDGPU_OK && nold > 0) {
+        cudaError_t e = cudaMemcpyAsync(E->bufA[0], keepA, nold * recA, cudaMemcpyDeviceToDevice, E->stream);
+        if (e == cudaSuccess && keepB)
+            e = cudaMemcpyAsync(E->bufB[0], keepB, nold * 16, cudaMemcpyDeviceToDevice, E->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(E->x0_d, keepX0, nold * 3 * sizeof(double), cudaMemcpyDeviceToDevice, E->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(E->stream);
+        if (e != cudaSuccess) rc = fail(E, RDGPU_ERR_CUDA, std::string("buffer growth: ") + cudaGetErrorString(e));
+    }
+    cudaFree(keepA);
+    if (keepB) cudaFree(keepB);
+    cudaFree(keepX0);
+    return rc;
+}
+
+// Reaction edits of one frame on the device (ReaDDyGPU.cpp:303-461 semantics):
+// delete by gpu index, append new particles, survivors keep their order and
+// the appended ones follow; ids are renumbered 0 .. n-1 in that order.
+template <class R> int apply_edits_impl(Engine* E, const float* ed, long long count)
+{
+    const long long N = E->npart_tot;
+    const int S = E->desc.n_types;
+    std::vector<char> gone(std::max<long long>(N, 1), 0);
+    std::vector<int> del;
+    std::vector<double> axyz;
+    std::vector<int> atype;
+    for (long long r = 0; r < count; ++r) {
+        const float* e = ed + 6 * r;
+        const double ft = e[1], fi = e[5];
+        if (!(std::isfinite(ft) && std::isfinite(fi)) || ft != std::floor(ft) || fi != std::floor(fi))
+            return fail(E, RDGPU_ERR_ARG, "reaction entry " + std::to_string(r) + ": type and index must be integers");
+        const long long index = (long long)fi;
+        const int newType = (int)ft;
+        if (index != -1) {
+            if (index < 0 || index >= N || gone[index])
+                return fail(E, RDGPU_ERR_ARG, "reaction entry " + std::to_string(r) + ": invalid or repeated gpu index");
+            gone[index] = 1;
+            del.push_back((int)index);
+        }
+        if (newType != -1) {
+            if (newType < 0 || newType >= S)
+                return fail(E, RDGPU_ERR_ARG, "reaction entry " + std::to_string(r) + ": type out of range");
+            axyz.push_back(e[2]);
+            axyz.push_back(e[3]);
+            axyz.push_back(e[4]);
+            atype.push_back(newType);
+        }
+    }
+    const long long nd = (long long)del.size(), na = (long long)atype.size();
+    if (nd == 0 && na == 0) return RDGPU_OK;
+    const long long nkeep = N - nd, N2 = nkeep + na;
+    if (N2 > 0x7fffffff) return fail(E, RDGPU_ERR_ARG, "at most 2^31-1 particles per handle");
+    int rc = grow_preserving<R>(E, N2);
+    if (rc) { E->part_off.clear(); return rc; }
+    drop_graphs(E);   // launch shapes depend on the particle count
+    auto bad = [&](const char* what) { E->part_off.clear(); return fail(E, RDGPU_ERR_CUDA, what); };
+    // the frame's edits on the device: appended coordinates, types, deleted indices
+    const size_t need = (size_t)na * 3 * sizeof(double) + (size_t)(na + nd) * sizeof(int);
+    if (need > E->ed_buf_bytes) {
+        dfree(E->ed_buf);
+        E->ed_buf_bytes = 0;
+        if (cudaMalloc(&E->ed_buf, need) != cudaSuccess) return bad("device allocation failed");
+        E->ed_buf_bytes = need;
+    }
+    double* axyz_d = (double*)E->ed_buf;
+    int* atype_d = (int*)(axyz_d + 3 * na);
+    int* del_d = atype_d + na;
+    if (nd) CK(cudaMemcpyAsync(del_d, del.data(), nd * sizeof(int), cudaMemcpyHostToDevice, E->stream));
+    if (na) {
+        CK(cudaMemcpyAsync(axyz_d, axyz.data(), 3 * na * sizeof(double), cudaMemcpyHostToDevice, E->stream));
+        CK(cudaMemcpyAsync(atype_d, atype.data(), na * sizeof(int), cudaMemcpyHostToDevice, E->stream));
+    }
+    CK(cudaMemsetAsync(E->ed_flag, 0, (N + 1) * sizeof(int), E->stream));
+    CK(cudaMemsetAsync(E->err, 0, sizeof(int), E->stream));
+    if (nd) edit_mark_kernel<<<grid_for(nd), 256, 0, E->stream>>>(del_d, nd, E->ed_flag);
+    if (N > 0) {
+        const int nt = (int)((N + SCAN_TILE - 1) / SCAN_TILE);
+        edit_keep_kernel<<<grid_for(N), 256, 0, E->stream>>>(E->ed_flag, N, E->ed_keep);
+        scan_tiles_kernel<<<nt, SCAN_BLOCK, 0, E->stream>>>(E->ed_keep, N, E->ed_tile, E->err, nullptr);
+        scan_apply_kernel<<<nt, SCAN_BLOCK, 0, E->stream>>>(E->ed_keep, N, E->ed_tile, nt, E->ed_newid, E->err,
+                                                            nullptr);
+        // survivors and appended particles at their new ids in the staging buffer
+        edit_restage_kernel<R><<<grid_for(N), 256, 0, E->stream>>>(E->sys_d, N, cur_state<R>(E), stg_state<R>(E),
+                                                                    E->ed_flag, E->ed_newid, E->tcell, E->tslot,
+                                                                    E->counts, E->x0_d, E->vec_d);
+    }
+    if (na)
+        edit_append_kernel<R><<<grid_for(na), 256, 0, E->stream>>>(E->sys_d, nkeep, na, axyz_d, atype_d, S,
+                                                                   stg_state<R>(E), E->tcell, E->tslot, E->counts,
+                                                                   E->vec_d, E->err);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(E->pinned_err, E->err, sizeof(int), cudaMemcpyDeviceToHost, E->stream));
+    CK(cudaStreamSynchronize(E->stream));
+    if (*E->pinned_err & EF_BADINPUT) {
+        // the staging buffer is rejected; the current state is untouched, but
+        // the counts hold the staged particles: clear them
+        CK(cudaMemsetAsync(E->counts, 0, std::max<long long>(E->ncells_tot, 1) * sizeof(int), E->stream));
+        CK(cudaMemsetAsync(E->err, 0, sizeof(int), E->stream));
+        CK(cudaStreamSynchronize(E->stream));
+        return fail(E, RDGPU_ERR_ARG, "appended particle with a non-finite coordinate or far outside the box");
+    }
+    // the new MSD origins and particle count, then the counting sort staging -> current
+    if (N2 > 0) CK(cudaMemcpyAsync(E->x0_d, E->vec_d, N2 * 3 * sizeof(double), cudaMemcpyDeviceToDevice, E->stream));
+    E->npart_tot = N2;
+    E->sys_h[0].npart = (int)N2;
+    E->part_off = {0, N2};
+    CK(cudaMemsetAsync(E->sys_of, 0, std::max<long long>(N2, 1) * sizeof(unsigned short), E->stream));
+    CK(cudaMemcpyAsync(E->sys_d, E->sys_h.data(), sizeof(SysDev), cudaMemcpyHostToDevice, E->stream));
+    launch_sort<R>(E);
+    CK(cudaGetLastError());
+    // host copy of the types by id
+    std::vector<int> nt;
+    nt.reserve(N2);
+    for (long long i = 0; i < N; ++i)
+        if (!gone[i]) nt.push_back(E->types_h[i]);
+    for (int t : atype) nt.push_back(t);
+    E->types_h.swap(nt);
+    rc = reset_counters(E, E->step_h);
+    if (rc) return rc;
+    if (E->nb_mode == RDGPU_NB_LIST && N2 > 0) {
+        rc = ensure_list(E, list_cap_estimate(E));
+        if (!rc) rc = resort<R>(E, true);
+        if (rc) { E->part_off.clear(); return rc; }
+    }
+    return RDGPU_OK;
+}
+
 template <class R> int get_particles_impl(Engine* E, double* xyz, int* types)
 {
     const long long N = E->npart_tot;
@@ -1447,7 +1599,7 @@ int rdgpu_destroy(rdgpu_handle h)
     dfree(E->sys_d); dfree(E->tab_d); dfree(E->ext_d); dfree(E->start); dfree(E->counts); dfree(E->tile_sum);
     dfree(E->err); dfree(E->err_step); dfree(E->step_d); dfree(E->ctl); dfree(E->rl2_d);
     if (E->pinned_ctl) cudaFreeHost(E->pinned_ctl);
-    dfree(E->red_d); dfree(E->redc_d); dfree(E->part_d); dfree(E->pcnt_d); dfree(E->rdf_acc); dfree(E->rdf_tmp); dfree(E->rdf_e2);
+    dfree(E->red_d); dfree(E->redc_d); dfree(E->part_d); dfree(E->pcnt_d); dfree(E->ed_buf); dfree(E->rdf_acc); dfree(E->rdf_tmp); dfree(E->rdf_e2);
     if (E->pinned_err) cudaFreeHost(E->pinned_err);
     if (E->pinned_step) cudaFreeHost(E->pinned_step);
     if (E->stream) cudaStreamDestroy(E->stream);
@@ -1479,6 +1631,16 @@ int rdgpu_set_particles(rdgpu_handle h, const int64_t* offsets, int64_t n_total,
     GUARD(E);
     if (n_total < 0 || (n_total > 0 && (!xyz || !types))) return fail(E, RDGPU_ERR_ARG, "invalid particle arrays");
     return DISPATCH(E, set_particles_impl, E, (const long long*)offsets, (long long)n_total, xyz, (const int*)types);
+}
+
+int rdgpu_apply_edits(rdgpu_handle h, const float* edits, int64_t count)
+{
+    Engine* E = (Engine*)h;
+    GUARD(E);
+    NEED_PARTICLES(E);
+    if (E->nsys != 1) return fail(E, RDGPU_ERR_ARG, "reaction edits are defined for a single system");
+    if (count < 0 || (count > 0 && !edits)) return fail(E, RDGPU_ERR_ARG, "invalid edit array");
+    return DISPATCH(E, apply_edits_impl, E, edits, (long long)count);
 }
 
 int rdgpu_get_particles(rdgpu_handle h, double* xyz, int32_t* types)

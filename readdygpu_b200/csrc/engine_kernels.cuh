@@ -755,6 +755,56 @@ __device__ __forceinline__ bool wrap_rel_dev(double& x, double L, int per)
     return true;
 }
 
+// one particle from absolute coordinates into staging slot g with the given
+// id: box-relative FP64 (or FP32 + compensation) coordinates, its cell and
+// slot, and its MSD origin
+template <class R>
+__device__ __forceinline__ void ingest_one(const SysDev& s, long long g, int id, const double* __restrict__ x3, int t,
+                                           int ntypes, State<R> stg, int* __restrict__ tcell,
+                                           int* __restrict__ tslot, int* __restrict__ counts,
+                                           double* __restrict__ x0, int* err)
+{
+    bool ok = t >= 0 && t < ntypes;
+    R xs[3];
+    if constexpr (sizeof(R) == 4) {
+        float h[3], c[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float Lf = s.Lf[a];
+            double xr = __dsub_rn(x3[a], s.lo[a]);
+            ok = ok && isfinite(xr) && wrap_rel_dev(xr, (double)Lf, s.per[a]);
+            float hh = __double2float_rn(xr);
+            if (s.per[a] && hh >= Lf) { hh = 0.0f; xr = __dsub_rn(xr, (double)Lf); }
+            h[a] = hh;
+            c[a] = __double2float_rn(__dsub_rn((double)hh, xr));
+            x0[3 * g + a] = xr;
+            xs[a] = hh;
+        }
+        stg.pos[g] = make_float4(h[0], h[1], h[2], __int_as_float(t));
+        stg.aux[g] = make_float4(c[0], c[1], c[2], __int_as_float(id));
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            double xr = __dsub_rn(x3[a], s.lo[a]);
+            ok = ok && isfinite(xr) && wrap_rel_dev(xr, s.L[a], s.per[a]);
+            xs[a] = xr;
+            x0[3 * g + a] = xr;
+        }
+        Rec64 r;
+        r.x = xs[0]; r.y = xs[1]; r.z = xs[2]; r.w = t; r.id = id;
+        stg.rec[g] = r;
+    }
+    if (!ok) {
+        atomicOr(err, EF_BADINPUT);
+        xs[0] = xs[1] = xs[2] = R(0);
+    }
+    int cc[3];
+    cell_coords(s, xs, cc);
+    const long long cell = s.cell_base + ((long long)cc[2] * s.n[1] + cc[1]) * s.n[0] + cc[0];
+    tcell[g] = (int)cell;
+    tslot[g] = atomicAdd(counts + cell, 1);
+}
+
 // writes the particles (input order) into the staging arrays with their cell
 // and slot, ready for scan + scatter
 template <class R>
@@ -766,48 +816,73 @@ __global__ void ingest_kernel(const SysDev* __restrict__ sys, const unsigned sho
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ntot;
          g += (long long)gridDim.x * blockDim.x) {
         const SysDev& s = sys[sys_of[g]];
-        const int t = types[g];
-        bool ok = t >= 0 && t < ntypes;
-        const int id = (int)(g - s.part_base);
-        R xs[3];
-        if constexpr (sizeof(R) == 4) {
-            float h[3], c[3];
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                const float Lf = s.Lf[a];
-                double xr = __dsub_rn(xyz[3 * g + a], s.lo[a]);
-                ok = ok && isfinite(xr) && wrap_rel_dev(xr, (double)Lf, s.per[a]);
-                float hh = __double2float_rn(xr);
-                if (s.per[a] && hh >= Lf) { hh = 0.0f; xr = __dsub_rn(xr, (double)Lf); }
-                h[a] = hh;
-                c[a] = __double2float_rn(__dsub_rn((double)hh, xr));
-                x0[3 * g + a] = xr;
-                xs[a] = hh;
-            }
-            stg.pos[g] = make_float4(h[0], h[1], h[2], __int_as_float(t));
-            stg.aux[g] = make_float4(c[0], c[1], c[2], __int_as_float(id));
-        } else {
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                double xr = __dsub_rn(xyz[3 * g + a], s.lo[a]);
-                ok = ok && isfinite(xr) && wrap_rel_dev(xr, s.L[a], s.per[a]);
-                xs[a] = xr;
-                x0[3 * g + a] = xr;
-            }
-            Rec64 r;
-            r.x = xs[0]; r.y = xs[1]; r.z = xs[2]; r.w = t; r.id = id;
-            stg.rec[g] = r;
-        }
-        if (!ok) {
-            atomicOr(err, EF_BADINPUT);
-            xs[0] = xs[1] = xs[2] = R(0);
-        }
-        int cc[3];
-        cell_coords(s, xs, cc);
-        const long long cell = s.cell_base + ((long long)cc[2] * s.n[1] + cc[1]) * s.n[0] + cc[0];
-        tcell[g] = (int)cell;
-        tslot[g] = atomicAdd(counts + cell, 1);
+        ingest_one<R>(s, g, (int)(g - s.part_base), xyz + 3 * g, types[g], ntypes, stg, tcell, tslot, counts, x0,
+                      err);
     }
+}
+
+// ---------------------------------------------------------------------------
+// Reaction edits on the device (one system): the deleted ids are flagged,
+// the survivors get new ids by an exclusive scan of the keep flags over the
+// old ids (their order is kept), and survivors and appended particles are
+// staged at their new ids for the counting sort.
+// ---------------------------------------------------------------------------
+__global__ void edit_mark_kernel(const int* __restrict__ del, long long nd, int* __restrict__ flag)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nd; k += (long long)gridDim.x * blockDim.x)
+        flag[del[k]] = 1;
+}
+
+__global__ void edit_keep_kernel(const int* __restrict__ flag, long long n, int* __restrict__ keep)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        keep[i] = 1 - flag[i];
+}
+
+template <class R>
+__global__ void edit_restage_kernel(const SysDev* __restrict__ sys, long long n, State<R> cur, State<R> stg,
+                                    const int* __restrict__ flag, const int* __restrict__ newid,
+                                    int* __restrict__ tcell, int* __restrict__ tslot, int* __restrict__ counts,
+                                    const double* __restrict__ x0, double* __restrict__ x0n)
+{
+    const SysDev& s = sys[0];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int id = load_id(cur, i);
+        if (flag[id]) continue;
+        const int nid = newid[id];
+        R x[3];
+        if constexpr (sizeof(R) == 4) {
+            const float4 p = cur.pos[i];
+            float4 q = cur.aux[i];
+            q.w = __int_as_float(nid);
+            stg.pos[nid] = p;
+            stg.aux[nid] = q;
+            x[0] = p.x; x[1] = p.y; x[2] = p.z;
+        } else {
+            Rec64 r = cur.rec[i];
+            r.id = nid;
+            stg.rec[nid] = r;
+            x[0] = r.x; x[1] = r.y; x[2] = r.z;
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) x0n[3 * (long long)nid + a] = x0[3 * (long long)id + a];
+        int cc[3];
+        cell_coords(s, x, cc);
+        const long long cell = s.cell_base + ((long long)cc[2] * s.n[1] + cc[1]) * s.n[0] + cc[0];
+        tcell[nid] = (int)cell;
+        tslot[nid] = atomicAdd(counts + cell, 1);
+    }
+}
+
+template <class R>
+__global__ void edit_append_kernel(const SysDev* __restrict__ sys, long long base, long long na,
+                                   const double* __restrict__ xyz, const int* __restrict__ types, int ntypes,
+                                   State<R> stg, int* __restrict__ tcell, int* __restrict__ tslot,
+                                   int* __restrict__ counts, double* __restrict__ x0n, int* err)
+{
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < na; k += (long long)gridDim.x * blockDim.x)
+        ingest_one<R>(sys[0], base + k, (int)(base + k), xyz + 3 * k, types[k], ntypes, stg, tcell, tslot, counts,
+                      x0n, err);
 }
 
 // sorted arrays -> absolute coordinates and types by global index

@@ -167,49 +167,40 @@ extern "C" JNIEXPORT void JNICALL Java_readdy_impl_sim_top_TopGPU_cCreateSimulat
                    (long long)count);
             break;
         }
-        std::vector<int32_t> ntypes(types);
-        std::vector<double> nxyz(xyz);
-        std::vector<int32_t> nids(ids);
+        // the readdy ids follow the edits on the host; the particles are edited
+        // on the device (rdgpu_apply_edits), nothing is re-uploaded
+        std::vector<char> gone(n, 0);
+        std::vector<int32_t> added;
         bool bad = false;
         for (int64_t r = 0; r < count; ++r) {
             const float* e = &R[1 + 6 * r];
             int id = (int)e[0], newType = (int)e[1], index = (int)e[5];
             if (index != -1) {
-                if (index < 0 || index >= n || ntypes[index] == -1) { bad = true; break; }
-                ntypes[index] = -1;
+                if (index < 0 || index >= n || gone[index]) { bad = true; break; }
+                gone[index] = 1;
             }
             if (newType != -1) {
                 if (newType < 0 || newType >= desc.n_types) { bad = true; break; }
-                nxyz.push_back(e[2]);
-                nxyz.push_back(e[3]);
-                nxyz.push_back(e[4]);
-                ntypes.push_back(newType);
-                nids.push_back(id);
+                added.push_back(id);
             }
         }
         if (bad) {
             printf("error: invalid reaction entry in cReactions\n");
             break;
         }
-        xyz.clear();
-        types.clear();
-        ids.clear();
-        for (size_t i = 0; i < ntypes.size(); ++i) {
-            if (ntypes[i] == -1) continue;
-            xyz.push_back(nxyz[3 * i]);
-            xyz.push_back(nxyz[3 * i + 1]);
-            xyz.push_back(nxyz[3 * i + 2]);
-            types.push_back(ntypes[i]);
-            ids.push_back(nids[i]);
-        }
-        n = (int64_t)types.size();
-        // re-upload and re-bin (copyPosToDevice ... resizeCuRand, ReaDDyGPU.cpp:421-460);
-        // the step counter restarts, the Philox stream continues through the seed + frame
-        rdgpu_set_seed(h, 0, opt.seed + 0x9E3779B97F4A7C15ull * (uint64_t)(frame + 1));
-        if (rdgpu_set_particles(h, nullptr, n, xyz.data(), types.data()) != RDGPU_OK) {
+        if (rdgpu_apply_edits(h, &R[1], count) != RDGPU_OK) {
             printf("error while applying reactions: %s\n", rdgpu_last_error(h));
             break;
         }
+        std::vector<int32_t> nids;
+        nids.reserve(ids.size() + added.size());
+        for (int64_t i = 0; i < n; ++i)
+            if (!gone[i]) nids.push_back(ids[i]);
+        for (int32_t id : added) nids.push_back(id);
+        ids.swap(nids);
+        n = (int64_t)ids.size();
+        xyz.resize(3 * n);
+        types.resize(n);
     }
     rdgpu_destroy(h);
     printf("END\n");

@@ -127,6 +127,15 @@ class Engine:
         self._check(_lib().rdgpu_get_particles(self._h, _p(xyz, C.c_double), _p(types, C.c_int32)))
         return xyz, types
 
+    def apply_edits(self, edits):
+        """Reaction edits in the layout of ReaDDy's cReactions entries:
+        rows of (readdyId, newType, x, y, z, gpuIndex)."""
+        e = np.ascontiguousarray(edits, dtype=np.float32).reshape(-1, 6)
+        self._check(_lib().rdgpu_apply_edits(self._h, _p(e, C.c_float), e.shape[0]))
+        n = C.c_int64()
+        _lib().rdgpu_num_particles(self._h, C.byref(n))
+        self.n = n.value
+
     # -- dynamics --------------------------------------------------------
     def step(self, nsteps=1):
         self._check(_lib().rdgpu_step(self._h, int(nsteps)))
