@@ -292,14 +292,16 @@ def run_ours(args):
     if not args.no_e2e:
         frame = 100
         frames = max(1, min(20, args.steps // frame))
-        xh, th = eng.get_particles()
-        xh = np.ascontiguousarray(xh)
+        # pinned host buffers, as a host application would keep them
+        xh = torch.empty((w.n, 3), dtype=torch.float64, pin_memory=True).numpy()
+        th = torch.empty(w.n, dtype=torch.int32, pin_memory=True).numpy()
+        eng.get_particles(xh, th)
         barrier()
         t0 = time.perf_counter()
         for _ in range(frames):
             eng.set_particles(xh, th, offsets=w.offsets)
             eng.step(frame)
-            xh, th = eng.get_particles()
+            eng.get_particles(xh, th)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         tt = torch.tensor([dt], dtype=torch.float64, device=f"cuda:{local}")

@@ -75,6 +75,7 @@ struct rdgpu_engine {
     double* red_d = nullptr;
     long long* redc_d = nullptr;
     double* part_d = nullptr;            // partial sums of the typed reductions
+    long long* off_d = nullptr;          // particle offsets of the systems (n_systems + 1)
     long long* pcnt_d = nullptr;
     int* pinned_err = nullptr;
     long long* pinned_step = nullptr;
@@ -1124,18 +1125,17 @@ template <class R> int set_particles_impl(Engine* E, const long long* offsets, l
     if (ntot != E->npart_tot) drop_graphs(E);   // launch shapes depend on the particle count
     int rc = ensure_particle_buffers(E, ntot);
     if (rc) return rc;
-    std::vector<unsigned short> so(std::max<long long>(ntot, 1));
     for (int s = 0; s < E->nsys; ++s) {
         E->sys_h[s].part_base = off[s];
         E->sys_h[s].npart = (int)(off[s + 1] - off[s]);
-        for (long long g = off[s]; g < off[s + 1]; ++g) so[g] = (unsigned short)s;
     }
     E->npart_tot = ntot;
     CK(cudaMemcpyAsync(E->sys_d, E->sys_h.data(), E->nsys * sizeof(SysDev), cudaMemcpyHostToDevice, E->stream));
     CK(cudaMemsetAsync(E->err, 0, sizeof(int), E->stream));
     CK(cudaMemsetAsync(E->counts, 0, std::max<long long>(E->ncells_tot, 1) * sizeof(int), E->stream));
     if (ntot > 0) {
-        CK(cudaMemcpyAsync(E->sys_of, so.data(), ntot * sizeof(unsigned short), cudaMemcpyHostToDevice, E->stream));
+        CK(cudaMemcpyAsync(E->off_d, off.data(), (E->nsys + 1) * sizeof(long long), cudaMemcpyHostToDevice, E->stream));
+        sys_of_kernel<<<grid_for(ntot), 256, 0, E->stream>>>(E->off_d, E->nsys, ntot, E->sys_of);
         CK(cudaMemcpyAsync(E->vec_d, xyz, ntot * 3 * sizeof(double), cudaMemcpyHostToDevice, E->stream));
         CK(cudaMemcpyAsync(E->ityp_d, types, ntot * sizeof(int), cudaMemcpyHostToDevice, E->stream));
         ingest_kernel<R><<<grid_for(ntot), 256, 0, E->stream>>>(E->sys_d, E->sys_of, ntot, E->vec_d, E->ityp_d,
@@ -1532,6 +1532,7 @@ int create_impl(const rdgpu_system_desc* desc, int nsys, const rdgpu_box* boxes,
         cudaMalloc(&E->red_d, (RDGPU_MAX_TYPES + 1) * sizeof(double)) != cudaSuccess ||
         cudaMalloc(&E->redc_d, (RDGPU_MAX_TYPES + 1) * sizeof(long long)) != cudaSuccess ||
         cudaMalloc(&E->part_d, (RDGPU_MAX_TYPES + 1) * kSumParts * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&E->off_d, (nsys + 1) * sizeof(long long)) != cudaSuccess ||
         cudaMalloc(&E->pcnt_d, (RDGPU_MAX_TYPES + 1) * kSumParts * sizeof(long long)) != cudaSuccess ||
         cudaMallocHost(&E->pinned_err, sizeof(int)) != cudaSuccess ||
         cudaMallocHost(&E->pinned_step, sizeof(long long)) != cudaSuccess)
@@ -1599,7 +1600,7 @@ int rdgpu_destroy(rdgpu_handle h)
     dfree(E->sys_d); dfree(E->tab_d); dfree(E->ext_d); dfree(E->start); dfree(E->counts); dfree(E->tile_sum);
     dfree(E->err); dfree(E->err_step); dfree(E->step_d); dfree(E->ctl); dfree(E->rl2_d);
     if (E->pinned_ctl) cudaFreeHost(E->pinned_ctl);
-    dfree(E->red_d); dfree(E->redc_d); dfree(E->part_d); dfree(E->pcnt_d); dfree(E->ed_buf); dfree(E->rdf_acc); dfree(E->rdf_tmp); dfree(E->rdf_e2);
+    dfree(E->red_d); dfree(E->redc_d); dfree(E->part_d); dfree(E->pcnt_d); dfree(E->ed_buf); dfree(E->off_d); dfree(E->rdf_acc); dfree(E->rdf_tmp); dfree(E->rdf_e2);
     if (E->pinned_err) cudaFreeHost(E->pinned_err);
     if (E->pinned_step) cudaFreeHost(E->pinned_step);
     if (E->stream) cudaStreamDestroy(E->stream);

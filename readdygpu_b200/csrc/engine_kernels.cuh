@@ -755,6 +755,21 @@ __device__ __forceinline__ bool wrap_rel_dev(double& x, double L, int per)
     return true;
 }
 
+// system of every particle from the prefix offsets (off[0] = 0, off[nsys] = ntot)
+__global__ void sys_of_kernel(const long long* __restrict__ off, int nsys, long long ntot,
+                              unsigned short* __restrict__ so)
+{
+    for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ntot;
+         g += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = nsys;            // off[lo] <= g < off[hi]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (off[mid] <= g) lo = mid; else hi = mid;
+        }
+        so[g] = (unsigned short)lo;
+    }
+}
+
 // one particle from absolute coordinates into staging slot g with the given
 // id: box-relative FP64 (or FP32 + compensation) coordinates, its cell and
 // slot, and its MSD origin

@@ -121,9 +121,15 @@ class Engine:
         self._check(_lib().rdgpu_set_particles(self._h, offp, n, _p(xyz, C.c_double), _p(types, C.c_int32)))
         self.n = n
 
-    def get_particles(self):
-        xyz = np.empty((self.n, 3))
-        types = np.empty(self.n, np.int32)
+    def get_particles(self, xyz=None, types=None):
+        """Positions (n, 3) float64 and types; into the given C-contiguous
+        arrays when passed (e.g. pinned host buffers)."""
+        if xyz is None:
+            xyz = np.empty((self.n, 3))
+        if types is None:
+            types = np.empty(self.n, np.int32)
+        assert xyz.dtype == np.float64 and xyz.shape == (self.n, 3) and xyz.flags.c_contiguous
+        assert types.dtype == np.int32 and types.shape == (self.n,) and types.flags.c_contiguous
         self._check(_lib().rdgpu_get_particles(self._h, _p(xyz, C.c_double), _p(types, C.c_int32)))
         return xyz, types
 
