@@ -1292,8 +1292,9 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) list_step_kerne
     const int cnt = __float_as_int(xr.w);
     const int* nb = v.nbr + i;
     // the partners in chunks of LCHUNK: all their indices, then all their
-    // positions are requested before the first pair is evaluated
-    constexpr int LCHUNK = 4;
+    // positions are requested before the first pair is evaluated (5 measured
+    // best among 2..8 at about 6 partners per particle)
+    constexpr int LCHUNK = 5;
     for (int k0 = 0; k0 < cnt; k0 += LCHUNK) {
         int jj[LCHUNK];
 #pragma unroll
