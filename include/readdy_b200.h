@@ -197,6 +197,21 @@ int rdgpu_get_particles(rdgpu_handle h, double* xyz, int32_t* types);
 
 int rdgpu_num_particles(rdgpu_handle h, int64_t* n_total);
 
+/* Bonded pairs of particle groups (ReaDDy group potentials): each bond
+   applies one pair potential to two particles at any distance (minimum
+   image).  ij: 2 x n_bonds particle indices; pot: n_bonds indices into
+   pots[n_pots] (kind HARMONIC or WEAK_INTERACTION_PIECEWISE_HARMONIC; r0 < 0
+   takes the collision-radius sum of the two types; `pairs` is not used).
+   Replaces the reference's groups kernel (CudaSimulation.cu:1829-1836,
+   launched at :2454) with the Java group semantics: every listed pair with
+   its own potential and each particle's own type (the reference passes
+   particle 1's type twice and applies potential 0 to every pair).  The
+   bonds replace any earlier ones; rdgpu_set_particles clears them;
+   rdgpu_apply_edits drops the bonds of deleted particles and renumbers the
+   rest.  Single-system handles only.                                          */
+int rdgpu_set_bonds(rdgpu_handle h, int64_t n_bonds, const int32_t* ij, const int32_t* pot, int32_t n_pots,
+                    const rdgpu_pair_pot* pots);
+
 /* Applies one frame's reaction edits on the device, in the layout of ReaDDy's
    cReactions field: count entries of (readdyId, newType, x, y, z, gpuIndex).
    gpuIndex != -1 deletes that particle; newType != -1 appends a particle of

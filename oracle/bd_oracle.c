@@ -511,6 +511,39 @@ int orc_forces_f64(const rdgpu_system_desc* d, int64_t n, const double* xrel,
     return 0;
 }
 
+/* Adds the forces and energy of bonded pairs (ReaDDy particle groups): each
+   bond applies one pair potential at any distance, minimum image, r0 from
+   the potential or the collision-radius sum of the two types
+   (group semantics of the Java core; the reference GPU's groups kernel,
+   CudaSimulation.cu:1829-1836, passes particle 1's type twice).            */
+int orc_bond_forces_f64(const rdgpu_system_desc* d, int64_t n, const double* x, const int32_t* types,
+                        int64_t nb, const int32_t* ij, const int32_t* pot, int32_t npots,
+                        const rdgpu_pair_pot* pots, double* forces, double* energy)
+{
+    tables_t t;
+    make_tables(d, &t);
+    double etot = 0.0;
+    for (int64_t b = 0; b < nb; ++b) {
+        const int64_t i = ij[2 * b], j = ij[2 * b + 1];
+        if (i < 0 || j < 0 || i >= n || j >= n || pot[b] < 0 || pot[b] >= npots) return -1;
+        const rdgpu_pair_pot* pp = &pots[pot[b]];
+        const int ti = types[i], tj = types[j];
+        double dx = mimg(x[3 * i + 0], x[3 * j + 0], t.L[0], t.half[0], t.per[0]);
+        double dy = mimg(x[3 * i + 1], x[3 * j + 1], t.L[1], t.half[1], t.per[1]);
+        double dz = mimg(x[3 * i + 2], x[3 * j + 2], t.L[2], t.half[2], t.per[2]);
+        double r = sqrt(dx * dx + dy * dy + dz * dz);
+        double r0 = (pp->r0 >= 0.0) ? pp->r0 : t.r0[ti * MT + tj];
+        double pre, pe;
+        if (pair_scalar(pp, r0, r, &pre, &pe)) return -1;
+        /* force on i = pre * (x_j - x_i) = -pre * (x_i - x_j) */
+        forces[3 * i + 0] -= pre * dx; forces[3 * i + 1] -= pre * dy; forces[3 * i + 2] -= pre * dz;
+        forces[3 * j + 0] += pre * dx; forces[3 * j + 1] += pre * dy; forces[3 * j + 2] += pre * dz;
+        etot += pe;
+    }
+    if (energy) *energy += etot;
+    return 0;
+}
+
 /* ------------------------------------------------------------------------ */
 /* Neighbour digests (bit-exact predicates).                                */
 /* ------------------------------------------------------------------------ */

@@ -71,6 +71,11 @@ void orc_neighbor_digest_f32(const rdgpu_system_desc* d, int64_t n,
 /* One Euler-Maruyama step with injected noise (3 per particle):
    x <- x + D dt/(kB T) F + sqrt(2 D dt) xi, then periodic wrap.
    Returns 0, or RDGPU_ERR_JUMP if a particle moved more than a box length.  */
+/* Adds the forces and energy of bonded pairs (particle groups).           */
+int orc_bond_forces_f64(const rdgpu_system_desc* d, int64_t n, const double* x, const int32_t* types,
+                        int64_t nb, const int32_t* ij, const int32_t* pot, int32_t npots,
+                        const rdgpu_pair_pot* pots, double* forces, double* energy);
+
 int orc_step_f64(const rdgpu_system_desc* d, int64_t n, double* xrel,
                  const int32_t* types, const double* noise, int n_threads);
 

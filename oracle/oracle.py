@@ -42,6 +42,8 @@ def lib():
             "orc_splitmix64": (C.c_uint64, [C.c_uint64]),
             "orc_run_steps_f64": (C.c_int, [SD, C.c_int64, DP, I32P, C.c_uint64, C.c_int64, C.c_int64, C.c_int]),
             "orc_max_threads": (C.c_int, []),
+            "orc_bond_forces_f64": (C.c_int, [SD, C.c_int64, DP, I32P, C.c_int64, I32P, I32P, C.c_int32,
+                                              C.POINTER(A.PairPot), DP, DP]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -101,6 +103,22 @@ def forces_f64(desc, xrel, types, threads=1):
     e = C.c_double()
     lib().orc_forces_f64(C.byref(desc), n, _p(xrel, C.c_double), _p(types, C.c_int32),
                          _p(F, C.c_double), C.byref(e), threads)
+    return F, e.value
+
+
+def bond_forces(desc, xrel, types, ij, pot, pots, F=None, energy=0.0):
+    """Adds the forces/energy of bonded pairs (pots: C PairPot structs) to F."""
+    xrel = _c(xrel, np.float64); types = _c(types, np.int32)
+    ij = _c(ij, np.int32).reshape(-1); pot = _c(pot, np.int32).reshape(-1)
+    n = types.size
+    F = np.zeros((n, 3)) if F is None else np.ascontiguousarray(F, dtype=np.float64)
+    arr = (A.PairPot * max(1, len(pots)))(*pots)
+    e = C.c_double(energy)
+    rc = lib().orc_bond_forces_f64(C.byref(desc), n, _p(xrel, C.c_double), _p(types, C.c_int32), pot.size,
+                                   _p(ij, C.c_int32), _p(pot, C.c_int32), len(pots), arr, _p(F, C.c_double),
+                                   C.byref(e))
+    if rc:
+        raise ValueError("invalid bond")
     return F, e.value
 
 

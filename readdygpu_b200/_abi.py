@@ -115,6 +115,7 @@ FUNCTIONS = [
     ("rdgpu_step_profile", C.c_int, [P, C.c_int64, DP, DP]),
     ("rdgpu_autotune", C.c_int, [P]),
     ("rdgpu_apply_edits", C.c_int, [P, C.POINTER(C.c_float), C.c_int64]),
+    ("rdgpu_set_bonds", C.c_int, [P, C.c_int64, I32P, I32P, C.c_int32, C.c_void_p]),
     ("rdgpu_rdf_counts_noalloc", C.c_int, [P, P, C.c_int64, C.c_int32, DP, DP, I32P, C.c_int32, C.c_double,
                                            P, P]),
 ]

@@ -7,6 +7,7 @@
 // steps of rdgpu_step are replayed from a captured CUDA graph of
 // step_kernel -> scan_tiles -> scan_apply -> scatter per step.
 #include <algorithm>
+#include <map>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -68,6 +69,16 @@ struct rdgpu_engine {
     int* ed_tile = nullptr;              // tile sums of the id scan
     void* ed_buf = nullptr;              // deleted indices and appended particles of one frame
     size_t ed_buf_bytes = 0;
+    // bonded pairs (particle groups)
+    int* inv = nullptr;                  // sorted index of each particle id
+    long long nbonds = 0;
+    int* bstart = nullptr;               // CSR by particle id
+    int* bpart = nullptr;
+    int* bterm = nullptr;
+    void* btab = nullptr;                // PairTerm<R> per (potential, type pair) in use
+    std::vector<int> bond_ij_h;          // 2 per bond
+    std::vector<int> bond_pot_h;
+    std::vector<rdgpu_pair_pot> bond_pots_h;
     // control
     int* err = nullptr;
     long long* err_step = nullptr;
@@ -290,7 +301,7 @@ void free_particles(Engine* E)
     E->list_stride = 0;
     E->list_cap = 0;
     dfree(E->sys_of); dfree(E->x0_d); dfree(E->vec_d); dfree(E->val_d); dfree(E->ityp_d); dfree(E->u64_d);
-    dfree(E->ed_flag); dfree(E->ed_keep); dfree(E->ed_newid); dfree(E->ed_tile);
+    dfree(E->ed_flag); dfree(E->ed_keep); dfree(E->ed_newid); dfree(E->ed_tile); dfree(E->inv);
     E->cap_particles = 0;
 }
 
@@ -320,6 +331,7 @@ int ensure_particle_buffers(Engine* E, long long ntot)
     CK(cudaMalloc(&E->ed_keep, (M + 1) * sizeof(int)));
     CK(cudaMalloc(&E->ed_newid, (M + 1) * sizeof(int)));
     CK(cudaMalloc(&E->ed_tile, ((M + SCAN_TILE - 1) / SCAN_TILE + 1) * sizeof(int)));
+    CK(cudaMalloc(&E->inv, M * sizeof(int)));
     E->cap_particles = M;
     return RDGPU_OK;
 }
@@ -355,6 +367,13 @@ template <class R> Args<R> make_args(Engine* E)
     a.err = E->err;
     a.err_step = E->err_step;
     a.step_ptr = E->step_d;
+    if (E->nbonds > 0) {
+        a.bstart = E->bstart;
+        a.bpart = E->bpart;
+        a.bterm = E->bterm;
+        a.btab = (const PairTerm<R>*)E->btab;
+        a.inv = E->inv;
+    }
     return a;
 }
 
@@ -375,7 +394,8 @@ template <class R> void launch_sort(Engine* E)
                                                                E->start, E->err, nullptr);
     if (E->npart_tot > 0)
         scatter_kernel<R><<<grid_for(E->npart_tot), 256, 0, E->stream>>>(
-            stg_state<R>(E), cur_state<R>(E), E->tcell, E->tslot, E->start, E->npart_tot, E->err);
+            stg_state<R>(E), cur_state<R>(E), E->tcell, E->tslot, E->start, E->npart_tot, E->err,
+            E->nbonds > 0 ? E->inv : nullptr);
     E->launches += (E->npart_tot > 0) ? 3 : 2;
 }
 
@@ -1103,6 +1123,113 @@ template <class R> int profile_impl(Engine* E, long long nsteps, double* kms, do
     return RDGPU_OK;
 }
 
+// ---------------------------------------------------------------------------
+// bonded pairs (particle groups)
+// ---------------------------------------------------------------------------
+void free_bonds(Engine* E)
+{
+    dfree(E->bstart); dfree(E->bpart); dfree(E->bterm); dfree(E->btab);
+    if (E->nbonds > 0) drop_graphs(E);   // kernel arguments change
+    E->nbonds = 0;
+}
+
+void clear_bonds(Engine* E)
+{
+    free_bonds(E);
+    E->bond_ij_h.clear();
+    E->bond_pot_h.clear();
+    E->bond_pots_h.clear();
+}
+
+// the bonds of bond_ij_h / bond_pot_h to the device: a list per particle id
+// (each bond in both of its particles' lists) with its potential resolved for
+// the two types, and the sorted index of every id
+template <class R> int upload_bonds(Engine* E)
+{
+    free_bonds(E);
+    const long long nb = (long long)E->bond_pot_h.size();
+    if (nb == 0 || E->npart_tot == 0) return RDGPU_OK;
+    const long long N = E->npart_tot;
+    const int M = RDGPU_MAX_TYPES;
+    std::vector<int> start(N + 1, 0), part(2 * nb), term(2 * nb);
+    for (long long b = 0; b < nb; ++b) { start[E->bond_ij_h[2 * b] + 1]++; start[E->bond_ij_h[2 * b + 1] + 1]++; }
+    for (long long i = 0; i < N; ++i) start[i + 1] += start[i];
+    std::vector<int> fill(start.begin(), start.end() - 1);
+    std::vector<PairTerm<R>> tab;
+    std::map<long long, int> key_to_term;
+    auto term_of = [&](int p, int ta, int tb) {
+        const long long key = ((long long)p * M + ta) * M + tb;
+        auto it = key_to_term.find(key);
+        if (it != key_to_term.end()) return it->second;
+        const rdgpu_pair_pot& q = E->bond_pots_h[p];
+        const double r0pair = E->desc.coll_radius[ta * M + tb] + E->desc.coll_radius[tb * M + ta];
+        PairTerm<R> t;
+        memset(&t, 0, sizeof(t));
+        t.kind = q.kind;
+        t.sub = q.subtype;
+        t.k = (R)q.k;
+        t.r0 = (R)(q.r0 >= 0.0 ? q.r0 : r0pair);
+        t.l = (R)q.length;
+        t.d = (R)q.depth;
+        t.q = (R)(q.length > 0 ? (1.0 / (0.5 * q.length)) * (1.0 / (0.5 * q.length)) : 0.0);
+        tab.push_back(t);
+        key_to_term[key] = (int)tab.size() - 1;
+        return (int)tab.size() - 1;
+    };
+    for (long long b = 0; b < nb; ++b) {
+        const int i = E->bond_ij_h[2 * b], j = E->bond_ij_h[2 * b + 1], p = E->bond_pot_h[b];
+        const int ti = E->types_h[i], tj = E->types_h[j];
+        const int ki = fill[i]++, kj = fill[j]++;
+        part[ki] = j;
+        term[ki] = term_of(p, ti, tj);
+        part[kj] = i;
+        term[kj] = term_of(p, tj, ti);
+    }
+    CK(cudaMalloc(&E->bstart, (N + 1) * sizeof(int)));
+    CK(cudaMalloc(&E->bpart, 2 * nb * sizeof(int)));
+    CK(cudaMalloc(&E->bterm, 2 * nb * sizeof(int)));
+    CK(cudaMalloc(&E->btab, tab.size() * sizeof(PairTerm<R>)));
+    CK(cudaMemcpyAsync(E->bstart, start.data(), (N + 1) * sizeof(int), cudaMemcpyHostToDevice, E->stream));
+    CK(cudaMemcpyAsync(E->bpart, part.data(), 2 * nb * sizeof(int), cudaMemcpyHostToDevice, E->stream));
+    CK(cudaMemcpyAsync(E->bterm, term.data(), 2 * nb * sizeof(int), cudaMemcpyHostToDevice, E->stream));
+    CK(cudaMemcpyAsync(E->btab, tab.data(), tab.size() * sizeof(PairTerm<R>), cudaMemcpyHostToDevice, E->stream));
+    inv_kernel<R><<<grid_for(N), 256, 0, E->stream>>>(cur_state<R>(E), N, E->inv);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(E->stream));
+    E->nbonds = nb;
+    drop_graphs(E);
+    return RDGPU_OK;
+}
+
+template <class R> int set_bonds_impl(Engine* E, long long nb, const int* ij, const int* pot, int npots,
+                                      const rdgpu_pair_pot* pots)
+{
+    const long long N = E->npart_tot;
+    for (int p = 0; p < npots; ++p) {
+        const rdgpu_pair_pot& q = pots[p];
+        if (q.kind == RDGPU_P2_HARMONIC) {
+            if (q.subtype < 1 || q.subtype > 3) return fail(E, RDGPU_ERR_ARG, "bond potential: invalid harmonic subtype");
+        } else if (q.kind == RDGPU_P2_WEAK_PIECEWISE) {
+            if (!(q.length > 0)) return fail(E, RDGPU_ERR_ARG, "bond potential: weak interaction needs length > 0");
+        } else {
+            return fail(E, RDGPU_ERR_ARG, "bond potential: unknown kind");
+        }
+    }
+    for (long long b = 0; b < nb; ++b) {
+        const long long i = ij[2 * b], j = ij[2 * b + 1];
+        if (i < 0 || j < 0 || i >= N || j >= N || i == j)
+            return fail(E, RDGPU_ERR_ARG, "bond " + std::to_string(b) + ": particle index out of range or self bond");
+        if (pot[b] < 0 || pot[b] >= npots) return fail(E, RDGPU_ERR_ARG, "bond " + std::to_string(b) + ": potential index out of range");
+    }
+    clear_bonds(E);
+    E->bond_ij_h.assign(ij, ij + 2 * nb);
+    E->bond_pot_h.assign(pot, pot + nb);
+    E->bond_pots_h.assign(pots, pots + npots);
+    int rc = upload_bonds<R>(E);
+    if (rc) clear_bonds(E);
+    return rc;
+}
+
 template <class R> int set_particles_impl(Engine* E, const long long* offsets, long long ntot,
                                           const double* xyz, const int* types)
 {
@@ -1122,6 +1249,7 @@ template <class R> int set_particles_impl(Engine* E, const long long* offsets, l
     }
     if (ntot > 0x7fffffff) return fail(E, RDGPU_ERR_ARG, "at most 2^31-1 particles per handle");
     E->part_off.clear();   // no valid state until this call completes
+    clear_bonds(E);        // bonds name particles of the previous upload
     if (ntot != E->npart_tot) drop_graphs(E);   // launch shapes depend on the particle count
     int rc = ensure_particle_buffers(E, ntot);
     if (rc) return rc;
@@ -1298,6 +1426,25 @@ template <class R> int apply_edits_impl(Engine* E, const float* ed, long long co
         if (!gone[i]) nt.push_back(E->types_h[i]);
     for (int t : atype) nt.push_back(t);
     E->types_h.swap(nt);
+    // bonds: those of deleted particles go, the rest follow the new ids
+    if (!E->bond_pot_h.empty()) {
+        std::vector<int> nid(std::max<long long>(N, 1), -1);
+        long long c = 0;
+        for (long long i = 0; i < N; ++i)
+            if (!gone[i]) nid[i] = (int)c++;
+        std::vector<int> ij, pot;
+        for (size_t b = 0; b < E->bond_pot_h.size(); ++b) {
+            const int i = nid[E->bond_ij_h[2 * b]], j = nid[E->bond_ij_h[2 * b + 1]];
+            if (i < 0 || j < 0) continue;
+            ij.push_back(i);
+            ij.push_back(j);
+            pot.push_back(E->bond_pot_h[b]);
+        }
+        E->bond_ij_h.swap(ij);
+        E->bond_pot_h.swap(pot);
+        rc = upload_bonds<R>(E);
+        if (rc) { E->part_off.clear(); return rc; }
+    }
     rc = reset_counters(E, E->step_h);
     if (rc) return rc;
     if (E->nb_mode == RDGPU_NB_LIST && N2 > 0) {
@@ -1642,6 +1789,19 @@ int rdgpu_apply_edits(rdgpu_handle h, const float* edits, int64_t count)
     if (E->nsys != 1) return fail(E, RDGPU_ERR_ARG, "reaction edits are defined for a single system");
     if (count < 0 || (count > 0 && !edits)) return fail(E, RDGPU_ERR_ARG, "invalid edit array");
     return DISPATCH(E, apply_edits_impl, E, edits, (long long)count);
+}
+
+int rdgpu_set_bonds(rdgpu_handle h, int64_t n_bonds, const int32_t* ij, const int32_t* pot, int32_t n_pots,
+                    const rdgpu_pair_pot* pots)
+{
+    Engine* E = (Engine*)h;
+    GUARD(E);
+    NEED_PARTICLES(E);
+    if (E->nsys != 1) return fail(E, RDGPU_ERR_ARG, "bonds are defined for a single system");
+    if (n_bonds < 0 || n_pots < 0 || (n_bonds > 0 && (!ij || !pot || !pots || n_pots < 1)))
+        return fail(E, RDGPU_ERR_ARG, "invalid bond arrays");
+    if (n_bonds > 0x3fffffff) return fail(E, RDGPU_ERR_ARG, "too many bonds");
+    return DISPATCH(E, set_bonds_impl, E, (long long)n_bonds, (const int*)ij, (const int*)pot, (int)n_pots, pots);
 }
 
 int rdgpu_get_particles(rdgpu_handle h, double* xyz, int32_t* types)

@@ -58,6 +58,12 @@ template <class R> struct Args {
     const long long* step_ptr;
     int step_off;
     const double* noise;            // injected noise (3 per global index) or null
+    // bonded pairs of particle groups (single system; null: none)
+    const int* bstart;              // bonds of particle id: bstart[id] .. bstart[id+1]
+    const int* bpart;               // partner id of each bond entry
+    const int* bterm;               // its potential term
+    const PairTerm<R>* btab;        // resolved bond potential terms
+    int* inv;                       // sorted index of each particle id (kept by the scatters)
 };
 
 // force accumulators: FP32 sums pair forces in 2^-32 fixed point (exact,
@@ -520,6 +526,40 @@ __device__ __forceinline__ int em_update(double x[3], double* /*c*/, int& w, con
 // ---------------------------------------------------------------------------
 // The step kernel: one thread per particle of the sorted arrays
 // ---------------------------------------------------------------------------
+// forces (and, for MODE 1, half energies) of the bonds of particle id: one
+// pair potential each, at any distance, minimum image (the groups of
+// ReaDDy; CudaSimulation.cu:1829-1836 with each particle's own type)
+template <class R, int MODE>
+__device__ __forceinline__ void bond_forces(const Args<R>& a, const State<R>& st, int id, const R xi[3],
+                                            const SysDev& s, Acc<R>& acc)
+{
+    Box<R> bx;
+    bx.load(s);
+    for (int b = a.bstart[id]; b < a.bstart[id + 1]; ++b) {
+        const int j = a.inv[a.bpart[b]];
+        R xj[3];
+        int wj;
+        load_pos(st, j, xj, wj);
+        const R dx = mimg_sel(xi[0], xj[0], bx.L[0], bx.half[0], s.per[0]);
+        const R dy = mimg_sel(xi[1], xj[1], bx.L[1], bx.half[1], s.per[1]);
+        const R dz = mimg_sel(xi[2], xj[2], bx.L[2], bx.half[2], s.per[2]);
+        const R r = sqrt(dist2(dx, dy, dz));
+        R pre, e;
+        pair_term(a.btab[a.bterm[b]], r, pre, e);
+        acc.add(pre, dx, dy, dz);
+        if (MODE == 1) acc.e += R(0.5) * e;
+    }
+}
+
+// sorted index of every particle id
+template <class R>
+__global__ void inv_kernel(State<R> cur, long long ntot, int* __restrict__ inv)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ntot;
+         i += (long long)gridDim.x * blockDim.x)
+        inv[load_id(cur, i)] = (int)i;
+}
+
 template <class R, bool VALUE_IMAGE, bool HREP, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) step_kernel(Args<R> a)
 {
@@ -576,6 +616,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) step_kernel(Arg
     else
         neighbourhood_flat<R, HREP, BLOCK, CAP>(a.cur, a.start, s, cc, i, xi, ti, s_rc2, &s_ft, a.tab, acc,
                                                 s_rmax2[ti], s_j0, s_j1, s_list);
+    if (a.bstart) bond_forces<R, 0>(a, a.cur, id, xi, s, acc);
     R F[3];
     acc.force(F);
     if (a.n_ext > 0) {
@@ -714,17 +755,21 @@ __global__ void __launch_bounds__(SCAN_BLOCK) scan_apply_kernel(int* __restrict_
 
 template <class R>
 __global__ void scatter_kernel(State<R> stg, State<R> dst, const int* __restrict__ tcell, const int* __restrict__ tslot,
-                               const int* __restrict__ start, long long ntot, const int* err)
+                               const int* __restrict__ start, long long ntot, const int* err, int* __restrict__ inv)
 {
     if (*((volatile const int*)err)) return;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ntot;
          i += (long long)gridDim.x * blockDim.x) {
         const long long d = start[tcell[i]] + tslot[i];
         if constexpr (sizeof(R) == 4) {
+            const float4 q = stg.aux[i];
             dst.pos[d] = stg.pos[i];
-            dst.aux[d] = stg.aux[i];
+            dst.aux[d] = q;
+            if (inv) inv[__float_as_int(q.w)] = (int)d;
         } else {
-            dst.rec[d] = stg.rec[i];
+            const Rec64 r = stg.rec[i];
+            dst.rec[d] = r;
+            if (inv) inv[r.id] = (int)d;
         }
     }
 }
@@ -958,6 +1003,7 @@ __global__ void diag_kernel(Args<R> a, double* forces, double* energy, int* ncou
         unsigned long long hh = 0;
         neighbourhood<R, MODE, VALUE_IMAGE, false>(a.cur, a.start, s, cc, (int)i, xi, ti, s_rc2, nullptr, a.tab,
                                                    acc, nc, hh, s_rmax2[ti]);
+        if (MODE == 1 && a.bstart) bond_forces<R, 1>(a, a.cur, load_id(a.cur, i), xi, s, acc);
         if (MODE == 2) {
             ncount[g] = nc;
             hashes[g] = hh;
@@ -1335,6 +1381,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) list_step_kerne
             }
         }
     }
+    if (a.bstart) bond_forces<R, 0>(a, cur, id, xi, s, acc);
     R F[3];
     acc.force(F);
     if (a.n_ext > 0) {
@@ -1395,10 +1442,14 @@ __global__ void list_scatter_kernel(Args<R> a, ListArgs<R> v, long long off)
          i += (long long)gridDim.x * blockDim.x) {
         const long long d = a.start[a.tcell[i]] + a.tslot[i];
         if constexpr (sizeof(R) == 4) {
+            const float4 q = src.aux[i];
             dst.pos[d] = src.pos[i];
-            dst.aux[d] = src.aux[i];
+            dst.aux[d] = q;
+            if (a.inv) a.inv[__float_as_int(q.w)] = (int)d;
         } else {
-            dst.rec[d] = src.rec[i];
+            const Rec64 r = src.rec[i];
+            dst.rec[d] = r;
+            if (a.inv) a.inv[r.id] = (int)d;
         }
     }
 }

@@ -133,6 +133,18 @@ class Engine:
         self._check(_lib().rdgpu_get_particles(self._h, _p(xyz, C.c_double), _p(types, C.c_int32)))
         return xyz, types
 
+    def set_bonds(self, ij, pot, potentials):
+        """Bonded pairs of particle groups: ij (n, 2) particle indices, pot (n,)
+        indices into potentials (PairPotential, type pairs ignored)."""
+        from .system import System
+        ij = np.ascontiguousarray(ij, dtype=np.int32).reshape(-1, 2)
+        pot = np.ascontiguousarray(pot, dtype=np.int32).reshape(-1)
+        arr = (A.PairPot * max(1, len(potentials)))()
+        for k, p in enumerate(potentials):
+            arr[k] = System.pot_struct(p)
+        self._check(_lib().rdgpu_set_bonds(self._h, ij.shape[0], _p(ij, C.c_int32), _p(pot, C.c_int32),
+                                           len(potentials), C.cast(arr, C.c_void_p)))
+
     def apply_edits(self, edits):
         """Reaction edits in the layout of ReaDDy's cReactions entries:
         rows of (readdyId, newType, x, y, z, gpuIndex)."""

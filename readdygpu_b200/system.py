@@ -109,6 +109,18 @@ class System:
                 m = max(m, c)
         return m
 
+    @staticmethod
+    def pot_struct(p):
+        """A PairPotential as a C rdgpu_pair_pot (type pairs not filled: for bonds)."""
+        q = A.PairPot()
+        q.kind = p.kind
+        q.subtype = A.SUBTYPES[p.subtype] if p.kind == A.P2_HARMONIC else 0
+        q.k = p.k
+        q.r0 = -1.0 if p.r0 is None else float(p.r0)
+        q.length = p.length
+        q.depth = p.depth
+        return q
+
     def to_desc(self):
         """Pack into the C struct rdgpu_system_desc."""
         if not 1 <= self.n_types <= A.MAX_TYPES:
