@@ -26,9 +26,8 @@ typedef struct {
     int32_t reserved;
 } rdgpu_run_params;
 
-/* Parse the input files.  Paths may be NULL/empty for param_groups and
-   tplgy_groups (groups are not part of this core).  Returns RDGPU_OK or
-   RDGPU_ERR_ARG with a message in rdgpu_inputs_error(NULL).                 */
+/* Parse the input files (groups: rdgpu_inputs_read_groups).  Returns
+   RDGPU_OK or RDGPU_ERR_ARG with a message in rdgpu_inputs_error(NULL).      */
 int rdgpu_inputs_read(const char* param_particles, const char* tplgy_potentials,
                       const char* param_global, const char* tplgy_coordinates,
                       double max_cutoff, rdgpu_inputs_handle* out);
@@ -36,6 +35,19 @@ int rdgpu_inputs_desc(rdgpu_inputs_handle h, rdgpu_system_desc* desc, rdgpu_run_
 int64_t rdgpu_inputs_count(rdgpu_inputs_handle h);
 /* xyz: 3n doubles, types: n, ids: n (the ReaDDy particle ids)               */
 int rdgpu_inputs_particles(rdgpu_inputs_handle h, double* xyz, int32_t* types, int32_t* ids);
+/* Particle groups (param_groups.xml, tplgy_groups.xml) as bonded pairs for
+   rdgpu_set_bonds: the k-th <particleGroup> is group type k; each of its
+   HARMONIC / WEAK_INTERACTION_PIECEWISE_HARMONIC potentials acts on the
+   internal-id pairs of its affectedInternalIdPairs; each <g type="k"
+   internalAndParticleId="[[u,id];...]"> instance maps internal ids to the
+   ReaDDy particle ids of tplgy_coordinates.  Replaces GroupParametersHandler
+   (GroupParametersHandler.cpp:41-190) and GroupReader (GroupReader.cpp:13-40).
+   Other group potential types are counted in n_unsupported and skipped.     */
+int rdgpu_inputs_read_groups(rdgpu_inputs_handle h, const char* param_groups, const char* tplgy_groups);
+int rdgpu_inputs_bond_counts(rdgpu_inputs_handle h, int64_t* n_bonds, int32_t* n_pots, int32_t* n_unsupported);
+/* ij: 2 x n_bonds gpu indices (positions in tplgy_coordinates), pot: n_bonds,
+   pots: n_pots                                                               */
+int rdgpu_inputs_bonds(rdgpu_inputs_handle h, int32_t* ij, int32_t* pot, rdgpu_pair_pot* pots);
 const char* rdgpu_inputs_error(rdgpu_inputs_handle h);
 void rdgpu_inputs_free(rdgpu_inputs_handle h);
 

@@ -72,12 +72,30 @@ extern "C" JNIEXPORT void JNICALL Java_readdy_impl_sim_top_TopGPU_cCreateSimulat
     std::vector<double> xyz(3 * n);
     std::vector<int32_t> types(n), ids(n);
     rdgpu_inputs_particles(in, xyz.data(), types.data(), ids.data());
+    // particle groups -> bonded pairs (the reference's groups kernel,
+    // CudaSimulation.cu:1829-1836, fed by GroupReader.cpp:13-40)
+    std::vector<int32_t> bond_ij, bond_pot;
+    std::vector<rdgpu_pair_pot> bond_pots;
+    if (file_has(tgr, "<g ")) {
+        if (rdgpu_inputs_read_groups(in, pgr.c_str(), tgr.c_str()) != RDGPU_OK) {
+            printf("error while reading groups: %s\n", rdgpu_inputs_error(in));
+            rdgpu_inputs_free(in);
+            fflush(stdout);
+            return;
+        }
+        int64_t nb = 0;
+        int32_t np = 0, nu = 0;
+        rdgpu_inputs_bond_counts(in, &nb, &np, &nu);
+        bond_ij.resize(2 * nb);
+        bond_pot.resize(nb);
+        bond_pots.resize(np);
+        rdgpu_inputs_bonds(in, bond_ij.data(), bond_pot.data(), bond_pots.data());
+        if (nu > 0) printf("note: %d group potential(s) not handled by this core were skipped\n", nu);
+    }
     rdgpu_inputs_free(in);
     const bool verbose = testmode || run.testmode;
     if (run.n_unsupported > 0)
         printf("note: %d potential(s) not handled by this core were skipped\n", run.n_unsupported);
-    if (file_has(tgr, "<g ") || file_has(pgr, "<group"))
-        printf("note: particle groups are not handled by this core\n");
 
     rdgpu_options opt;
     memset(&opt, 0, sizeof(opt));
@@ -92,7 +110,9 @@ extern "C" JNIEXPORT void JNICALL Java_readdy_impl_sim_top_TopGPU_cCreateSimulat
         fflush(stdout);
         return;
     }
-    if (rdgpu_set_particles(h, nullptr, n, xyz.data(), types.data()) != RDGPU_OK) {
+    if (rdgpu_set_particles(h, nullptr, n, xyz.data(), types.data()) != RDGPU_OK ||
+        (!bond_pot.empty() && rdgpu_set_bonds(h, (int64_t)bond_pot.size(), bond_ij.data(), bond_pot.data(),
+                                              (int32_t)bond_pots.size(), bond_pots.data()) != RDGPU_OK)) {
         printf("error during initialization: %s\n", rdgpu_last_error(h));
         rdgpu_destroy(h);
         fflush(stdout);

@@ -1,5 +1,6 @@
 // xml_input.cpp -- Xerces-free reader of the ReaDDy input files and the
 // C API of include/readdy_b200_inputs.h.
+#include <map>
 #include "xml_input.h"
 
 #include <cmath>
@@ -152,6 +153,10 @@ struct rdgpu_inputs {
     std::vector<double> xyz;
     std::vector<int32_t> types, ids;
     std::string error;
+    // particle groups as bonds: gpu indices, potential index, potentials
+    std::vector<int32_t> bond_ij, bond_pot;
+    std::vector<rdgpu_pair_pot> bond_pots;
+    int32_t groups_unsupported = 0;
 };
 
 namespace {
@@ -345,9 +350,106 @@ int read_all(rdgpu_inputs* I, const char* pp, const char* tp, const char* pg, co
     }
     return RDGPU_OK;
 }
+// param_groups.xml / tplgy_groups.xml (GroupParametersHandler.cpp:41-190,
+// GroupReader.cpp:13-40): group type k is the k-th <particleGroup>; each of
+// its HARMONIC / WEAK_INTERACTION_PIECEWISE_HARMONIC potentials acts on the
+// internal-id pairs it names; a <g type="k" internalAndParticleId="[[u,id];...]">
+// instance maps internal ids to ReaDDy particle ids.
+int read_groups(rdgpu_inputs* I, const char* pgr, const char* tgr)
+{
+    I->bond_ij.clear();
+    I->bond_pot.clear();
+    I->bond_pots.clear();
+    I->groups_unsupported = 0;
+    std::unique_ptr<rdxml::Node> root;
+    if (!load(pgr, root, I->error)) return RDGPU_ERR_ARG;
+    struct GroupPot { int index; std::vector<std::pair<int, int>> pairs; };
+    std::vector<std::vector<GroupPot>> gtypes;
+    for (const rdxml::Node* g : root->children("particleGroup")) {
+        std::vector<GroupPot> gp;
+        if (const rdxml::Node* ps = g->child("potentials")) {
+            for (const rdxml::Node* p : ps->children("pot")) {
+                auto at = [&](const char* kk, const char* dflt = "") {
+                    auto it = p->attrs.find(kk);
+                    return it == p->attrs.end() ? std::string(dflt) : it->second;
+                };
+                const std::string type = at("type");
+                if (type != "HARMONIC" && type != "WEAK_INTERACTION_PIECEWISE_HARMONIC") {
+                    I->groups_unsupported++;   // e.g. StiffnessInteraction
+                    continue;
+                }
+                rdgpu_pair_pot q;
+                memset(&q, 0, sizeof(q));
+                q.kind = type == "HARMONIC" ? RDGPU_P2_HARMONIC : RDGPU_P2_WEAK_PIECEWISE;
+                q.subtype = q.kind == RDGPU_P2_HARMONIC ? subtype_of(at("subtype")) : 0;
+                if (q.kind == RDGPU_P2_HARMONIC && q.subtype == 0) { I->error = "param_groups: harmonic subtype missing"; return RDGPU_ERR_ARG; }
+                q.k = atof(at("forceConst", "0").c_str());
+                const std::string r0 = rdxml::trim(at("r0", "null"));
+                q.r0 = (r0.empty() || r0 == "null") ? -1.0 : atof(r0.c_str());
+                q.length = atof(at("length", "0").c_str());
+                q.depth = atof(at("depth", "0").c_str());
+                I->bond_pots.push_back(q);
+                std::vector<std::pair<int, int>> prs;
+                std::vector<double> v = numbers(at("affectedInternalIdPairs"));
+                for (size_t t = 0; t + 1 < v.size(); t += 2) prs.push_back({(int)v[t], (int)v[t + 1]});
+                gp.push_back({(int)I->bond_pots.size() - 1, prs});
+            }
+        }
+        gtypes.push_back(gp);
+    }
+    if (!load(tgr, root, I->error)) return RDGPU_ERR_ARG;
+    std::map<int, int> index_of;   // ReaDDy particle id -> gpu index
+    for (size_t i = 0; i < I->ids.size(); ++i) index_of[I->ids[i]] = (int)i;
+    for (const rdxml::Node* g : root->children("g")) {
+        auto it = g->attrs.find("type");
+        auto ip = g->attrs.find("internalAndParticleId");
+        if (it == g->attrs.end() || ip == g->attrs.end()) { I->error = "tplgy_groups: <g> needs type and internalAndParticleId"; return RDGPU_ERR_ARG; }
+        const int gt = atoi(it->second.c_str());
+        if (gt < 0 || gt >= (int)gtypes.size()) { I->error = "tplgy_groups: group type out of range"; return RDGPU_ERR_ARG; }
+        std::map<int, int> part;
+        std::vector<double> v = numbers(ip->second);
+        for (size_t t = 0; t + 1 < v.size(); t += 2) {
+            auto f = index_of.find((int)v[t + 1]);
+            if (f == index_of.end()) { I->error = "tplgy_groups: unknown particle id " + std::to_string((int)v[t + 1]); return RDGPU_ERR_ARG; }
+            part[(int)v[t]] = f->second;
+        }
+        for (const GroupPot& p : gtypes[gt])
+            for (auto& pr : p.pairs) {
+                if (!part.count(pr.first) || !part.count(pr.second)) { I->error = "tplgy_groups: internal id missing from a group instance"; return RDGPU_ERR_ARG; }
+                I->bond_ij.push_back(part[pr.first]);
+                I->bond_ij.push_back(part[pr.second]);
+                I->bond_pot.push_back(p.index);
+            }
+    }
+    return RDGPU_OK;
+}
 }  // namespace
 
 extern "C" {
+
+int rdgpu_inputs_read_groups(rdgpu_inputs_handle h, const char* param_groups, const char* tplgy_groups)
+{
+    if (!h) return RDGPU_ERR_ARG;
+    return read_groups(h, param_groups, tplgy_groups);
+}
+
+int rdgpu_inputs_bond_counts(rdgpu_inputs_handle h, int64_t* n_bonds, int32_t* n_pots, int32_t* n_unsupported)
+{
+    if (!h) return RDGPU_ERR_ARG;
+    if (n_bonds) *n_bonds = (int64_t)h->bond_pot.size();
+    if (n_pots) *n_pots = (int32_t)h->bond_pots.size();
+    if (n_unsupported) *n_unsupported = h->groups_unsupported;
+    return RDGPU_OK;
+}
+
+int rdgpu_inputs_bonds(rdgpu_inputs_handle h, int32_t* ij, int32_t* pot, rdgpu_pair_pot* pots)
+{
+    if (!h) return RDGPU_ERR_ARG;
+    if (ij) memcpy(ij, h->bond_ij.data(), h->bond_ij.size() * sizeof(int32_t));
+    if (pot) memcpy(pot, h->bond_pot.data(), h->bond_pot.size() * sizeof(int32_t));
+    if (pots) memcpy(pots, h->bond_pots.data(), h->bond_pots.size() * sizeof(rdgpu_pair_pot));
+    return RDGPU_OK;
+}
 
 int rdgpu_inputs_read(const char* param_particles, const char* tplgy_potentials, const char* param_global,
                       const char* tplgy_coordinates, double max_cutoff, rdgpu_inputs_handle* out)

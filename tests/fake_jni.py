@@ -137,10 +137,11 @@ class FakeJVM:
         f(C.byref(self.env), obj, int(testmode), *js)
 
 
-def write_inputs(d, n=400, frames=3, seed=1, L=40.0):
+def write_inputs(d, n=400, frames=3, seed=1, L=40.0, dimers=0):
     """ReaDDy input files (param_particles, tplgy_potentials, param_global,
-    tplgy_coordinates; empty groups) for a 2-species system in a periodic box
-    with a CUBE wall and harmonic repulsion."""
+    tplgy_coordinates, param_groups, tplgy_groups) for a 2-species system in
+    a periodic box with a CUBE wall and harmonic repulsion; the first
+    2 x dimers particles form spring-bonded dimer groups."""
     rng = np.random.default_rng(seed)
     p = {k: str(d / f"{k}.xml") for k in ("param_particles", "tplgy_potentials", "param_groups",
                                           "tplgy_coordinates", "tplgy_groups", "param_global")}
@@ -182,11 +183,38 @@ def write_inputs(d, n=400, frames=3, seed=1, L=40.0):
 """)
     xyz = rng.uniform(-h + 1, h - 1, size=(n, 3))
     types = rng.integers(0, 2, n)
+    for g in range(dimers):   # partner 3 nm away along x
+        xyz[2 * g + 1] = xyz[2 * g] + [3.0, 0.0, 0.0]
+        types[2 * g] = types[2 * g + 1] = 0
     lines = ['<tplgy_coords version="1.1" stepId="0">']
     for i in range(n):
         lines.append(f'<p id="{1000 + i}" type="{types[i]}" c="{float(xyz[i, 0])!r},{float(xyz[i, 1])!r},{float(xyz[i, 2])!r}"/>')
     lines.append("</tplgy_coords>")
     open(p["tplgy_coordinates"], "w").write("\n".join(lines) + "\n")
-    open(p["param_groups"], "w").write('<param_groups version="1.1"></param_groups>\n')
-    open(p["tplgy_groups"], "w").write('<tplgy_groups version="1.1"></tplgy_groups>\n')
+    if dimers:
+        open(p["param_groups"], "w").write("""<param_groups version="1.1">
+ <particleGroup>
+  <type>dimer</type>
+  <templateOrigin>[0.0,0.0,0.0]</templateOrigin>
+  <templateNormal>[0,0,1]</templateNormal>
+  <buildingBlocks>
+   <particle internalId="0" type="A" templateC="[0.0,0.0,0.0]"/>
+   <particle internalId="1" type="A" templateC="[3.0,0.0,0.0]"/>
+  </buildingBlocks>
+  <potentials>
+   <pot name="spring" type="HARMONIC" subtype="spring" forceConst="20.0" affectedInternalIdPairs="[[0,1]]"/>
+   <pot name="stiff" type="StiffnessInteraction" forceConst="3" affectedInternalIdPairs="[[0,1]]"/>
+  </potentials>
+  <maxNumberOfGroupAssignmentsPerParticle>1</maxNumberOfGroupAssignmentsPerParticle>
+ </particleGroup>
+</param_groups>
+""")
+        g = ['<tplgy_groups version="1.1">']
+        for i in range(dimers):
+            g.append(f'<g id="{i}" type="0" internalAndParticleId="[[0,{1000 + 2 * i}];[1,{1001 + 2 * i}]]"/>')
+        g.append("</tplgy_groups>")
+        open(p["tplgy_groups"], "w").write("\n".join(g) + "\n")
+    else:
+        open(p["param_groups"], "w").write('<param_groups version="1.1"></param_groups>\n')
+        open(p["tplgy_groups"], "w").write('<tplgy_groups version="1.1"></tplgy_groups>\n')
     return p, xyz, types

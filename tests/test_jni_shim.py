@@ -24,6 +24,24 @@ class RunParams(C.Structure):
                 ("reserved", C.c_int32)]
 
 
+def inputs_lib():
+    L = jni_lib()
+    V, I64P, I32P = C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int32)
+    L.rdgpu_inputs_read.restype = C.c_int
+    L.rdgpu_inputs_read.argtypes = [C.c_char_p] * 4 + [C.c_double, C.POINTER(C.c_void_p)]
+    L.rdgpu_inputs_read_groups.restype = C.c_int
+    L.rdgpu_inputs_read_groups.argtypes = [V, C.c_char_p, C.c_char_p]
+    L.rdgpu_inputs_bond_counts.restype = C.c_int
+    L.rdgpu_inputs_bond_counts.argtypes = [V, I64P, I32P, I32P]
+    L.rdgpu_inputs_bonds.restype = C.c_int
+    L.rdgpu_inputs_bonds.argtypes = [V, I32P, I32P, C.POINTER(A.PairPot)]
+    L.rdgpu_inputs_error.restype = C.c_char_p
+    L.rdgpu_inputs_error.argtypes = [V]
+    L.rdgpu_inputs_free.restype = None
+    L.rdgpu_inputs_free.argtypes = [V]
+    return L
+
+
 def read_inputs(paths, max_cutoff=10.0):
     L = jni_lib()
     L.rdgpu_inputs_read.restype = C.c_int
@@ -156,6 +174,49 @@ def test_jni_protocol_frames_and_reactions(tmp_path, capfd):
     assert ids2[-2:] == [5000, 5001]
     np.testing.assert_array_equal(r2[:, 3], np.arange(n0 - 1))
     assert np.abs(r2[-2, :3] - [1.0, 2.0, 3.0]).max() < 1.0
+
+
+def test_input_groups_as_bonds(tmp_path):
+    """param_groups / tplgy_groups become bonded pairs: one spring per dimer
+    instance, gpu indices from the particle ids; unsupported group potentials
+    are counted and skipped."""
+    paths, _, _ = write_inputs(tmp_path, n=50, dimers=5)
+    L = inputs_lib()
+    h = C.c_void_p()
+    assert L.rdgpu_inputs_read(paths["param_particles"].encode(), paths["tplgy_potentials"].encode(),
+                               paths["param_global"].encode(), paths["tplgy_coordinates"].encode(), 10.0,
+                               C.byref(h)) == 0
+    assert L.rdgpu_inputs_read_groups(h, paths["param_groups"].encode(), paths["tplgy_groups"].encode()) == 0
+    nb, npot, nu = C.c_int64(), C.c_int32(), C.c_int32()
+    L.rdgpu_inputs_bond_counts(h, C.byref(nb), C.byref(npot), C.byref(nu))
+    assert (nb.value, npot.value, nu.value) == (5, 1, 1)
+    ij = (C.c_int32 * 10)()
+    pot = (C.c_int32 * 5)()
+    pots = (A.PairPot * 1)()
+    L.rdgpu_inputs_bonds(h, ij, pot, pots)
+    assert list(ij) == [0, 1, 2, 3, 4, 5, 6, 7, 8, 9] and list(pot) == [0] * 5
+    assert pots[0].kind == A.P2_HARMONIC and pots[0].subtype == A.SUBTYPES["spring"] and pots[0].k == 20.0
+    assert pots[0].r0 == -1.0
+    # a group instance naming an unknown particle id is an error
+    open(paths["tplgy_groups"], "w").write('<tplgy_groups><g id="0" type="0" internalAndParticleId="[[0,5];[1,6]]"/></tplgy_groups>')
+    assert L.rdgpu_inputs_read_groups(h, paths["param_groups"].encode(), paths["tplgy_groups"].encode()) != 0
+    assert b"unknown particle id" in L.rdgpu_inputs_error(h)
+    L.rdgpu_inputs_free(h)
+
+
+@pytest.mark.gpu
+def test_jni_groups_hold_dimers_together(tmp_path, capfd):
+    """Spring-bonded dimers from the group files stay at about their rest
+    length (3 nm, sqrt(kT/k) = 0.35 nm) through the frames."""
+    paths, _, _ = write_inputs(tmp_path, n=200, frames=5, dimers=20)
+    seen = {}
+    jvm = FakeJVM(lambda f, a: seen.__setitem__(f, a.copy()) or True)
+    jvm.run(jni_lib(), paths)
+    out = capfd.readouterr().out
+    assert "END" in out and "error" not in out.lower()
+    rec = seen[4][1:].reshape(-1, 5)
+    d = np.linalg.norm(rec[0:40:2, :3] - rec[1:40:2, :3], axis=1)
+    assert np.all(np.abs(d - 3.0) < 2.0), d
 
 
 @pytest.mark.gpu
