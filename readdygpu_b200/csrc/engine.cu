@@ -684,10 +684,17 @@ template <class R> int add_conditional_chain(Engine* E, const Args<R>& a, const 
 template <class R> void launch_list_step_kernel(Engine* E, const Args<R>& a, const ListArgs<R>& v)
 {
     const int grid = (int)((E->npart_tot + kStepBlock - 1) / kStepBlock);
-    if (E->hrep)
-        list_step_kernel<R, true, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a, v);
+    bool allper = true;
+    for (int s = 0; s < E->nsys; ++s)
+        for (int q = 0; q < 3; ++q) allper = allper && E->sys_h[s].per[q];
+    if (E->hrep && allper)
+        list_step_kernel<R, true, true, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a, v);
+    else if (E->hrep)
+        list_step_kernel<R, true, false, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a, v);
+    else if (allper)
+        list_step_kernel<R, false, true, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a, v);
     else
-        list_step_kernel<R, false, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a, v);
+        list_step_kernel<R, false, false, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a, v);
     ++E->launches;
 }
 

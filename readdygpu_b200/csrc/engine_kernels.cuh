@@ -571,7 +571,8 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) step_kernel(Arg
     __shared__ int s_j0[FLAT ? 9 * BLOCK : 1], s_j1[FLAT ? 9 * BLOCK : 1];
     __shared__ PairRec<R> s_list[FLAT ? CAP * BLOCK : 1];
     if (*((volatile int*)a.err)) return;   // an earlier step failed: keep its input intact
-    for (int k = threadIdx.x; k < MAXT * MAXT; k += BLOCK) {
+    // rows of the S types in use (entries (ti, tj) with ti >= S are never read)
+    for (int k = threadIdx.x; k < MAXT * a.tab->S; k += BLOCK) {
         s_rc2[k] = a.tab->rc2[k];
         if (HREP) {
             s_ft.k[k] = a.tab->nterm[k] ? a.tab->term[k * MAX_TERMS].k : R(0);
@@ -1293,14 +1294,16 @@ __device__ __forceinline__ void store_state(const State<double>& st, long long i
     st.rec[i] = r;
 }
 
-// one BD step of every particle over its pair list
-template <class R, bool HREP, int BLOCK>
+// one BD step of every particle over its pair list; ALLPER: every axis of
+// every system is periodic (the minimum image needs no per-axis test)
+template <class R, bool HREP, bool ALLPER, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) list_step_kernel(Args<R> a, ListArgs<R> v)
 {
     __shared__ R s_rc2[MAXT * MAXT];
     __shared__ FastTab<R> s_ft;
     if (*((volatile int*)a.err)) return;   // an earlier step failed: keep its input intact
-    for (int k = threadIdx.x; k < MAXT * MAXT; k += BLOCK) {
+    // rows of the S types in use (entries (ti, tj) with ti >= S are never read)
+    for (int k = threadIdx.x; k < MAXT * a.tab->S; k += BLOCK) {
         s_rc2[k] = a.tab->rc2[k];
         if (HREP) {
             s_ft.k[k] = a.tab->nterm[k] ? a.tab->term[k * MAX_TERMS].k : R(0);
@@ -1355,9 +1358,9 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) list_step_kerne
 #pragma unroll
         for (int u = 0; u < LCHUNK; ++u) {
             if (jj[u] < 0) continue;
-            const R dx = mimg_sel(xi[0], xj[u][0], bx.L[0], bx.half[0], p0);
-            const R dy = mimg_sel(xi[1], xj[u][1], bx.L[1], bx.half[1], p1);
-            const R dz = mimg_sel(xi[2], xj[u][2], bx.L[2], bx.half[2], p2);
+            const R dx = mimg_sel(xi[0], xj[u][0], bx.L[0], bx.half[0], ALLPER ? 1 : p0);
+            const R dy = mimg_sel(xi[1], xj[u][1], bx.L[1], bx.half[1], ALLPER ? 1 : p1);
+            const R dz = mimg_sel(xi[2], xj[u][2], bx.L[2], bx.half[2], ALLPER ? 1 : p2);
             const R r2 = dist2(dx, dy, dz);
             const int pidx = ti * MAXT + (wj[u] & 0xff);
             if (r2 < s_rc2[pidx]) {
