@@ -121,10 +121,8 @@ class Clocks:
 
 
 def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
+    from readdygpu_b200 import replicas
+    return replicas.env()
 
 
 def workload(config, rank):
@@ -235,18 +233,16 @@ def run_ours(args):
     import torch
     import readdygpu_b200 as R
 
+    from readdygpu_b200 import replicas
     ws, rank, local = dist_env()
-    if ws > 1:
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     torch.cuda.set_device(local)
+    replicas.init("nccl")
     w = workload(args.config, rank)
     kw = {}
     if w.boxes is not None:
         # each rank owns its own replicate ensemble: shift the seeds
-        kw["boxes"] = [(lo, hi, per, sd + 7919 * rank) for (lo, hi, per, sd) in w.boxes]
-    eng = R.Engine(w.system, precision=args.precision, device=local, seed=11 + rank,
+        kw["boxes"] = replicas.replica_boxes(w.boxes, rank)
+    eng = R.Engine(w.system, precision=args.precision, device=local, seed=replicas.replica_seed(11, rank),
                    neighbour_mode=args.neighbour, skin=args.skin, **kw)
     eng.set_particles(w.xyz, w.types, offsets=w.offsets)
     stream = torch.cuda.ExternalStream(eng.stream, device=local)
@@ -255,9 +251,7 @@ def run_ours(args):
     nb = eng.metrics()
 
     def barrier():
-        torch.cuda.synchronize()
-        if ws > 1:
-            torch.distributed.barrier()
+        replicas.barrier()
 
     # ---- device-timed, state resident in HBM ----------------------------
     l0 = eng.launch_count()
@@ -274,12 +268,9 @@ def run_ours(args):
     ms = ev0.elapsed_time(ev1)
     # the dominant kernel alone: CUDA events around each fused step-kernel launch
     kernel_ms, sort_ms = eng.step_profile(min(100, max(10, args.steps // 5)))
-    t = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
-    if ws > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = replicas.max_over_ranks(ms, f"cuda:{local}")
     n_all = w.n * ws
-    value = n_all * args.steps / (ms_max / 1e3)
+    value = replicas.job_rate(w.n, ws, args.steps, ms_max / 1e3)
     ms_step = ms_max / args.steps
     per_launch_s = kernel_ms / 1e3
     alg = ALG_BYTES[args.precision] * w.n
@@ -304,10 +295,7 @@ def run_ours(args):
             eng.get_particles(xh, th)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
-        tt = torch.tensor([dt], dtype=torch.float64, device=f"cuda:{local}")
-        if ws > 1:
-            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        dt = float(tt.item())
+        dt = replicas.max_over_ranks(dt, f"cuda:{local}")
         h2d = w.n * (3 * 8 + 4) + (len(w.offsets) * 8 if w.offsets is not None else 0)
         d2h = w.n * (3 * 8 + 4)
         e2e = {"value": n_all * frame * frames / dt, "unit": "particle-steps/s",
@@ -343,8 +331,7 @@ def run_ours(args):
                 "plain_f64": plain, "vs_plain_f64": (value / ws / plain["value"]) if plain else None}
         print(json.dumps(line), flush=True)
     eng.close()
-    if ws > 1:
-        torch.distributed.destroy_process_group()
+    replicas.finalize()
 
 
 def main():
