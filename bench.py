@@ -4,11 +4,15 @@
                     [--config 4] [--precision f32c|f64]
 
 A "step" is one Brownian-dynamics step of the whole workload (all systems of
-the batch): pair forces over 27-cell neighbourhoods, external forces, the
-Euler-Maruyama update with Philox noise and the re-binning, i.e. one launch
-of the fused step kernel.  The default workload is the batched ensemble
-(512 periodic systems, N log-uniform in [500, 20000], 2.45 M particles), the
-configuration the FP32-batched-vs-FP64 metric is quoted on.
+the batch): pair forces, external forces, the Euler-Maruyama update with
+Philox noise and whatever neighbour bookkeeping the step needs.  With the
+neighbour search the autotuner picks (rdgpu_autotune, outside the timed
+region) that is either the cell walk (step kernel + counting sort) or the
+pair list (step kernel + a conditional re-sort and list build when a
+particle has moved more than about skin/2).  The default workload is the
+batched ensemble (512 periodic systems, N log-uniform in [500, 20000],
+2.45 M particles), the configuration the FP32-batched-vs-FP64 metric is
+quoted on.
 
 value: particle-steps/s with the state resident in HBM, device-timed with CUDA
        events on the engine's stream (max over ranks).  The per-step state
@@ -17,6 +21,8 @@ e2e:   the same metric through the C ABI with host buffers: every frame of
        100 steps uploads the particles from pinned host memory
        (rdgpu_set_particles), steps, and downloads them (rdgpu_get_particles),
        the per-frame traffic of the reference's JNI frame loop.
+plain_f64: the north star's denominator, the plain FP64 single-system path:
+       32 of the workload's systems, each alone in its own FP64 handle.
 --impl reference: the CPU path of the reference semantics (the C oracle port,
        all host threads, the reference's Java core cannot run here) on a
        bounded sample of the same workload.

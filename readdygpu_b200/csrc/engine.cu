@@ -532,7 +532,6 @@ int configure_cells(Engine* E, double cut, std::string& why)
         if (nc > (1LL << 26)) { why = "too many cells in one system (box / cutoff too large)"; return RDGPU_ERR_ARG; }
         v.ncells = (int)nc;
         v.cell_base = cb;
-        v.slot_base = 0;
         cb += nc;
     }
     if (cb >= 0x7fffffffLL) { why = "too many cells in the batch"; return RDGPU_ERR_ARG; }
@@ -1033,9 +1032,7 @@ int setup_systems(Engine* E, std::string& why)
             v.half[a] = 0.5 * L;
             v.lo[a] = b.lo[a];
         }
-        v.cap_log2 = 0;
         v.seed = b.seed;
-        v.lanes_log2 = 0;
     }
     if (cudaMalloc(&E->tab_d, tabsz) != cudaSuccess) { why = "cudaMalloc failed"; return -2; }
     cudaMemcpy(E->tab_d, tabbuf.data(), tabsz, cudaMemcpyHostToDevice);

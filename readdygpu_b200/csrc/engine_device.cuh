@@ -1,25 +1,18 @@
-// engine_device.cuh -- device code of the B200 Brownian-dynamics engine.
+// engine_device.cuh -- device-side types and helpers of the B200
+// Brownian-dynamics engine: per-system constants (SysDev), per-type tables,
+// pair and external potentials with the Java semantics, Philox-4x32-10 noise
+// and Box-Muller, IEEE-exact minimum image and distance, error flags.
 //
 // Data layout in HBM (per handle; all systems of a batch share the arrays):
-//   cells:  every system owns ncells = n0*n1*n2 cells of edge L/n (>= cutoff),
-//           cell id = (z*n1 + y)*n0 + x, placed at cell_base in the global cell
-//           arrays.  A cell owns 2^cap_log2 slots starting at
-//           slot_base + (cell << cap_log2).
-//   state:  FP32C: pos[slot] = float4(x, y, z, bits(type | images)),
-//                  cmp[slot] = float4(cx, cy, cz, bits(id)); true = pos - cmp.
-//           FP64:  Rec64{double x, y, z; int w (type | images); int id}.
+//   cells:  every system owns n0*n1*n2 cells of edge L/n (>= the cutoff, or
+//           the cutoff + skin with the pair list), cell id (z*n1 + y)*n0 + x
+//           placed at cell_base in the global cell arrays.
+//   state:  sorted by cell (CSR: particles of cell c are start[c] ..
+//           start[c+1]); FP32C pos[i] = float4(x, y, z, bits(type | images)),
+//           aux[i] = float4(cx, cy, cz, bits(id)), true position x - cx;
+//           FP64 Rec64{double x, y, z; int w (type | images); int id}.
 //           Coordinates are box-relative, in [0, L) on periodic axes.
-//   counts: cnt[3][cells] rotating: step t reads cnt[t%3], claims slots of
-//           the next layout in cnt[(t+1)%3] and clears cnt[(t+2)%3].
-//   Two state buffers alternate: step t reads buffer t&1, writes (t+1)&1.
-//
-// One BD step is ONE kernel (step_kernel): for every particle it sums the
-// pair forces over its 27-cell neighbourhood, adds the external forces, does
-// the Euler-Maruyama update with Philox noise, wraps, and writes the particle
-// into its new cell of the next buffer.  This replaces the reference's
-// orderOne / warpOrderTwo / update sequence with its linked-list relinking
-// (lib/ReaDDyGPU_Cpp/CudaKernels/CudaSimulation.cu:1034-1236, 1402-1782,
-// 1838-1919).
+//   Two state buffers: a step reads one and writes the other.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -31,7 +24,6 @@ constexpr int MAX_TERMS = 4;
 constexpr unsigned FULL = 0xffffffffu;
 
 // error flags
-constexpr int EF_OVERFLOW = 1;
 constexpr int EF_NONFINITE = 2;
 constexpr int EF_JUMP = 4;
 
@@ -44,12 +36,9 @@ struct SysDev {
     int n[3];
     int per[3];
     int ncells;
-    int cap_log2;
     long long cell_base;
-    long long slot_base;
     long long part_base;
     int npart;
-    int lanes_log2;
     float Lf[3], halff[3], invcf[3];
     double L[3], half[3], invc[3];
     double lo[3];
@@ -387,26 +376,6 @@ __device__ __forceinline__ void ext_force(const ExtTerm<R>& p, R prad, const R x
             g[a] += (p.sub == 1) ? -gi : gi;
         }
     }
-}
-
-// neighbour offset d along an axis with n cells: valid and wrapped cell
-__device__ __forceinline__ bool axis_cell(int c, int d, int n, int per, int& out)
-{
-    int v = c + d;
-    if (!per) {
-        out = v;
-        return v >= 0 && v < n;
-    }
-    if (n >= 3) {
-        out = (v < 0) ? v + n : (v >= n ? v - n : v);
-        return true;
-    }
-    if (n == 2) {
-        out = v & 1;
-        return d != -1;   // -1 and +1 are the same cell
-    }
-    out = 0;
-    return d == 0;
 }
 
 __device__ __forceinline__ int warp_incl_scan(int v, int lane)

@@ -17,6 +17,9 @@
 //   scan_tiles      tile sums of the cell counts
 //   scan_apply      cell starts (exclusive prefix), counts cleared
 //   scatter_kernel  staging -> sorted arrays at start[cell] + slot
+// With the pair list (list_step_kernel and the re-sort chain further down) a
+// step is the step kernel and, only when some particle has moved more than
+// about skin/2 since the last build, the re-sort and list build.
 // This replaces the reference's orderOne / warpOrderTwo / update launches and
 // its linked-list relinking under spin locks
 // (lib/ReaDDyGPU_Cpp/CudaKernels/CudaSimulation.cu:1034-1236, 1402-1782,
