@@ -676,23 +676,34 @@ static void rdf_core(const rdgpu_system_desc* d, int64_t n, const double* x,
     const int S = d->n_types;
     cells_t c;
     build_cells(&t, rmax, n, x, &c);
-    for (int64_t i = 0; i < n; ++i) {
-        const int ti = types[i];
-        int64_t st[27], en[27];
-        int nr = neighbour_ranges(&c, &t, x, i, n, st, en);
-        for (int rr = 0; rr < nr; ++rr) for (int64_t q = st[rr]; q < en[rr]; ++q) {
-            const int64_t j = NB_J(&c, q);
-            if (j == i) continue;
-            const int tj = types[j];
-            double dx = mimg(x[3 * i + 0], x[3 * j + 0], t.L[0], t.half[0], t.per[0]);
-            double dy = mimg(x[3 * i + 1], x[3 * j + 1], t.L[1], t.half[1], t.per[1]);
-            double dz = mimg(x[3 * i + 2], x[3 * j + 2], t.L[2], t.half[2], t.per[2]);
-            double r2 = (dx * dx + dy * dy) + dz * dz;
-            if (r2 < e2[nbins]) {
-                int b = rdf_bin(e2, nbins, w, r2);
-                counts[((int64_t)ti * S + tj) * nbins + b] += 1;
+    const int64_t H = (int64_t)S * S * nbins;
+    /* per-thread histograms; integer sums, so the result does not depend on
+       the number of threads                                                 */
+#pragma omp parallel
+    {
+        uint64_t* h = (uint64_t*)calloc((size_t)H, sizeof(uint64_t));
+#pragma omp for schedule(dynamic, 1024)
+        for (int64_t i = 0; i < n; ++i) {
+            const int ti = types[i];
+            int64_t st[27], en[27];
+            int nr = neighbour_ranges(&c, &t, x, i, n, st, en);
+            for (int rr = 0; rr < nr; ++rr) for (int64_t q = st[rr]; q < en[rr]; ++q) {
+                const int64_t j = NB_J(&c, q);
+                if (j == i) continue;
+                const int tj = types[j];
+                double dx = mimg(x[3 * i + 0], x[3 * j + 0], t.L[0], t.half[0], t.per[0]);
+                double dy = mimg(x[3 * i + 1], x[3 * j + 1], t.L[1], t.half[1], t.per[1]);
+                double dz = mimg(x[3 * i + 2], x[3 * j + 2], t.L[2], t.half[2], t.per[2]);
+                double r2 = (dx * dx + dy * dy) + dz * dz;
+                if (r2 < e2[nbins]) {
+                    int b = rdf_bin(e2, nbins, w, r2);
+                    h[((int64_t)ti * S + tj) * nbins + b] += 1;
+                }
             }
         }
+#pragma omp critical
+        for (int64_t q = 0; q < H; ++q) counts[q] += h[q];
+        free(h);
     }
     free_cells(&c);
     free(e2);
