@@ -29,8 +29,11 @@ def test_config3_rdf_full_size_bit_exact(oracle, config3_full, prec):
             e.set_particles(w.xyz, w.types)
             c, _ = e.rdf(200, 20.0, accumulate=False)
         assert np.array_equal(c.reshape(-1), co), (mode, np.abs(c.reshape(-1).astype(np.int64) - co.astype(np.int64)).max())
-    # RSA without overlap: no pair closer than 2 radii (4 nm = bin 40)
-    assert co[:40].sum() == 0 and co.sum() > 0
+    assert co.sum() > 0
+    if prec == "f64":
+        # RSA without overlap: no pair closer than 2 radii (4 nm = bin 40);
+        # FP32 rounding may move near-contact pairs into bin 39
+        assert co[:40].sum() == 0
 
 
 @pytest.mark.parametrize("cfg", [2, 4, 5])
