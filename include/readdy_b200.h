@@ -40,7 +40,7 @@ extern "C" {
 #define RDGPU_OK              0
 #define RDGPU_ERR_ARG        -1   /* invalid argument / description          */
 #define RDGPU_ERR_CUDA       -2   /* CUDA runtime error or no device          */
-#define RDGPU_ERR_OVERFLOW   -3   /* cell occupancy cap could not be grown    */
+#define RDGPU_ERR_OVERFLOW   -3   /* reserved; not returned                   */
 #define RDGPU_ERR_NONFINITE  -4   /* a particle position became NaN/Inf       */
 #define RDGPU_ERR_STATE      -5   /* call out of order (e.g. no particles)    */
 #define RDGPU_ERR_NOMEM      -6   /* device allocation failed                 */
