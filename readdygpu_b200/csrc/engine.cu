@@ -109,7 +109,7 @@ struct rdgpu_engine {
     ListCtl* ctl = nullptr;
     ListCtl* pinned_ctl = nullptr;
     int nbuild_h = 0;
-    int* nbr = nullptr;                  // pair lists, list_cap x list_stride
+    int* nbr = nullptr;                  // pair lists, list_cap x list_stride (groups of 4 per particle)
     float4* xref = nullptr;              // positions at the build and list lengths
     cudaStream_t stream2 = nullptr;      // captures the re-sort into conditional graph nodes
     bool capturing = false;
@@ -607,7 +607,9 @@ int ensure_list(Engine* E, int cap)
 {
     const long long stride = std::max<long long>(E->cap_particles, 1);
     if (cap <= E->list_cap && stride == E->list_stride && E->nbr) return RDGPU_OK;
-    cap = std::max(cap, E->list_cap);
+    // groups of 4 entries (one int4), at least two of them: the step kernel
+    // requests the first 8 entries before it knows the list length
+    cap = (std::max(std::max(cap, E->list_cap), 8) + 3) & ~3;
     if (E->lgraph) { cudaGraphExecDestroy(E->lgraph); E->lgraph = nullptr; }
     dfree(E->nbr); dfree(E->xref);
     E->list_cap = 0;
@@ -1028,6 +1030,7 @@ int setup_systems(Engine* E, std::string& why)
             v.per[a] = b.periodic[a] ? 1 : 0;
             v.Lf[a] = Lf;
             v.halff[a] = 0.5f * Lf;
+            v.ilf[a] = b.periodic[a] ? 1.0f / Lf : 0.0f;
             v.L[a] = L;
             v.half[a] = 0.5 * L;
             v.lo[a] = b.lo[a];

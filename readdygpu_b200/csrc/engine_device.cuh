@@ -40,6 +40,7 @@ struct SysDev {
     long long part_base;
     int npart;
     float Lf[3], halff[3], invcf[3];
+    float ilf[3];     // 1/Lf on periodic axes, 0 on open ones (image by rounding)
     double L[3], half[3], invc[3];
     double lo[3];
     unsigned long long seed;
@@ -167,6 +168,87 @@ __device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, 
 __device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
+// ---------------------------------------------------------------------------
+// Packed FP32 pairs: add/sub/mul/fma.rn.f32x2 of sm_100 work on two floats
+// held in one 64-bit register pair, each lane rounded as the scalar op (an
+// instruction with an explicit rounding mode is never contracted).
+// ---------------------------------------------------------------------------
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 f2_pack(float lo, float hi)
+{
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(f32x2 v, float& lo, float& hi)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 f2_add(f32x2 a, f32x2 b)
+{
+    f32x2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 f2_sub(f32x2 a, f32x2 b)
+{
+    f32x2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 f2_mul(f32x2 a, f32x2 b)
+{
+    f32x2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c)
+{
+    f32x2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+// Operands of pair_disp_x2 for one particle i of system s.
+struct PairFrame {
+    f32x2 xy, il_xy, l_xy;   // (x, y) of i, 1/L or 0, L
+    float z, il_z, l_z;
+    __device__ __forceinline__ void load(const SysDev& s, const float xi[3])
+    {
+        xy = f2_pack(xi[0], xi[1]);
+        il_xy = f2_pack(s.ilf[0], s.ilf[1]);
+        l_xy = f2_pack(s.Lf[0], s.Lf[1]);
+        z = xi[2];
+        il_z = s.ilf[2];
+        l_z = s.Lf[2];
+    }
+};
+
+// FP32 minimum-image displacement and squared distance of a listed pair, x
+// and y as one packed pair.  The image k in {-1, 0, 1} is rint((xi - xj)/L),
+// rounded by adding and subtracting 1.5 2^23 to the exact product with 1/L
+// (0 on open axes, so k = 0); then dx = xi - (xj + k L) and r^2 = (dx^2 +
+// dy^2) + dz^2, one rounding per operation as in mimg and dist2.  k differs
+// from the comparison with L/2 of mimg only when |xi - xj| is within a few
+// ulp of L/2, and then both images are at least L/2 >= 1.5 (rc + skin) apart
+// on that axis (the pair list needs >= 3 cells of edge rc + skin on every
+// periodic axis): the pair is rejected either way, the forces are unchanged.
+__device__ __forceinline__ void pair_disp_x2(const PairFrame& f, float xj, float yj, float zj, float& dx, float& dy,
+                                             float& dz, float& r2)
+{
+    const float M = 12582912.0f;     // 1.5 2^23
+    const f32x2 M2 = f2_pack(M, M), NM2 = f2_pack(-M, -M);
+    const f32x2 xyj = f2_pack(xj, yj);
+    const f32x2 k = f2_add(f2_fma(f2_sub(f.xy, xyj), f.il_xy, M2), NM2);
+    const f32x2 d = f2_sub(f.xy, f2_fma(k, f.l_xy, xyj));
+    float px, py;
+    f2_unpack(f2_mul(d, d), px, py);
+    f2_unpack(d, dx, dy);
+    const float kz = __fadd_rn(__fmaf_rn(__fsub_rn(f.z, zj), f.il_z, M), -M);
+    dz = __fsub_rn(f.z, __fmaf_rn(kz, f.l_z, zj));
+    r2 = __fadd_rn(__fadd_rn(px, py), __fmul_rn(dz, dz));
+}
 
 template <class R> struct Box;
 template <> struct Box<float> {

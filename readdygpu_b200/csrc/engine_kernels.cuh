@@ -1261,7 +1261,8 @@ struct ListCtl {
 template <class R> struct ListArgs {
     State<R> b0, b1;     // the two state buffers
     ListCtl* ctl;
-    int* nbr;            // nbr[k * stride + i]: k-th partner of sorted particle i; null: sort only
+    int* nbr;            // k-th partner of sorted particle i at nbr[4 ((k/4) stride + i) + k%4]: groups
+                         // of 4 as one int4, column-major over i; null: sort only
     float4* xref;        // position of particle i at the build; w: bits of its list length
     long long stride;
     int cap;             // list capacity per particle
@@ -1342,15 +1343,21 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) list_step_kerne
     acc.zero();
     const float4 xr = __ldg(v.xref + i);
     const int cnt = __float_as_int(xr.w);
-    const int* nb = v.nbr + i;
-    // the partners in chunks of LCHUNK: all their indices, then all their
-    // positions are requested before the first pair is evaluated (5 measured
-    // best among 2..8 at about 6 partners per particle)
-    constexpr int LCHUNK = 5;
+    // the first 8 list entries (capacity >= 8) are requested together with
+    // the particle's own state, before its list length is known; entries
+    // past the length are never used
+    const int4* nb4 = reinterpret_cast<const int4*>(v.nbr) + i;
+    const int4 q0 = __ldg(nb4), q1 = __ldg(nb4 + v.stride);
+    PairFrame pf;
+    if constexpr (sizeof(R) == 4) pf.load(s, xi);
+    // the partners in groups of 4: all their positions are requested before
+    // the first pair is evaluated
+    constexpr int LCHUNK = 4;
     for (int k0 = 0; k0 < cnt; k0 += LCHUNK) {
-        int jj[LCHUNK];
+        const int4 q = k0 == 0 ? q0 : (k0 == 4 ? q1 : __ldg(nb4 + (long long)(k0 >> 2) * v.stride));
+        int jj[LCHUNK] = {q.x, q.y, q.z, q.w};
 #pragma unroll
-        for (int u = 0; u < LCHUNK; ++u) jj[u] = (k0 + u < cnt) ? __ldg(nb + (long long)(k0 + u) * v.stride) : -1;
+        for (int u = 0; u < LCHUNK; ++u) jj[u] = (k0 + u < cnt) ? jj[u] : -1;
         R xj[LCHUNK][3];
         int wj[LCHUNK];
 #pragma unroll
@@ -1361,10 +1368,15 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) list_step_kerne
 #pragma unroll
         for (int u = 0; u < LCHUNK; ++u) {
             if (jj[u] < 0) continue;
-            const R dx = mimg_sel(xi[0], xj[u][0], bx.L[0], bx.half[0], ALLPER ? 1 : p0);
-            const R dy = mimg_sel(xi[1], xj[u][1], bx.L[1], bx.half[1], ALLPER ? 1 : p1);
-            const R dz = mimg_sel(xi[2], xj[u][2], bx.L[2], bx.half[2], ALLPER ? 1 : p2);
-            const R r2 = dist2(dx, dy, dz);
+            R dx, dy, dz, r2;
+            if constexpr (sizeof(R) == 4) {
+                pair_disp_x2(pf, xj[u][0], xj[u][1], xj[u][2], dx, dy, dz, r2);
+            } else {
+                dx = mimg_sel(xi[0], xj[u][0], bx.L[0], bx.half[0], ALLPER ? 1 : p0);
+                dy = mimg_sel(xi[1], xj[u][1], bx.L[1], bx.half[1], ALLPER ? 1 : p1);
+                dz = mimg_sel(xi[2], xj[u][2], bx.L[2], bx.half[2], ALLPER ? 1 : p2);
+                r2 = dist2(dx, dy, dz);
+            }
             const int pidx = ti * MAXT + (wj[u] & 0xff);
             if (r2 < s_rc2[pidx]) {
                 if (HREP) {
@@ -1463,7 +1475,7 @@ __global__ void list_scatter_kernel(Args<R> a, ListArgs<R> v, long long off)
 // appends the pairs of one candidate range closer than their list radius
 template <class R>
 __device__ __forceinline__ void list_range(const State<R>& st, int j0, int j1, int self, const R xi[3], R sx, R sy,
-                                           R sz, const R* __restrict__ rl2, int* __restrict__ nb, long long stride,
+                                           R sz, const R* __restrict__ rl2, int* __restrict__ nb, long long stride4,
                                            int cap, int& cnt)
 {
     for (int j = j0; j < j1; ++j) {
@@ -1474,27 +1486,18 @@ __device__ __forceinline__ void list_range(const State<R>& st, int j0, int j1, i
         const R dy = sub_rn(xi[1], add_rn(xj[1], sy));
         const R dz = sub_rn(xi[2], add_rn(xj[2], sz));
         if (dist2(dx, dy, dz) < rl2[wj & 0xff] && j != self) {
-            if (cnt < cap) nb[(long long)cnt * stride] = j;
+            if (cnt < cap) nb[(long long)(cnt >> 2) * stride4 + (cnt & 3)] = j;
             ++cnt;
         }
     }
 }
 
-// re-sort, part 4: the pair list of every particle of the re-sorted state,
-// from its 27-cell neighbourhood (every periodic axis has >= 3 cells here).
-// A flattened walk (one candidate sequence per thread, as neighbourhood_flat)
-// measured slower here than the per-row loops: the candidate test is short.
-template <class R, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) list_build_kernel(Args<R> a, ListArgs<R> v, long long off)
+// the pair list of sorted particle i from its 27-cell neighbourhood (every
+// periodic axis has >= 3 cells here)
+template <class R>
+__device__ __forceinline__ void list_build_one(const Args<R>& a, const ListArgs<R>& v, const State<R>& st, int i,
+                                              const R* __restrict__ s_rl2, long long off)
 {
-    __shared__ R s_rl2[MAXT * MAXT];
-    if (!list_gate(a, v)) return;
-    for (int k = threadIdx.x; k < MAXT * MAXT; k += BLOCK) s_rl2[k] = v.rl2t[k];
-    __syncthreads();
-    const int sel = list_sel(a, v, off);
-    const State<R> st = sel ? v.b0 : v.b1;     // the scatter's destination
-    const int i = blockIdx.x * BLOCK + threadIdx.x;
-    if (i >= a.ntot) return;
     const SysDev& s = a.sys[a.sys_of[i]];
     R xi[3];
     int wi;
@@ -1512,7 +1515,8 @@ __global__ void __launch_bounds__(BLOCK) list_build_kernel(Args<R> a, ListArgs<R
         f[q] = xi[q] - (R)c[q] * cw[q];
     }
     const R lim = v.rl2max * R(1.0001);
-    int* nb = v.nbr + i;
+    int* nb = v.nbr + 4LL * i;
+    const long long stride4 = 4 * v.stride;
     int cnt = 0;
     for (int dz = -1; dz <= 1; ++dz) {
         const R gz = gap2(dz, f[2], cw[2]);
@@ -1543,16 +1547,16 @@ __global__ void __launch_bounds__(BLOCK) list_build_kernel(Args<R> a, ListArgs<R
             } else {
                 if (xa < 0) {
                     list_range<R>(st, a.start[row + n0 - 1], a.start[row + n0], i, xi, -bx.L[0], sy, sz, rl2, nb,
-                                  v.stride, v.cap, cnt);
+                                  stride4, v.cap, cnt);
                     xa = 0;
                 }
                 if (xb >= n0) {
-                    list_range<R>(st, a.start[row], a.start[row + 1], i, xi, bx.L[0], sy, sz, rl2, nb, v.stride,
+                    list_range<R>(st, a.start[row], a.start[row + 1], i, xi, bx.L[0], sy, sz, rl2, nb, stride4,
                                   v.cap, cnt);
                     xb = n0 - 1;
                 }
             }
-            list_range<R>(st, a.start[row + xa], a.start[row + xb + 1], i, xi, R(0), sy, sz, rl2, nb, v.stride,
+            list_range<R>(st, a.start[row + xa], a.start[row + xb + 1], i, xi, R(0), sy, sz, rl2, nb, stride4,
                           v.cap, cnt);
         }
     }
@@ -1562,6 +1566,25 @@ __global__ void __launch_bounds__(BLOCK) list_build_kernel(Args<R> a, ListArgs<R
         atomicOr(a.err, EF_LISTOVF);
         atomicMin((unsigned long long*)a.err_step, (unsigned long long)(*a.step_ptr + off));
     }
+}
+
+// re-sort, part 4: the pair list of every particle of the re-sorted state.
+// A flattened walk (one candidate sequence per thread, as neighbourhood_flat)
+// measured slower here than the per-row loops: the candidate test is short.
+// Ranking each tile of particles by list length, so that the step kernel's
+// warps walk lists of about the same length, cut the step's instructions by
+// a fifth but not its time (it waits on loads, and the ranking adds one).
+template <class R, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) list_build_kernel(Args<R> a, ListArgs<R> v, long long off)
+{
+    __shared__ R s_rl2[MAXT * MAXT];
+    if (!list_gate(a, v)) return;
+    for (int k = threadIdx.x; k < MAXT * MAXT; k += BLOCK) s_rl2[k] = v.rl2t[k];
+    __syncthreads();
+    const int sel = list_sel(a, v, off);
+    const State<R> st = sel ? v.b0 : v.b1;     // the scatter's destination
+    const int i = blockIdx.x * BLOCK + threadIdx.x;
+    if (i < a.ntot) list_build_one<R>(a, v, st, i, s_rl2, off);
 }
 
 // sets the condition of the graph node that holds the re-sort of this step
