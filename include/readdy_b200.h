@@ -126,12 +126,16 @@ typedef struct {
 
 /* Neighbour search of the step.  CELLS walks the 27-cell neighbourhood of
    every particle in every step.  LIST evaluates a pair list of radius
-   rc_max + skin that is rebuilt (with a re-sort by cell) whenever a particle
-   has moved more than about skin/2 since the last build; the pair set and the
-   FP32 forces are identical to CELLS.  AUTO starts with CELLS and, at the
-   first rdgpu_step of >= 4 x graph_steps steps, times CELLS and LIST at
-   skins of 0.1 .. 0.5 x rc_max on the handle's particles and keeps the
-   fastest.                                                                     */
+   rc + skin per type pair that is rebuilt (with a re-sort by cell) when a
+   pair closer than its cutoff is missing from it, or a particle has moved
+   more than about skin since the last build; after every step the particles
+   that moved more than about skin/2 have their current neighbourhood
+   checked against the list.  The pair set and the FP32 forces are identical
+   to CELLS.  AUTO starts with CELLS and, at the first rdgpu_step of >= 4 x
+   graph_steps steps, times CELLS and LIST at skins of 0.1 .. 0.5 x rc_max on
+   the handle's particles and keeps the fastest.  Every energy, force, digest
+   or RDF evaluation in LIST mode re-sorts and rebuilds the list (one build in
+   list_builds).                                                                */
 #define RDGPU_NB_AUTO  0
 #define RDGPU_NB_CELLS 1
 #define RDGPU_NB_LIST  2
@@ -152,7 +156,8 @@ typedef struct {
     int64_t  count[RDGPU_MAX_TYPES];    /* particles per type                        */
     int64_t  step;                      /* steps done since rdgpu_set_particles      */
     int32_t  neighbour_mode;            /* RDGPU_NB_CELLS or RDGPU_NB_LIST in effect */
-    int32_t  list_builds;               /* pair-list builds so far                   */
+    int32_t  list_builds;               /* pair-list builds so far (before this call's
+                                           energy evaluation, which adds one)          */
     double   skin;                      /* pair-list skin in effect [nm], 0: cells   */
     int32_t  list_capacity;             /* pair-list slots per particle              */
     int32_t  reserved;

@@ -22,6 +22,9 @@ using namespace rdgpu;
 namespace {
 thread_local std::string g_create_error;
 constexpr int kStepBlock = 128;
+// hot particles (moved more than about skin/2 since the build) the list check
+// looks at after a step; with more, the step rebuilds the list instead
+constexpr int kHotMax = 256;
 }  // namespace
 
 std::string& rdgpu_global_error() { return g_create_error; }
@@ -111,6 +114,7 @@ struct rdgpu_engine {
     int nbuild_h = 0;
     int* nbr = nullptr;                  // pair lists, list_cap x list_stride (groups of 4 per particle)
     float4* xref = nullptr;              // positions at the build and list lengths
+    int* hot = nullptr;                  // particles that moved more than about skin/2 since the build
     cudaStream_t stream2 = nullptr;      // captures the re-sort into conditional graph nodes
     bool capturing = false;
     long long list_stride = 0;
@@ -297,7 +301,7 @@ void free_particles(Engine* E)
 {
     for (int b = 0; b < 2; ++b) { dfree(E->bufA[b]); dfree(E->bufB[b]); }
     dfree(E->tcell); dfree(E->tslot);
-    dfree(E->nbr); dfree(E->xref);
+    dfree(E->nbr); dfree(E->xref); dfree(E->hot);
     E->list_stride = 0;
     E->list_cap = 0;
     dfree(E->sys_of); dfree(E->x0_d); dfree(E->vec_d); dfree(E->val_d); dfree(E->ityp_d); dfree(E->u64_d);
@@ -569,13 +573,16 @@ template <class R> ListArgs<R> make_list_args(Engine* E, bool with_list)
     v.ctl = E->ctl;
     v.nbr = with_list ? E->nbr : nullptr;
     v.xref = E->xref;
+    v.hot = E->hot;
     v.stride = E->list_stride;
     v.cap = E->list_cap;
-    // list radius and rebuild threshold.  A pair closer than its cutoff at a
-    // later step was closer than rc_max + 2 th at the build, th being the
-    // largest displacement since; th is kept below skin/2 by a margin for the
-    // FP32 rounding of positions (a few ulp of the largest box edge) and of
-    // the squared distances.
+    // list radius and displacement thresholds.  A pair missing from the list
+    // that is closer than its cutoff at a later step has moved by more than
+    // 2 th together, th being kept below skin/2 by a margin for the FP32
+    // rounding of positions (a few ulp of the largest box edge) and of the
+    // squared distances: one of the two moved more than th (list_check_kernel
+    // looks at those).  Beyond 2 th the check's cell walk may miss partners,
+    // and the step kernel asks for a rebuild outright.
     v.rl2t = (const R*)E->rl2_d;
     const double rl = E->max_rc + E->skin;
     v.rl2max = (R)(rl * rl * (1.0 + 1e-6));
@@ -584,6 +591,8 @@ template <class R> ListArgs<R> make_list_args(Engine* E, bool with_list)
         for (int a = 0; a < 3; ++a) lmax = std::max(lmax, E->sys_h[s].L[a]);
     const double th = 0.5 * E->skin * (1.0 - 2e-3) - 4.0 * lmax * std::ldexp(1.0, -20);
     v.thr2 = (float)(th > 0 ? th * th : 0.0);
+    v.cap2 = (float)(th > 0 ? 4.0 * th * th : 0.0);
+    v.hot_max = kHotMax;
     return v;
 }
 
@@ -611,11 +620,12 @@ int ensure_list(Engine* E, int cap)
     // requests the first 8 entries before it knows the list length
     cap = (std::max(std::max(cap, E->list_cap), 8) + 3) & ~3;
     if (E->lgraph) { cudaGraphExecDestroy(E->lgraph); E->lgraph = nullptr; }
-    dfree(E->nbr); dfree(E->xref);
+    dfree(E->nbr); dfree(E->xref); dfree(E->hot);
     E->list_cap = 0;
     E->list_stride = 0;
     CK(cudaMalloc(&E->nbr, (size_t)cap * stride * sizeof(int)));
     CK(cudaMalloc(&E->xref, stride * sizeof(float4)));
+    CK(cudaMalloc(&E->hot, kHotMax * sizeof(int)));
     E->list_cap = cap;
     E->list_stride = stride;
     return RDGPU_OK;
@@ -650,6 +660,14 @@ template <class R> void launch_chain(Engine* E, const Args<R>& a, const ListArgs
     list_finish_kernel<<<1, 32, 0, st>>>(E->ctl, E->err);
 }
 
+// the list check after a step (list_check_kernel): one block of 32 warps,
+// one hot particle per warp at a time
+template <class R> void launch_check(Engine* E, const Args<R>& a, const ListArgs<R>& v, long long off,
+                                     cudaGraphConditionalHandle h, int set_cond, cudaStream_t st)
+{
+    list_check_kernel<R, 1024><<<1, 1024, 0, st>>>(a, v, off, h, set_cond);
+}
+
 // Inside a stream capture: the re-sort of a step becomes a conditional graph
 // node whose body (the chain above) runs only when the step raised the
 // rebuild flag, so steps without a rebuild launch two kernels, not eight.
@@ -663,7 +681,7 @@ template <class R> int add_conditional_chain(Engine* E, const Args<R>& a, const 
     CK(cudaStreamGetCaptureInfo(E->stream, &st, &id, &g, &deps, &nd));
     cudaGraphConditionalHandle h;
     CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
-    list_cond_kernel<<<1, 32, 0, E->stream>>>(h, E->ctl, E->err);
+    launch_check<R>(E, a, v, off, h, 1, E->stream);
     CK(cudaGetLastError());
     CK(cudaStreamGetCaptureInfo(E->stream, &st, &id, &g, &deps, &nd));
     cudaGraphNodeParams cp = {};
@@ -712,8 +730,9 @@ template <class R> int launch_list_steps(Engine* E, int n, const double* noise_d
             if (rc) return rc;
             ++E->launches;
         } else {
+            launch_check<R>(E, a, v, k + 1, 0, 0, E->stream);
             launch_chain<R>(E, a, v, k + 1, E->stream);
-            E->launches += v.nbr ? 6 : 5;
+            E->launches += v.nbr ? 7 : 6;
         }
     }
     advance_kernel<<<1, 32, 0, E->stream>>>(E->step_d, E->err, n);
@@ -730,6 +749,7 @@ int write_ctl(Engine* E, int need)
     c.nreb = (int)((E->cur ^ (int)(E->step_h & 1)) & 1);
     c.maxcnt = 0;
     c.nbuild = E->nbuild_h;
+    c.nhot = 0;
     CK(cudaMemcpyAsync(E->ctl, &c, sizeof(c), cudaMemcpyHostToDevice, E->stream));
     return reset_counters(E, E->step_h);
 }
@@ -931,7 +951,7 @@ template <class R> int tune(Engine* E)
     };
     int rc = snap(true);
     std::vector<double> skins = {0.0};
-    for (double f : {0.1, 0.2, 0.35, 0.5})
+    for (double f : {0.1, 0.2, 0.275, 0.35, 0.425, 0.5})
         if (list_eligible(E, f * E->max_rc)) skins.push_back(f * E->max_rc);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -950,8 +970,9 @@ template <class R> int tune(Engine* E)
         // a trial that fails (the dynamics itself, e.g. a particle leaving the
         // box) disqualifies the candidate; the real run reports the failure
         if (do_steps_mode<R>(E, E->graph_steps, nullptr) != RDGPU_OK) continue;
+        // three graphs: several rebuild intervals of the larger skins
         cudaEventRecord(e0, E->stream);
-        const int trial = do_steps_mode<R>(E, E->graph_steps, nullptr);
+        const int trial = do_steps_mode<R>(E, 3LL * E->graph_steps, nullptr);
         cudaEventRecord(e1, E->stream);
         cudaEventSynchronize(e1);
         if (trial != RDGPU_OK) continue;
@@ -1068,8 +1089,9 @@ template <class R> int profile_list(Engine* E, long long nsteps, double* kms, do
         CK(cudaEventRecord(e0, E->stream));
         launch_list_step_kernel<R>(E, a, v);
         CK(cudaEventRecord(e1, E->stream));
+        launch_check<R>(E, a, v, 1, 0, 0, E->stream);
         launch_chain<R>(E, a, v, 1, E->stream);
-        E->launches += 6;
+        E->launches += 7;
         CK(cudaEventRecord(e2, E->stream));
         advance_kernel<<<1, 32, 0, E->stream>>>(E->step_d, E->err, 1);
         ++E->launches;

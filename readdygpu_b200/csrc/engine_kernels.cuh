@@ -1256,6 +1256,7 @@ struct ListCtl {
     int nreb;        // parity bit, flipped by every re-sort
     int maxcnt;      // longest list met by an overflowing build
     int nbuild;      // builds so far
+    int nhot;        // hot particles of the last step (reset by the list check)
 };
 
 template <class R> struct ListArgs {
@@ -1268,7 +1269,10 @@ template <class R> struct ListArgs {
     int cap;             // list capacity per particle
     const R* rl2t;       // squared list radius (rc + skin) per type pair; 0: no potential, never listed
     R rl2max;            // the largest of them
-    float thr2;          // squared displacement since the build that triggers a rebuild
+    float thr2;          // squared displacement since the build above which the list check looks at a particle
+    float cap2;          // squared displacement since the build that triggers a rebuild by itself
+    int* hot;            // hot particles (moved more than sqrt(thr2)) of the last step, hot_max at most
+    int hot_max;         // more hot particles than this: rebuild rather than check them
 };
 
 template <class R>
@@ -1420,7 +1424,19 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) list_step_kerne
     const float d0 = mimg((float)xi[0], xr.x, s.Lf[0], s.halff[0], p0);
     const float d1 = mimg((float)xi[1], xr.y, s.Lf[1], s.halff[1], p1);
     const float d2 = mimg((float)xi[2], xr.z, s.Lf[2], s.halff[2], p2);
-    if (d0 * d0 + d1 * d1 + d2 * d2 > v.thr2) *((volatile int*)&v.ctl->need) = 1;
+    const float dd = d0 * d0 + d1 * d1 + d2 * d2;
+    if (dd > v.cap2) *((volatile int*)&v.ctl->need) = 1;
+    const bool hot = dd > v.thr2;
+    const unsigned act = __activemask();
+    const unsigned hm = __ballot_sync(act, hot);
+    if (hm) {
+        const int lane = threadIdx.x & 31;
+        const int lead = __ffs(hm) - 1;
+        int base = 0;
+        if (lane == lead) base = atomicAdd(&v.ctl->nhot, __popc(hm));
+        base = __shfl_sync(act, base, lead) + __popc(hm & ((1u << lane) - 1u));
+        if (hot && base < v.hot_max) v.hot[base] = i;
+    }
     store_state(nxt, i, xi, wi, c, id);
     if (ef) {
         atomicOr(a.err, ef);
@@ -1492,74 +1508,93 @@ __device__ __forceinline__ void list_range(const State<R>& st, int j0, int j1, i
     }
 }
 
-// the pair list of sorted particle i from its 27-cell neighbourhood (every
-// periodic axis has >= 3 cells here)
+// Position x in the list's cell grid (>= 3 cells of edge >= rc_max + skin on
+// every periodic axis): its cell and offset within it.
+template <class R> struct ListCell {
+    int c[3];
+    R cw[3], fr[3];
+    __device__ __forceinline__ void locate(const SysDev& s, const R x[3])
+    {
+        cell_coords(s, x, c);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            if constexpr (sizeof(R) == 4) cw[q] = R(1) / s.invcf[q]; else cw[q] = R(1) / s.invc[q];
+            fr[q] = x[q] - (R)c[q] * cw[q];
+        }
+    }
+};
+
+// The cells of row (dz, dy) around x that can hold a sorted particle closer
+// than sqrt(lim) to x: f(j0, j1, sx, sy, sz) for every range [j0, j1) of
+// sorted particles (two where the row wraps), with the periodic shift of its
+// cells.
+template <class R, class F>
+__device__ __forceinline__ void list_row_ranges(const Args<R>& a, const SysDev& s, const ListCell<R>& g, R lim,
+                                                int dz, int dy, F&& f)
+{
+    const R gz = gap2(dz, g.fr[2], g.cw[2]);
+    if (gz >= lim) return;
+    Box<R> bx;
+    bx.load(s);
+    const int n0 = s.n[0], n1 = s.n[1], n2 = s.n[2];
+    int z = g.c[2] + dz;
+    R sz = R(0);
+    if (z < 0 || z >= n2) {
+        if (!s.per[2]) return;
+        sz = z < 0 ? -bx.L[2] : bx.L[2];
+        z = z < 0 ? z + n2 : z - n2;
+    }
+    const R gyz = gz + gap2(dy, g.fr[1], g.cw[1]);
+    if (gyz >= lim) return;
+    int y = g.c[1] + dy;
+    R sy = R(0);
+    if (y < 0 || y >= n1) {
+        if (!s.per[1]) return;
+        sy = y < 0 ? -bx.L[1] : bx.L[1];
+        y = y < 0 ? y + n1 : y - n1;
+    }
+    const int row = (int)s.cell_base + (z * n1 + y) * n0;
+    const R f0 = g.fr[0], w0 = g.cw[0];
+    int xa = (gyz + f0 * f0 < lim) ? g.c[0] - 1 : g.c[0];
+    int xb = (gyz + (w0 - f0) * (w0 - f0) < lim) ? g.c[0] + 1 : g.c[0];
+    const R L0 = bx.L[0];
+    if (!s.per[0]) {
+        xa = max(xa, 0);
+        xb = min(xb, n0 - 1);
+    } else {
+        if (xa < 0) {
+            f(a.start[row + n0 - 1], a.start[row + n0], -L0, sy, sz);
+            xa = 0;
+        }
+        if (xb >= n0) {
+            f(a.start[row], a.start[row + 1], L0, sy, sz);
+            xb = n0 - 1;
+        }
+    }
+    f(a.start[row + xa], a.start[row + xb + 1], R(0), sy, sz);
+}
+
+// the pair list of sorted particle i from its 27-cell neighbourhood
 template <class R>
 __device__ __forceinline__ void list_build_one(const Args<R>& a, const ListArgs<R>& v, const State<R>& st, int i,
-                                              const R* __restrict__ s_rl2, long long off)
+                                               const R* __restrict__ s_rl2, long long off)
 {
     const SysDev& s = a.sys[a.sys_of[i]];
     R xi[3];
     int wi;
     load_pos(st, i, xi, wi);
     const R* rl2 = s_rl2 + (wi & 0xff) * MAXT;
-    int c[3];
-    cell_coords(s, xi, c);
-    Box<R> bx;
-    bx.load(s);
-    const int n0 = s.n[0], n1 = s.n[1], n2 = s.n[2];
-    R cw[3], f[3];
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-        if constexpr (sizeof(R) == 4) cw[q] = R(1) / s.invcf[q]; else cw[q] = R(1) / s.invc[q];
-        f[q] = xi[q] - (R)c[q] * cw[q];
-    }
-    const R lim = v.rl2max * R(1.0001);
     int* nb = v.nbr + 4LL * i;
     const long long stride4 = 4 * v.stride;
     int cnt = 0;
-    for (int dz = -1; dz <= 1; ++dz) {
-        const R gz = gap2(dz, f[2], cw[2]);
-        if (gz >= lim) continue;
-        int z = c[2] + dz;
-        R sz = R(0);
-        if (z < 0 || z >= n2) {
-            if (!s.per[2]) continue;
-            sz = z < 0 ? -bx.L[2] : bx.L[2];
-            z = z < 0 ? z + n2 : z - n2;
-        }
-        for (int dy = -1; dy <= 1; ++dy) {
-            const R gyz = gz + gap2(dy, f[1], cw[1]);
-            if (gyz >= lim) continue;
-            int y = c[1] + dy;
-            R sy = R(0);
-            if (y < 0 || y >= n1) {
-                if (!s.per[1]) continue;
-                sy = y < 0 ? -bx.L[1] : bx.L[1];
-                y = y < 0 ? y + n1 : y - n1;
-            }
-            const int row = (int)s.cell_base + (z * n1 + y) * n0;
-            int xa = (gyz + f[0] * f[0] < lim) ? c[0] - 1 : c[0];
-            int xb = (gyz + (cw[0] - f[0]) * (cw[0] - f[0]) < lim) ? c[0] + 1 : c[0];
-            if (!s.per[0]) {
-                xa = max(xa, 0);
-                xb = min(xb, n0 - 1);
-            } else {
-                if (xa < 0) {
-                    list_range<R>(st, a.start[row + n0 - 1], a.start[row + n0], i, xi, -bx.L[0], sy, sz, rl2, nb,
-                                  stride4, v.cap, cnt);
-                    xa = 0;
-                }
-                if (xb >= n0) {
-                    list_range<R>(st, a.start[row], a.start[row + 1], i, xi, bx.L[0], sy, sz, rl2, nb, stride4,
-                                  v.cap, cnt);
-                    xb = n0 - 1;
-                }
-            }
-            list_range<R>(st, a.start[row + xa], a.start[row + xb + 1], i, xi, R(0), sy, sz, rl2, nb, stride4,
-                          v.cap, cnt);
-        }
-    }
+    ListCell<R> g;
+    g.locate(s, xi);
+    const R lim = v.rl2max * R(1.0001);
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            list_row_ranges<R>(a, s, g, lim, dz, dy, [&](int j0, int j1, R sx, R sy, R sz) {
+                list_range<R>(st, j0, j1, i, xi, sx, sy, sz, rl2, nb, stride4, v.cap, cnt);
+            });
     v.xref[i] = make_float4((float)xi[0], (float)xi[1], (float)xi[2], __int_as_float(min(cnt, v.cap)));
     if (cnt > v.cap) {
         atomicMax(&v.ctl->maxcnt, cnt);
@@ -1587,11 +1622,93 @@ __global__ void __launch_bounds__(BLOCK) list_build_kernel(Args<R> a, ListArgs<R
     if (i < a.ntot) list_build_one<R>(a, v, st, i, s_rl2, off);
 }
 
-// sets the condition of the graph node that holds the re-sort of this step
-__global__ void list_cond_kernel(cudaGraphConditionalHandle h, const ListCtl* ctl, const int* err)
+// j is in the pair list of i
+template <class R>
+__device__ __forceinline__ bool listed(const ListArgs<R>& v, int i, int j)
 {
-    if (threadIdx.x == 0 && blockIdx.x == 0)
-        cudaGraphSetConditional(h, (*((volatile const int*)err) == 0 && *((volatile const int*)&ctl->need)) ? 1u : 0u);
+    const int cnt = __float_as_int(__ldg(&v.xref[i].w));
+    const int4* nb4 = reinterpret_cast<const int4*>(v.nbr) + i;
+    for (int k0 = 0; k0 < cnt; k0 += 4) {
+        const int4 q = __ldg(nb4 + (long long)(k0 >> 2) * v.stride);
+        if (q.x == j || (k0 + 1 < cnt && q.y == j) || (k0 + 2 < cnt && q.z == j) || (k0 + 3 < cnt && q.w == j))
+            return true;
+    }
+    return false;
+}
+
+// every particle now closer to hot particle h than their cutoff is in h's
+// list, and h in its; one warp per hot particle, lane r < 9 walks cell row r
+// of the 27-cell neighbourhood
+template <class R>
+__device__ __forceinline__ bool hot_pairs_listed(const Args<R>& a, const ListArgs<R>& v, const State<R>& st, int h,
+                                                 int lane)
+{
+    const SysDev& s = a.sys[a.sys_of[h]];
+    R xh[3];
+    int wh;
+    load_pos(st, h, xh, wh);
+    bool ok = true;
+    if (lane < 9) {
+        const R* rc2 = a.tab->rc2 + (wh & 0xff) * MAXT;
+        Box<R> bx;
+        bx.load(s);
+        ListCell<R> g;
+        g.locate(s, xh);
+        list_row_ranges<R>(a, s, g, v.rl2max * R(1.0001), lane / 3 - 1, lane % 3 - 1, [&](int j0, int j1, R, R, R) {
+            for (int j = j0; j < j1 && ok; ++j) {
+                if (j == h) continue;
+                R xj[3];
+                int wj;
+                load_pos(st, j, xj, wj);
+                const R dx = mimg_sel(xh[0], xj[0], bx.L[0], bx.half[0], s.per[0]);
+                const R dy = mimg_sel(xh[1], xj[1], bx.L[1], bx.half[1], s.per[1]);
+                const R dz = mimg_sel(xh[2], xj[2], bx.L[2], bx.half[2], s.per[2]);
+                if (dist2(dx, dy, dz) < rc2[wj & 0xff] * R(1.0001) && !(listed(v, h, j) && listed(v, j, h)))
+                    ok = false;
+            }
+        });
+    }
+    return __all_sync(FULL, ok);
+}
+
+// After every step, before the next one's forces: is the pair list still
+// complete?  A pair missing from it was farther apart than its cutoff + skin
+// at the build, so it can be closer than its cutoff now only if the two
+// particles moved by skin together since: one of them moved more than
+// sqrt(thr2) ~ skin/2 (a hot particle; the step kernel collects them).  For
+// every hot particle h, each particle now within its cutoff of h must be in
+// h's list and h in its.  The cell rows around h's current position reach
+// every such particle while no particle has moved more than sqrt(cap2) ~
+// skin since the build (the step kernel raises the rebuild flag itself
+// beyond that).  A missing pair, or more than hot_max hot particles, raise
+// the flag.  One block; thread 0 then clears the count and sets the
+// condition of the graph node that holds the re-sort (set_cond).
+template <class R, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) list_check_kernel(Args<R> a, ListArgs<R> v, long long off,
+                                                           cudaGraphConditionalHandle hc, int set_cond)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (*((volatile const int*)a.err) == 0 && *((volatile const int*)&v.ctl->need) == 0) {
+        const int n = *((volatile const int*)&v.ctl->nhot);
+        if (n > v.hot_max) {
+            if (threadIdx.x == 0) *((volatile int*)&v.ctl->need) = 1;
+        } else if (n > 0) {
+            const State<R> st = list_sel(a, v, off) ? v.b1 : v.b0;
+            for (int k = warp; k < n; k += BLOCK / 32) {
+                if (!hot_pairs_listed<R>(a, v, st, __ldg(v.hot + k), lane)) {
+                    if (lane == 0) *((volatile int*)&v.ctl->need) = 1;
+                    break;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        v.ctl->nhot = 0;
+        if (set_cond)
+            cudaGraphSetConditional(
+                hc, (*((volatile const int*)a.err) == 0 && *((volatile const int*)&v.ctl->need)) ? 1u : 0u);
+    }
 }
 
 // re-sort, part 5: flip the buffer parity, clear the flag

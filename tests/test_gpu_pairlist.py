@@ -183,3 +183,74 @@ def test_list_falls_back_on_small_boxes():
         e.set_particles(xyz, np.zeros(20, np.int32))
         e.step(5)
         assert e.metrics()["neighbour_mode"] == "cells"
+
+
+def pair_system(skin=1.0):
+    """Two particles of radius 2 (harmonic repulsion below 4 nm) in a periodic
+    40 nm cube; D dt chosen so that a noise value of 1 moves sqrt(2e-3) nm."""
+    sys_ = System([ParticleType("A", 1e6, 2.0)], pair=[PairPotential(A.P2_HARMONIC, [(0, 0)], 10.0, "repulsive")],
+                  kT=2.437, dt=1e-9, lo=(0, 0, 0), hi=(40, 40, 40), periodic=(1, 1, 1))
+    return sys_, np.sqrt(2e-3)
+
+
+def moves(b, *dx):
+    """injected noise that moves particle k by dx[k] nm along x"""
+    return np.array([[d / b, 0.0, 0.0] for d in dx])
+
+
+def run_moves(sys_, xyz, prec, mode, steps):
+    """injected-noise steps; the final positions and the list builds so far
+    (the upload's included; metrics() reports the count before the re-sort
+    that its own energy evaluation does)"""
+    with Engine(sys_, precision=prec, neighbour_mode=mode, skin=1.0) as e:
+        e.set_particles(xyz, np.zeros(len(xyz), np.int32))
+        for mv in steps:
+            e.step_with_noise(mv)
+        x, _ = e.get_particles()
+        m = e.metrics()
+    assert m["neighbour_mode"] == mode
+    return x, m["list_builds"]
+
+
+@pytest.mark.parametrize("prec", ["f32c", "f64"])
+def test_list_check_keeps_list_for_an_isolated_hot_particle(prec):
+    """skin 1 nm: a particle that moved 0.7 nm (more than skin/2, less than
+    skin) with no partner nearby keeps the list; at 1.4 nm the list is rebuilt."""
+    sys_, b = pair_system()
+    xyz = np.array([[10.0, 10.0, 10.0], [30.0, 30.0, 30.0]])
+    x1, n1 = run_moves(sys_, xyz, prec, "list", [moves(b, 0.7, 0.0)])
+    x2, n2 = run_moves(sys_, xyz, prec, "list", [moves(b, 0.7, 0.0)] * 2)
+    assert n1 == 1 and n2 == 2
+    assert abs(x1[0, 0] - 10.7) < 1e-5 and abs(x2[0, 0] - 11.4) < 1e-5 and np.allclose(x2[1], 30.0)
+
+
+@pytest.mark.parametrize("prec", ["f32c", "f64"])
+def test_list_check_catches_an_approaching_pair(prec):
+    """Two particles 5.1 nm apart (outside the 5 nm list radius) approach by
+    0.6 nm per step, each moving less than the skin: after two steps they are
+    3.9 nm apart and unlisted; the check rebuilds the list before the next
+    step's forces, so the trajectory is the cell walk's."""
+    sys_, b = pair_system()
+    xyz = np.array([[10.0, 10.0, 10.0], [15.1, 10.0, 10.0]])
+    steps = [moves(b, 0.3, -0.3)] * 2
+    x2, n2 = run_moves(sys_, xyz, prec, "list", steps)
+    assert abs((x2[1, 0] - x2[0, 0]) - 3.9) < 1e-5
+    assert n2 == 2          # the upload's build and the check's
+    steps += [moves(b, 0.0, 0.0)] * 2
+    xc, _ = run_moves(sys_, xyz, prec, "cells", steps)
+    xl, _ = run_moves(sys_, xyz, prec, "list", steps)
+    # the repulsion acted: the pair moved apart in the force-only steps
+    assert xc[1, 0] - xc[0, 0] > 3.9 + 1e-3
+    same(prec, xc, xl)
+
+
+@pytest.mark.parametrize("prec", ["f32c", "f64"])
+def test_list_long_run_equals_cells(prec):
+    """config 1, 1200 steps at skin 1.0: long intervals between rebuilds, in
+    which the list check looks after the hot particles; the trajectory is the
+    cell walk's."""
+    sys_, xyz, types = cfg1(3000)
+    xc, _, _ = run(sys_, xyz, types, prec, 1200, neighbour_mode="cells")
+    xl, _, ml = run(sys_, xyz, types, prec, 1200, neighbour_mode="list", skin=1.0)
+    assert ml["neighbour_mode"] == "list"
+    same(prec, xc, xl)
