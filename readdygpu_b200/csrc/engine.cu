@@ -1052,6 +1052,7 @@ int setup_systems(Engine* E, std::string& why)
             v.Lf[a] = Lf;
             v.halff[a] = 0.5f * Lf;
             v.ilf[a] = b.periodic[a] ? 1.0f / Lf : 0.0f;
+            v.il[a] = b.periodic[a] ? 1.0 / L : 0.0;
             v.L[a] = L;
             v.half[a] = 0.5 * L;
             v.lo[a] = b.lo[a];

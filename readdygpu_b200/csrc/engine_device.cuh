@@ -42,6 +42,7 @@ struct SysDev {
     float Lf[3], halff[3], invcf[3];
     float ilf[3];     // 1/Lf on periodic axes, 0 on open ones (image by rounding)
     double L[3], half[3], invc[3];
+    double il[3];     // 1/L on periodic axes, 0 on open ones (image by rounding)
     double lo[3];
     unsigned long long seed;
 };
@@ -224,6 +225,19 @@ struct PairFrame {
         l_z = s.Lf[2];
     }
 };
+
+// FP64 minimum-image displacement of a listed pair along one axis: the image
+// k in {-1, 0, 1} is rint((xi - xj)/L), rounded by adding and subtracting
+// 1.5 2^52 to the exact product with il = 1/L (0 on an open axis), then
+// xi - (xj + k L), one rounding per operation as in mimg.  As for the FP32
+// pair_disp_x2 below, k differs from mimg's comparison with L/2 only for
+// pairs about L/2 apart on that axis, which no cutoff reaches.
+__device__ __forceinline__ double mimg_round(double xi, double xj, double L, double il)
+{
+    const double M = 6755399441055744.0;   // 1.5 2^52
+    const double k = __dadd_rn(__fma_rn(__dsub_rn(xi, xj), il, M), -M);
+    return __dsub_rn(xi, __fma_rn(k, L, xj));
+}
 
 // FP32 minimum-image displacement and squared distance of a listed pair, x
 // and y as one packed pair.  The image k in {-1, 0, 1} is rint((xi - xj)/L),

@@ -1353,7 +1353,9 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) list_step_kerne
     const int4* nb4 = reinterpret_cast<const int4*>(v.nbr) + i;
     const int4 q0 = __ldg(nb4), q1 = __ldg(nb4 + v.stride);
     PairFrame pf;
+    double il[3] = {0.0, 0.0, 0.0};
     if constexpr (sizeof(R) == 4) pf.load(s, xi);
+    else { il[0] = s.il[0]; il[1] = s.il[1]; il[2] = s.il[2]; }
     // the partners in groups of 4: all their positions are requested before
     // the first pair is evaluated
     constexpr int LCHUNK = 4;
@@ -1376,9 +1378,9 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) list_step_kerne
             if constexpr (sizeof(R) == 4) {
                 pair_disp_x2(pf, xj[u][0], xj[u][1], xj[u][2], dx, dy, dz, r2);
             } else {
-                dx = mimg_sel(xi[0], xj[u][0], bx.L[0], bx.half[0], ALLPER ? 1 : p0);
-                dy = mimg_sel(xi[1], xj[u][1], bx.L[1], bx.half[1], ALLPER ? 1 : p1);
-                dz = mimg_sel(xi[2], xj[u][2], bx.L[2], bx.half[2], ALLPER ? 1 : p2);
+                dx = mimg_round(xi[0], xj[u][0], bx.L[0], il[0]);
+                dy = mimg_round(xi[1], xj[u][1], bx.L[1], il[1]);
+                dz = mimg_round(xi[2], xj[u][2], bx.L[2], il[2]);
                 r2 = dist2(dx, dy, dz);
             }
             const int pidx = ti * MAXT + (wj[u] & 0xff);
