@@ -23,7 +23,8 @@ namespace {
 thread_local std::string g_create_error;
 constexpr int kStepBlock = 128;
 // hot particles (moved more than about skin/2 since the build) the list check
-// looks at after a step; with more, the step rebuilds the list instead
+// looks at after a step, at most (fewer for small handles); with more, the
+// step rebuilds the list instead
 constexpr int kHotMax = 256;
 }  // namespace
 
@@ -592,7 +593,9 @@ template <class R> ListArgs<R> make_list_args(Engine* E, bool with_list)
     const double th = 0.5 * E->skin * (1.0 - 2e-3) - 4.0 * lmax * std::ldexp(1.0, -20);
     v.thr2 = (float)(th > 0 ? th * th : 0.0);
     v.cap2 = (float)(th > 0 ? 4.0 * th * th : 0.0);
-    v.hot_max = kHotMax;
+    // checking a hot particle's neighbourhood costs about what rebuilding
+    // the lists of a thousand particles does
+    v.hot_max = (int)std::min<long long>(kHotMax, std::max<long long>(8, E->npart_tot / 1000));
     return v;
 }
 
@@ -1083,9 +1086,11 @@ template <class R> int profile_list(Engine* E, long long nsteps, double* kms, do
     CK(cudaEventCreate(&e1));
     CK(cudaEventCreate(&e2));
     Args<R> a = make_args<R>(E);
-    const ListArgs<R> v = make_list_args<R>(E, true);
+    ListArgs<R> v = make_list_args<R>(E, true);
     double tk = 0.0, ts = 0.0;
-    for (long long k = 0; k < nsteps; ++k) {
+    long long counted = 0;
+    const long long target = E->step_h + nsteps;
+    while (E->step_h < target) {
         a.step_off = 0;
         CK(cudaEventRecord(e0, E->stream));
         launch_list_step_kernel<R>(E, a, v);
@@ -1096,23 +1101,48 @@ template <class R> int profile_list(Engine* E, long long nsteps, double* kms, do
         CK(cudaEventRecord(e2, E->stream));
         advance_kernel<<<1, 32, 0, E->stream>>>(E->step_d, E->err, 1);
         ++E->launches;
-        CK(cudaEventSynchronize(e2));
-        float m1 = 0.f, m2 = 0.f;
-        cudaEventElapsedTime(&m1, e0, e1);
-        cudaEventElapsedTime(&m2, e1, e2);
-        tk += m1;
-        ts += m2;
+        CK(cudaMemcpyAsync(E->pinned_err, E->err, sizeof(int), cudaMemcpyDeviceToHost, E->stream));
+        CK(cudaStreamSynchronize(E->stream));
+        if (*E->pinned_err == 0) {
+            float m1 = 0.f, m2 = 0.f;
+            cudaEventElapsedTime(&m1, e0, e1);
+            cudaEventElapsedTime(&m2, e1, e2);
+            tk += m1;
+            ts += m2;
+            ++counted;
+            ++E->step_h;
+            continue;
+        }
+        // a failed step (the step kernel, or the re-sort for the next one): the
+        // input of the failing step tf is intact; a list overflow grows the
+        // lists and re-sorts (the step is not timed), anything else is reported
+        rc = read_back(E);
+        if (rc) break;
+        const int ef = *E->pinned_err;
+        E->step_h = *E->pinned_step;
+        set_cur(E, (int)((E->step_h + E->pinned_ctl->nreb) & 1));
+        if (ef != EF_LISTOVF) {
+            rc = prepare_step_state(E, E->step_h);
+            if (!rc) rc = fail(E, (ef & EF_NONFINITE) ? RDGPU_ERR_NONFINITE : RDGPU_ERR_JUMP,
+                               "a step failed during profiling at step " + std::to_string(E->step_h));
+            break;
+        }
+        rc = ensure_list(E, E->pinned_ctl->maxcnt + E->pinned_ctl->maxcnt / 4 + 8);
+        if (!rc) rc = resort<R>(E, true);
+        if (!rc) rc = write_ctl(E, 0);
+        if (rc) break;
+        a = make_args<R>(E);
+        v = make_list_args<R>(E, true);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaEventDestroy(e2);
+    if (rc) return rc;
     rc = read_back(E);
     if (rc) return rc;
-    if (*E->pinned_err) return fail(E, RDGPU_ERR_JUMP, "a step failed during profiling");
-    E->step_h += nsteps;
     set_cur(E, (int)((E->step_h + E->pinned_ctl->nreb) & 1));
-    if (kms) *kms = tk / nsteps;
-    if (sms) *sms = ts / nsteps;
+    if (kms) *kms = counted > 0 ? tk / counted : 0.0;
+    if (sms) *sms = counted > 0 ? ts / counted : 0.0;
     return RDGPU_OK;
 }
 
