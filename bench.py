@@ -8,8 +8,9 @@ the batch): pair forces, external forces, the Euler-Maruyama update with
 Philox noise and whatever neighbour bookkeeping the step needs.  With the
 neighbour search the autotuner picks (rdgpu_autotune, outside the timed
 region) that is either the cell walk (step kernel + counting sort) or the
-pair list (step kernel + a conditional re-sort and list build when a
-particle has moved more than about skin/2).  The default workload is the
+pair list (step kernel + a check of the particles that moved more than about
+skin/2 + a conditional re-sort and list build when that check finds a pair
+missing from the list).  The default workload is the
 batched ensemble (512 periodic systems, N log-uniform in [500, 20000],
 2.45 M particles), the configuration the FP32-batched-vs-FP64 metric is
 quoted on.
