@@ -25,7 +25,9 @@ constexpr int kStepBlock = 128;
 // hot particles (moved more than about skin/2 since the build) the list check
 // looks at after a step, at most (fewer for small handles); with more, the
 // step rebuilds the list instead
-constexpr int kHotMax = 256;
+constexpr int kHotMax = 2048;
+// blocks of 32 warps of the list check (one warp per hot particle at a time)
+constexpr int kCheckBlocks = 16;
 }  // namespace
 
 std::string& rdgpu_global_error() { return g_create_error; }
@@ -663,12 +665,12 @@ template <class R> void launch_chain(Engine* E, const Args<R>& a, const ListArgs
     list_finish_kernel<<<1, 32, 0, st>>>(E->ctl, E->err);
 }
 
-// the list check after a step (list_check_kernel): one block of 32 warps,
-// one hot particle per warp at a time
+// the list check after a step (list_check_kernel): kCheckBlocks blocks of 32
+// warps, one hot particle per warp at a time
 template <class R> void launch_check(Engine* E, const Args<R>& a, const ListArgs<R>& v, long long off,
                                      cudaGraphConditionalHandle h, int set_cond, cudaStream_t st)
 {
-    list_check_kernel<R, 1024><<<1, 1024, 0, st>>>(a, v, off, h, set_cond);
+    list_check_kernel<R, 1024><<<kCheckBlocks, 1024, 0, st>>>(a, v, off, h, set_cond);
 }
 
 // Inside a stream capture: the re-sort of a step becomes a conditional graph
@@ -753,6 +755,7 @@ int write_ctl(Engine* E, int need)
     c.maxcnt = 0;
     c.nbuild = E->nbuild_h;
     c.nhot = 0;
+    c.done = 0;
     CK(cudaMemcpyAsync(E->ctl, &c, sizeof(c), cudaMemcpyHostToDevice, E->stream));
     return reset_counters(E, E->step_h);
 }

@@ -1257,6 +1257,7 @@ struct ListCtl {
     int maxcnt;      // longest list met by an overflowing build
     int nbuild;      // builds so far
     int nhot;        // hot particles of the last step (reset by the list check)
+    int done;        // blocks of the list check finished (reset by its last block)
 };
 
 template <class R> struct ListArgs {
@@ -1683,8 +1684,9 @@ __device__ __forceinline__ bool hot_pairs_listed(const Args<R>& a, const ListArg
 // every such particle while no particle has moved more than sqrt(cap2) ~
 // skin since the build (the step kernel raises the rebuild flag itself
 // beyond that).  A missing pair, or more than hot_max hot particles, raise
-// the flag.  One block; thread 0 then clears the count and sets the
-// condition of the graph node that holds the re-sort (set_cond).
+// the flag.  One warp per hot particle at a time, over all blocks; the last
+// block to finish clears the counts and sets the condition of the graph node
+// that holds the re-sort (set_cond).
 template <class R, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) list_check_kernel(Args<R> a, ListArgs<R> v, long long off,
                                                            cudaGraphConditionalHandle hc, int set_cond)
@@ -1693,10 +1695,10 @@ __global__ void __launch_bounds__(BLOCK) list_check_kernel(Args<R> a, ListArgs<R
     if (*((volatile const int*)a.err) == 0 && *((volatile const int*)&v.ctl->need) == 0) {
         const int n = *((volatile const int*)&v.ctl->nhot);
         if (n > v.hot_max) {
-            if (threadIdx.x == 0) *((volatile int*)&v.ctl->need) = 1;
+            if (threadIdx.x == 0 && blockIdx.x == 0) *((volatile int*)&v.ctl->need) = 1;
         } else if (n > 0) {
             const State<R> st = list_sel(a, v, off) ? v.b1 : v.b0;
-            for (int k = warp; k < n; k += BLOCK / 32) {
+            for (int k = blockIdx.x * (BLOCK / 32) + warp; k < n; k += gridDim.x * (BLOCK / 32)) {
                 if (!hot_pairs_listed<R>(a, v, st, __ldg(v.hot + k), lane)) {
                     if (lane == 0) *((volatile int*)&v.ctl->need) = 1;
                     break;
@@ -1704,12 +1706,18 @@ __global__ void __launch_bounds__(BLOCK) list_check_kernel(Args<R> a, ListArgs<R
             }
         }
     }
+    // the last block to finish clears the counts and sets the condition
     __syncthreads();
     if (threadIdx.x == 0) {
-        v.ctl->nhot = 0;
-        if (set_cond)
-            cudaGraphSetConditional(
-                hc, (*((volatile const int*)a.err) == 0 && *((volatile const int*)&v.ctl->need)) ? 1u : 0u);
+        __threadfence();
+        if (atomicAdd(&v.ctl->done, 1) == (int)gridDim.x - 1) {
+            __threadfence();
+            v.ctl->done = 0;
+            v.ctl->nhot = 0;
+            if (set_cond)
+                cudaGraphSetConditional(
+                    hc, (*((volatile const int*)a.err) == 0 && *((volatile const int*)&v.ctl->need)) ? 1u : 0u);
+        }
     }
 }
 
