@@ -254,3 +254,30 @@ def test_list_long_run_equals_cells(prec):
     xl, _, ml = run(sys_, xyz, types, prec, 1200, neighbour_mode="list", skin=1.0)
     assert ml["neighbour_mode"] == "list"
     same(prec, xc, xl)
+
+
+@pytest.mark.parametrize("prec", ["f32c", "f64"])
+def test_list_check_overflow_of_hot_particles_rebuilds(prec):
+    """Every particle of 2000 moves 0.6 nm (more than skin/2, less than the
+    skin) in a random direction: far more hot particles than the check takes
+    (N/1000, at least 8), so the step rebuilds the list outright; then forces
+    act on the rebuilt list.  The trajectory is the cell walk's."""
+    sys_, xyz, types = cfg1(2000)
+    b = np.array([np.sqrt(2.0 * t.D * sys_.dt) for t in sys_.types])[types]
+    rng = np.random.default_rng(12)
+    u = rng.standard_normal((2000, 3))
+    u *= 0.6 / np.linalg.norm(u, axis=1, keepdims=True)
+    kick = u / b[:, None]
+    out = {}
+    for mode in ("cells", "list"):
+        with Engine(sys_, precision=prec, neighbour_mode=mode, skin=1.0) as e:
+            e.set_particles(xyz, types)
+            e.step_with_noise(kick)
+            for _ in range(3):
+                e.step_with_noise(np.zeros((2000, 3)))
+            x, _ = e.get_particles()
+            m = e.metrics()
+        out[mode] = (x, m)
+    assert out["list"][1]["neighbour_mode"] == "list"
+    assert out["list"][1]["list_builds"] >= 2
+    same(prec, out["cells"][0], out["list"][0])
