@@ -8,7 +8,8 @@ is about to be rebuilt)
   readdygpu_b200/libreaddy_b200.so   engine: hand-written CUDA for sm_100a + C ABI
   readdygpu_b200/libreaddy_workloads.so  seeded synthetic benchmark inputs
   readdygpu_b200/libCReaDDyGPU.so    the JNI entry point of the reference's
-                                     native core, on top of the C ABI
+                                     native core on top of the C ABI, the input
+                                     reader and the output writers
 Every CUDA source is compiled with -gencode arch=compute_100a,code=sm_100a.
 """
 import os
@@ -45,13 +46,14 @@ def build_engine(force=False):
 
 
 def build_jni(force=False):
-    srcs = [os.path.join(CSRC, f) for f in ("jni_shim.cpp", "xml_input.cpp")]
+    srcs = [os.path.join(CSRC, f) for f in ("jni_shim.cpp", "xml_input.cpp", "output.cpp")]
     if not all(os.path.exists(s) for s in srcs):
         return None
     out = os.path.join(HERE, "libCReaDDyGPU.so")
     deps = srcs + [os.path.join(CSRC, "xml_input.h")] + [
         os.path.join(ROOT, "include", h) for h in ("readdy_b200.h", "readdy_b200_jni.h",
-                                                    "readdy_b200_jni_types.h", "readdy_b200_inputs.h")] + [
+                                                    "readdy_b200_jni_types.h", "readdy_b200_inputs.h",
+                                                    "readdy_b200_output.h")] + [
         os.path.join(HERE, "libreaddy_b200.so")]
     if force or _stale(out, [d for d in deps if os.path.exists(d)]):
         _run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall"] + srcs +

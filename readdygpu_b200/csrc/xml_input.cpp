@@ -339,9 +339,16 @@ int read_all(rdgpu_inputs* I, const char* pp, const char* tp, const char* pg, co
         d.periodic[a] = 1;   // the GPU core is periodic in all axes (CudaSimulation.cu:1857-1858)
     }
     d.max_cutoff = max_cutoff;
-    // ---- tplgy_coordinates.xml (CoordReader.cpp:16-65)
+    // ---- tplgy_coordinates.xml (CoordReader.cpp:16-65); a trajectory written
+    // by rdgpu_traj_write (<traj> of frames) restarts from its last frame
     if (!load(tc, root, I->error)) return RDGPU_ERR_ARG;
-    for (const rdxml::Node* p : root->children("p")) {
+    const rdxml::Node* coords = root.get();
+    if (root->name == "traj") {
+        auto frames = root->children("tplgy_coords");
+        if (frames.empty()) { I->error = "tplgy_coordinates: <traj> without a <tplgy_coords> frame"; return RDGPU_ERR_ARG; }
+        coords = frames.back();
+    }
+    for (const rdxml::Node* p : coords->children("p")) {
         auto c = numbers(p->attrs.count("c") ? p->attrs.at("c") : "");
         if (c.size() != 3 || !p->attrs.count("type")) { I->error = "tplgy_coordinates: bad <p> entry"; return RDGPU_ERR_ARG; }
         I->ids.push_back(p->attrs.count("id") ? atoi(p->attrs.at("id").c_str()) : (int)I->ids.size());
