@@ -17,9 +17,10 @@
 //   scan_tiles      tile sums of the cell counts
 //   scan_apply      cell starts (exclusive prefix), counts cleared
 //   scatter_kernel  staging -> sorted arrays at start[cell] + slot
-// With the pair list (list_step_kernel and the re-sort chain further down) a
-// step is the step kernel and, only when some particle has moved more than
-// about skin/2 since the last build, the re-sort and list build.
+// With the pair list (list_step_kernel, list_check_kernel and the re-sort
+// chain further down) a step is the step kernel, the check of the particles
+// that moved more than about skin/2 since the last build and, only when the
+// check or the step asks for it, the re-sort and list build.
 // This replaces the reference's orderOne / warpOrderTwo / update launches and
 // its linked-list relinking under spin locks
 // (lib/ReaDDyGPU_Cpp/CudaKernels/CudaSimulation.cu:1034-1236, 1402-1782,
@@ -1233,16 +1234,18 @@ __global__ void __launch_bounds__(TSUM_BLOCK) typed_final_kernel(const double* _
 //
 // The cell walk of step_kernel finds the candidates of every particle again in
 // every step.  In pair-list mode a list of the pairs closer than
-// rl = rc_max + skin is built from the sorted cell layout, and each step
-// evaluates only the listed pairs.  The list stays complete -- every pair
-// closer than its cutoff at a later step is in it -- while no particle has
-// moved more than skin/2 since the build.  The step kernel checks that bound
-// for every particle and raises a flag; the kernels that follow it in the
-// same step (gated on the flag, no-ops otherwise) re-sort the particles by
-// cell and rebuild the list before the next step.  Pair displacements are the
-// minimum image with the same IEEE operations as the cell walk, so the
-// accepted pairs and the FP32 fixed-point forces are identical to the cell
-// walk's.
+// rl = rc + skin (per type pair) is built from the sorted cell layout, and
+// each step evaluates only the listed pairs.  A pair missing from the list
+// can come within its cutoff only after its two particles moved by skin
+// together, so one of them moved more than about skin/2 (hot): the step
+// kernel collects the hot particles, list_check_kernel checks their current
+// neighbourhoods against the lists, and a missing pair -- or a particle that
+// moved about a full skin, or too many hot particles -- raises a flag; the
+// kernels that follow in the same step (gated on the flag, no-ops otherwise)
+// re-sort the particles by cell and rebuild the list before the next step.
+// Pair displacements are the minimum image with the same IEEE operations as
+// the cell walk, so the accepted pairs and the FP32 fixed-point forces are
+// identical to the cell walk's.
 //
 // Between builds a particle keeps its sorted index; each step writes the
 // other of two state buffers at the same index, and so does the re-sort.  The
