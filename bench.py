@@ -176,6 +176,17 @@ def cpu_baseline(w, budget_s=12.0, threads=None):
                       f"C oracle, {threads} OpenMP threads, {dt:.1f} s"}
 
 
+def host_cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def plain_f64(w, local, steps=200, sample=32):
     """The plain FP64 single-system GPU path (the drop-in): each sampled system
     of the batch alone in its own FP64 handle with default options (autotuned
@@ -223,6 +234,7 @@ def run_reference(args):
         return
     w = workload(args.config, 0)
     cb = cpu_baseline(w, budget_s=20.0)
+    cb["cpu_model"] = host_cpu_model()
     line = {"impl": "reference", "metric": "particle-steps/s", "value": cb["value"], "unit": "particle-steps/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -313,6 +325,9 @@ def run_ours(args):
     cb = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(w)
+        # the same oracle on one host thread, and the host CPU model
+        cb["single_thread"] = cpu_baseline(w, budget_s=4.0, threads=1)["value"]
+        cb["cpu_model"] = host_cpu_model()
     plain = None
     if rank == 0 and not args.no_plain:
         plain = plain_f64(w, local)
