@@ -636,6 +636,15 @@ int ensure_list(Engine* E, int cap)
     return RDGPU_OK;
 }
 
+// capacity after an overflowing build: twice the longest list met, so that a
+// system that keeps clustering (attractive interactions) overflows a few
+// times at most; each overflow costs a re-sort and a new step graph
+int list_regrow_cap(Engine* E)
+{
+    const long long c = 2LL * E->pinned_ctl->maxcnt + 8;
+    return (int)std::min<long long>(c, 1 << 20);
+}
+
 // list capacity from the densest system, x2 for fluctuations and clusters
 int list_cap_estimate(Engine* E)
 {
@@ -793,7 +802,7 @@ template <class R> int resort(Engine* E, bool with_list)
         }
         if (ef != EF_LISTOVF) return fail(E, RDGPU_ERR_CUDA, "re-sort failed");
         // the scan cleared the counts; the current state is untouched
-        rc = ensure_list(E, E->pinned_ctl->maxcnt + E->pinned_ctl->maxcnt / 4 + 8);
+        rc = ensure_list(E, list_regrow_cap(E));
         if (rc) return rc;
     }
     return fail(E, RDGPU_ERR_CUDA, "pair-list build did not converge");
@@ -911,7 +920,7 @@ template <class R> int do_steps_list(Engine* E, long long nsteps, const double* 
         E->step_h = tf;
         set_cur(E, (int)((tf + nreb) & 1));
         if (ef == EF_LISTOVF) {
-            rc = ensure_list(E, E->pinned_ctl->maxcnt + E->pinned_ctl->maxcnt / 4 + 8);
+            rc = ensure_list(E, list_regrow_cap(E));
             if (rc) return rc;
             rc = resort<R>(E, true);
             if (rc) return rc;
@@ -1130,7 +1139,7 @@ template <class R> int profile_list(Engine* E, long long nsteps, double* kms, do
                                "a step failed during profiling at step " + std::to_string(E->step_h));
             break;
         }
-        rc = ensure_list(E, E->pinned_ctl->maxcnt + E->pinned_ctl->maxcnt / 4 + 8);
+        rc = ensure_list(E, list_regrow_cap(E));
         if (!rc) rc = resort<R>(E, true);
         if (!rc) rc = write_ctl(E, 0);
         if (rc) break;
