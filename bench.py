@@ -176,6 +176,20 @@ def cpu_baseline(w, budget_s=12.0, threads=None):
                       f"C oracle, {threads} OpenMP threads, {dt:.1f} s"}
 
 
+def rdf_frames(eng, nbins=200, rmax=20.0, frames=5, every=100):
+    """The RDF of config 3 (200 bins over 0-20 nm, one frame every 100 steps)
+    through the C ABI: re-sort on fresh cells, histogram kernel, counts to the
+    host; wall time of whole synchronous calls after one untimed frame."""
+    eng.rdf(nbins, rmax)
+    t0 = time.perf_counter()
+    for _ in range(frames):
+        eng.rdf(nbins, rmax)
+    ms = (time.perf_counter() - t0) * 1e3 / frames
+    return {"bins": nbins, "rmax_nm": rmax, "every_steps": every, "ms_per_frame": ms,
+            "ms_per_step_amortized": ms / every,
+            "note": "rdgpu_rdf: re-sort and list build, rdf_kernel, uint64 counts to the host"}
+
+
 def host_cpu_model():
     try:
         with open("/proc/cpuinfo") as f:
@@ -328,6 +342,9 @@ def run_ours(args):
         # the same oracle on one host thread, and the host CPU model
         cb["single_thread"] = cpu_baseline(w, budget_s=4.0, threads=1)["value"]
         cb["cpu_model"] = host_cpu_model()
+    rdf = None
+    if rank == 0 and args.config == 3:
+        rdf = rdf_frames(eng)
     plain = None
     if rank == 0 and not args.no_plain:
         plain = plain_f64(w, local)
@@ -351,6 +368,8 @@ def run_ours(args):
                              "alg_bytes_per_particle_step": ALG_BYTES[args.precision]},
                 "e2e": e2e, "cpu_baseline": cb, "gpu_launches": launches, "clocks": clk.summary(),
                 "plain_f64": plain, "vs_plain_f64": (value / ws / plain["value"]) if plain else None}
+        if rdf:
+            line["rdf"] = rdf
         print(json.dumps(line), flush=True)
     eng.close()
     replicas.finalize()

@@ -1638,9 +1638,13 @@ template <class R> int rdf_impl(Engine* E, int nbins, double rmax, int accumulat
         E->rdf_frames = 0;
     }
     CK(cudaMemsetAsync(E->rdf_tmp, 0, H * sizeof(unsigned long long), E->stream));
-    const int use_smem = (H * 4 <= 48 * 1024) ? 1 : 0;
+    // the block's histogram and the bin edges in shared memory when they fit
+    const size_t smem = (size_t)((H + 1) & ~1) * 4 + (size_t)(nbins + 1) * 8;
+    const int use_smem = smem <= 48 * 1024 ? 1 : 0;
     if (E->npart_tot > 0) {
-        rdf_kernel<R><<<grid_for(E->npart_tot, 128), 128, use_smem ? H * 4 : 0, E->stream>>>(
+        // one particle per thread: the per-particle work varies little
+        const int grid = (int)((E->npart_tot + 127) / 128);
+        rdf_kernel<R><<<grid, 128, use_smem ? smem : 0, E->stream>>>(
             E->sys_d, E->sys_of, E->npart_tot, cur_state<R>(E), E->start, S, nbins, E->rdf_e2,
             rmax / (double)nbins, use_smem, E->rdf_tmp);
         CK(cudaGetLastError());

@@ -1044,21 +1044,43 @@ __global__ void noise_kernel(const SysDev* sys, const unsigned short* sys_of, lo
 
 // ---------------------------------------------------------------------------
 // RDF: counts of ordered pairs by (ti, tj, bin), FP64 predicate on the stored
-// positions, stencil of +-R cells (CudaSimulation.cu:1784-1827 semantics).
+// positions (CudaSimulation.cu:1784-1827 semantics).
+//
+// The cells within rmax of particle i are walked as rows of x-adjacent cells
+// (one contiguous range of sorted particles each, split where the row wraps):
+// rows whose (y, z) gap to i is beyond rmax are skipped and each row's x range
+// is cut to the cells that can hold a partner.  An axis whose stencil would
+// wrap onto itself (2R + 1 >= n cells) is walked once, whole, with the
+// minimum image taken per candidate; otherwise the image is the cell wrap of
+// the row, which for pairs within rmax < L/2 is the minimum image.  Either way
+// dx = xi - (xj + k L) with the same IEEE operations as the oracle.
 // ---------------------------------------------------------------------------
+struct RdfAxis {
+    int lo, cnt;        // cells lo .. lo + cnt - 1 (before wrapping)
+    bool whole;         // the whole axis once, image per candidate
+};
+
+// 8 blocks of 128 per SM (64 registers, a few spilled) measured fastest
 template <class R>
-__global__ void rdf_kernel(const SysDev* __restrict__ sys, const unsigned short* __restrict__ sys_of, long long ntot,
+__global__ void __launch_bounds__(128, 8) rdf_kernel(const SysDev* __restrict__ sys, const unsigned short* __restrict__ sys_of, long long ntot,
                            State<R> cur, const int* __restrict__ start, int S, int nbins,
                            const double* __restrict__ e2, double w, int use_smem, unsigned long long* hist)
 {
+    // shared memory (use_smem): the block's histogram, then the squared bin
+    // edges; otherwise neither
     extern __shared__ unsigned int sh[];
     const int H = S * S * nbins;
+    const double* e2s = e2;
     if (use_smem) {
+        double* se2 = reinterpret_cast<double*>(sh + ((H + 1) & ~1));
         for (int i = threadIdx.x; i < H; i += blockDim.x) sh[i] = 0;
+        for (int i = threadIdx.x; i <= nbins; i += blockDim.x) se2[i] = e2[i];
+        e2s = se2;
         __syncthreads();
     }
     const double rmax2 = e2[nbins];
     const double rmax = w * nbins;
+    const float inv_wf = (float)(1.0 / w);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ntot;
          i += (long long)gridDim.x * blockDim.x) {
         const SysDev& s = sys[sys_of[i]];
@@ -1066,50 +1088,90 @@ __global__ void rdf_kernel(const SysDev* __restrict__ sys, const unsigned short*
         int wi;
         load_pos(cur, i, xr, wi);
         const int ti = wi & 0xff;
-        const double xi0 = (double)xr[0], xi1 = (double)xr[1], xi2 = (double)xr[2];
-        double L[3], half[3];
-        int cc[3], lo3[3], cntax[3];
+        const double xi[3] = {(double)xr[0], (double)xr[1], (double)xr[2]};
+        double L[3], half[3], cw[3], f[3];
+        int cc[3];
+        RdfAxis ax[3];
         cell_coords(s, xr, cc);
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             if constexpr (sizeof(R) == 4) L[a] = (double)s.Lf[a]; else L[a] = s.L[a];
             half[a] = 0.5 * L[a];
-            int r = (int)ceil(rmax * s.invc[a]);
+            cw[a] = L[a] / s.n[a];
+            f[a] = xi[a] - cc[a] * cw[a];
+            int r = (int)ceil(rmax / cw[a]);
             if (r < 1) r = 1;
-            if (s.per[a]) {
-                // the whole axis once if the stencil wraps onto itself
-                if (2 * r + 1 >= s.n[a]) { lo3[a] = 0; cntax[a] = s.n[a]; }
-                else { lo3[a] = cc[a] - r; cntax[a] = 2 * r + 1; }
+            if (s.per[a] && 2 * r + 1 >= s.n[a]) {
+                ax[a].lo = 0; ax[a].cnt = s.n[a]; ax[a].whole = true;
+            } else if (s.per[a]) {
+                ax[a].lo = cc[a] - r; ax[a].cnt = 2 * r + 1; ax[a].whole = false;
             } else {
                 const int l = max(0, cc[a] - r), h = min(s.n[a] - 1, cc[a] + r);
-                lo3[a] = l;
-                cntax[a] = h - l + 1;
+                ax[a].lo = l; ax[a].cnt = h - l + 1; ax[a].whole = false;
             }
         }
-        for (int iz = 0; iz < cntax[2]; ++iz) {
-            int z = lo3[2] + iz;
-            if (s.per[2]) z = (z % s.n[2] + s.n[2]) % s.n[2];
-            for (int iy = 0; iy < cntax[1]; ++iy) {
-                int y = lo3[1] + iy;
-                if (s.per[1]) y = (y % s.n[1] + s.n[1]) % s.n[1];
-                for (int ix = 0; ix < cntax[0]; ++ix) {
-                    int x = lo3[0] + ix;
-                    if (s.per[0]) x = (x % s.n[0] + s.n[0]) % s.n[0];
-                    const long long nc = s.cell_base + ((long long)z * s.n[1] + y) * s.n[0] + x;
-                    for (int j = start[nc]; j < start[nc + 1]; ++j) {
+        // squared distance from i to the cell slab at offset d along an axis
+        // (0 inside its own cell and for whole axes), shrunk by a margin that
+        // covers the rounding of the cell geometry
+        const double eps = 1e-9 * (rmax + cw[0] + cw[1] + cw[2]);
+        auto gap2a = [&](int a, int q) -> double {
+            if (ax[a].whole || q == cc[a]) return 0.0;
+            const double g = q > cc[a] ? (q - cc[a] - 1) * cw[a] + (cw[a] - f[a]) : (cc[a] - q - 1) * cw[a] + f[a];
+            const double gg = g - eps;
+            return gg > 0.0 ? gg * gg : 0.0;
+        };
+        for (int iz = 0; iz < ax[2].cnt; ++iz) {
+            const int zq = ax[2].lo + iz;
+            const double gz = gap2a(2, zq);
+            if (gz >= rmax2) continue;
+            int z = zq;
+            double sz = 0.0;
+            if (z < 0) { z += s.n[2]; sz = -L[2]; }
+            else if (z >= s.n[2]) { z -= s.n[2]; sz = L[2]; }
+            for (int iy = 0; iy < ax[1].cnt; ++iy) {
+                const int yq = ax[1].lo + iy;
+                const double gyz = gz + gap2a(1, yq);
+                if (gyz >= rmax2) continue;
+                int y = yq;
+                double sy = 0.0;
+                if (y < 0) { y += s.n[1]; sy = -L[1]; }
+                else if (y >= s.n[1]) { y -= s.n[1]; sy = L[1]; }
+                const long long row = s.cell_base + ((long long)z * s.n[1] + y) * s.n[0];
+                // x cells of this row that can hold a partner
+                int xa = ax[0].lo, xb = ax[0].lo + ax[0].cnt - 1;
+                if (!ax[0].whole) {
+                    while (xa < cc[0] && gyz + gap2a(0, xa) >= rmax2) ++xa;
+                    while (xb > cc[0] && gyz + gap2a(0, xb) >= rmax2) --xb;
+                }
+                // up to three contiguous ranges: wrapped left, inside, wrapped right
+                for (int part = 0; part < 3; ++part) {
+                    int c0, c1;
+                    double sx = 0.0;
+                    if (part == 0) { c0 = xa; c1 = min(xb, -1); sx = -L[0]; }
+                    else if (part == 1) { c0 = max(xa, 0); c1 = min(xb, s.n[0] - 1); }
+                    else { c0 = max(xa, s.n[0]); c1 = xb; sx = L[0]; }
+                    if (c0 > c1) continue;
+                    const int off = part == 0 ? s.n[0] : (part == 2 ? -s.n[0] : 0);
+                    const int j0 = start[row + c0 + off], j1 = start[row + c1 + off + 1];
+                    for (int j = j0; j < j1; ++j) {
                         if (j == i) continue;
                         R xq[3];
                         int wj;
                         load_pos(cur, j, xq, wj);
-                        const double dx = mimg(xi0, (double)xq[0], L[0], half[0], s.per[0]);
-                        const double dy = mimg(xi1, (double)xq[1], L[1], half[1], s.per[1]);
-                        const double dz = mimg(xi2, (double)xq[2], L[2], half[2], s.per[2]);
+                        const double dx = ax[0].whole ? mimg(xi[0], (double)xq[0], L[0], half[0], 1)
+                                                      : sub_rn(xi[0], add_rn((double)xq[0], sx));
+                        const double dy = ax[1].whole ? mimg(xi[1], (double)xq[1], L[1], half[1], 1)
+                                                      : sub_rn(xi[1], add_rn((double)xq[1], sy));
+                        const double dz = ax[2].whole ? mimg(xi[2], (double)xq[2], L[2], half[2], 1)
+                                                      : sub_rn(xi[2], add_rn((double)xq[2], sz));
                         const double r2 = dist2(dx, dy, dz);
                         if (!(r2 < rmax2)) continue;
-                        int k = (int)(sqrt(r2) / w);
+                        // the bin: an FP32 estimate, then the exact FP64 edges decide
+                        const float r2f = (float)r2;
+                        int k = r2f > 0.0f ? (int)(r2f * rsqrtf(r2f) * inv_wf) : 0;
                         k = min(max(k, 0), nbins - 1);
-                        while (k > 0 && e2[k] > r2) --k;
-                        while (k < nbins - 1 && e2[k + 1] <= r2) ++k;
+                        while (k > 0 && e2s[k] > r2) --k;
+                        while (k < nbins - 1 && e2s[k + 1] <= r2) ++k;
                         const int hidx = (ti * S + (wj & 0xff)) * nbins + k;
                         if (use_smem) atomicAdd(sh + hidx, 1u);
                         else atomicAdd(hist + hidx, 1ull);
