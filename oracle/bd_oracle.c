@@ -654,6 +654,20 @@ void orc_rdf_edges2(int32_t nbins, double rmax, double* edges2)
     }
 }
 
+/* RDF displacement, symmetric in i and j: (xi - xj) -/+ L when |xi - xj| >
+   L/2.  Swapping i and j negates every rounded intermediate, so both
+   orientations of a pair land in the same bin (the engine evaluates each pair
+   once and counts it for both, as CudaSimulation.cu:1815-1818 does).        */
+static inline double mimg_sym(double xi, double xj, double L, double half, int per)
+{
+    double d = xi - xj;
+    if (per) {
+        if (d > half) d = d - L;
+        else if (d < -half) d = d + L;
+    }
+    return d;
+}
+
 static int rdf_bin(const double* e2, int nbins, double w, double r2)
 {
     int k = (int)(sqrt(r2) / w);
@@ -691,9 +705,9 @@ static void rdf_core(const rdgpu_system_desc* d, int64_t n, const double* x,
                 const int64_t j = NB_J(&c, q);
                 if (j == i) continue;
                 const int tj = types[j];
-                double dx = mimg(x[3 * i + 0], x[3 * j + 0], t.L[0], t.half[0], t.per[0]);
-                double dy = mimg(x[3 * i + 1], x[3 * j + 1], t.L[1], t.half[1], t.per[1]);
-                double dz = mimg(x[3 * i + 2], x[3 * j + 2], t.L[2], t.half[2], t.per[2]);
+                double dx = mimg_sym(x[3 * i + 0], x[3 * j + 0], t.L[0], t.half[0], t.per[0]);
+                double dy = mimg_sym(x[3 * i + 1], x[3 * j + 1], t.L[1], t.half[1], t.per[1]);
+                double dz = mimg_sym(x[3 * i + 2], x[3 * j + 2], t.L[2], t.half[2], t.per[2]);
                 double r2 = (dx * dx + dy * dy) + dz * dz;
                 if (r2 < e2[nbins]) {
                     int b = rdf_bin(e2, nbins, w, r2);

@@ -297,6 +297,21 @@ __device__ __forceinline__ R mimg(R xi, R xj, R L, R half, int per)
     return d;
 }
 
+// Minimum-image displacement for the RDF, symmetric in i and j: d = xi - xj,
+// then d -/+ L when |d| > L/2, each step rounded once.  Swapping i and j
+// negates every intermediate exactly, so both orientations of a pair get the
+// same r^2 and the same bin, and a pair can be evaluated once for both.
+template <class R>
+__device__ __forceinline__ R mimg_sym(R xi, R xj, R L, R half, int per)
+{
+    const R d = sub_rn(xi, xj);
+    if (per) {
+        if (d > half) return sub_rn(d, L);
+        if (d < -half) return add_rn(d, L);
+    }
+    return d;
+}
+
 // The same displacement as mimg, with the image chosen first and one
 // subtraction path: xj + (-L) == xj - L exactly, and xj + 0 == xj up to the
 // sign of a zero (which no force or distance sees).

@@ -1044,16 +1044,20 @@ __global__ void noise_kernel(const SysDev* sys, const unsigned short* sys_of, lo
 
 // ---------------------------------------------------------------------------
 // RDF: counts of ordered pairs by (ti, tj, bin), FP64 predicate on the stored
-// positions (CudaSimulation.cu:1784-1827 semantics).
+// positions.  As in the reference (CudaSimulation.cu:1784-1827), each pair is
+// evaluated once, from its lower sorted index, and counted for both (ti, tj)
+// and (tj, ti); the displacement is symmetric in i and j (mimg_sym), so this
+// equals counting both orientations separately.
 //
 // The cells within rmax of particle i are walked as rows of x-adjacent cells
 // (one contiguous range of sorted particles each, split where the row wraps):
 // rows whose (y, z) gap to i is beyond rmax are skipped and each row's x range
-// is cut to the cells that can hold a partner.  An axis whose stencil would
-// wrap onto itself (2R + 1 >= n cells) is walked once, whole, with the
-// minimum image taken per candidate; otherwise the image is the cell wrap of
-// the row, which for pairs within rmax < L/2 is the minimum image.  Either way
-// dx = xi - (xj + k L) with the same IEEE operations as the oracle.
+// is cut to the cells that can hold a partner; within a range only partners
+// after i are taken.  An axis whose stencil would wrap onto itself (2R + 1 >=
+// n cells) is walked once, whole, with the minimum image taken per candidate;
+// otherwise the image is the cell wrap of the row, which for pairs within
+// rmax < L/2 is the minimum image.  Either way dx = (xi - xj) - k L with the
+// same IEEE operations as the oracle.
 // ---------------------------------------------------------------------------
 struct RdfAxis {
     int lo, cnt;        // cells lo .. lo + cnt - 1 (before wrapping)
@@ -1152,18 +1156,18 @@ __global__ void __launch_bounds__(128, 8) rdf_kernel(const SysDev* __restrict__ 
                     else { c0 = max(xa, s.n[0]); c1 = xb; sx = L[0]; }
                     if (c0 > c1) continue;
                     const int off = part == 0 ? s.n[0] : (part == 2 ? -s.n[0] : 0);
-                    const int j0 = start[row + c0 + off], j1 = start[row + c1 + off + 1];
+                    const int j1 = start[row + c1 + off + 1];
+                    const int j0 = max(start[row + c0 + off], (int)i + 1);
                     for (int j = j0; j < j1; ++j) {
-                        if (j == i) continue;
                         R xq[3];
                         int wj;
                         load_pos(cur, j, xq, wj);
-                        const double dx = ax[0].whole ? mimg(xi[0], (double)xq[0], L[0], half[0], 1)
-                                                      : sub_rn(xi[0], add_rn((double)xq[0], sx));
-                        const double dy = ax[1].whole ? mimg(xi[1], (double)xq[1], L[1], half[1], 1)
-                                                      : sub_rn(xi[1], add_rn((double)xq[1], sy));
-                        const double dz = ax[2].whole ? mimg(xi[2], (double)xq[2], L[2], half[2], 1)
-                                                      : sub_rn(xi[2], add_rn((double)xq[2], sz));
+                        const double dx = ax[0].whole ? mimg_sym(xi[0], (double)xq[0], L[0], half[0], 1)
+                                                      : sub_rn(sub_rn(xi[0], (double)xq[0]), sx);
+                        const double dy = ax[1].whole ? mimg_sym(xi[1], (double)xq[1], L[1], half[1], 1)
+                                                      : sub_rn(sub_rn(xi[1], (double)xq[1]), sy);
+                        const double dz = ax[2].whole ? mimg_sym(xi[2], (double)xq[2], L[2], half[2], 1)
+                                                      : sub_rn(sub_rn(xi[2], (double)xq[2]), sz);
                         const double r2 = dist2(dx, dy, dz);
                         if (!(r2 < rmax2)) continue;
                         // the bin: an FP32 estimate, then the exact FP64 edges decide
@@ -1172,9 +1176,15 @@ __global__ void __launch_bounds__(128, 8) rdf_kernel(const SysDev* __restrict__ 
                         k = min(max(k, 0), nbins - 1);
                         while (k > 0 && e2s[k] > r2) --k;
                         while (k < nbins - 1 && e2s[k + 1] <= r2) ++k;
-                        const int hidx = (ti * S + (wj & 0xff)) * nbins + k;
-                        if (use_smem) atomicAdd(sh + hidx, 1u);
-                        else atomicAdd(hist + hidx, 1ull);
+                        const int tj = wj & 0xff;
+                        const int h1 = (ti * S + tj) * nbins + k, h2 = (tj * S + ti) * nbins + k;
+                        if (use_smem) {
+                            if (h1 == h2) atomicAdd(sh + h1, 2u);
+                            else { atomicAdd(sh + h1, 1u); atomicAdd(sh + h2, 1u); }
+                        } else {
+                            if (h1 == h2) atomicAdd(hist + h1, 2ull);
+                            else { atomicAdd(hist + h1, 1ull); atomicAdd(hist + h2, 1ull); }
+                        }
                     }
                 }
             }

@@ -195,9 +195,9 @@ __global__ void na_rdf(const NaScratch* __restrict__ s, long long n, int S, int 
                         for (int j = s->off[nc]; j < s->off[nc + 1]; ++j) {
                             if (j == i) continue;
                             const NaRec q = s->rec[j];
-                            const double dx = mimg(p.x, q.x, b.L[0], b.half[0], b.per[0]);
-                            const double dy = mimg(p.y, q.y, b.L[1], b.half[1], b.per[1]);
-                            const double dz = mimg(p.z, q.z, b.L[2], b.half[2], b.per[2]);
+                            const double dx = mimg_sym(p.x, q.x, b.L[0], b.half[0], b.per[0]);
+                            const double dy = mimg_sym(p.y, q.y, b.L[1], b.half[1], b.per[1]);
+                            const double dz = mimg_sym(p.z, q.z, b.L[2], b.half[2], b.per[2]);
                             const double r2 = dist2(dx, dy, dz);
                             if (!(r2 < rmax2)) continue;
                             int k = (int)(sqrt(r2) / w);
