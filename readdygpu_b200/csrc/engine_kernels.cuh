@@ -1103,7 +1103,9 @@ __global__ void __launch_bounds__(128, 8) rdf_kernel(const SysDev* __restrict__ 
             half[a] = 0.5 * L[a];
             cw[a] = L[a] / s.n[a];
             f[a] = xi[a] - cc[a] * cw[a];
-            int r = (int)ceil(rmax / cw[a]);
+            // cells per side that can hold a partner; the margin keeps a
+            // quotient that rounds down onto an integer from dropping a layer
+            int r = (int)ceil(rmax / cw[a] * (1.0 + 1e-12));
             if (r < 1) r = 1;
             if (s.per[a] && 2 * r + 1 >= s.n[a]) {
                 ax[a].lo = 0; ax[a].cnt = s.n[a]; ax[a].whole = true;
