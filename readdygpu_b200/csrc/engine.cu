@@ -679,7 +679,10 @@ template <class R> void launch_chain(Engine* E, const Args<R>& a, const ListArgs
 template <class R> void launch_check(Engine* E, const Args<R>& a, const ListArgs<R>& v, long long off,
                                      cudaGraphConditionalHandle h, int set_cond, cudaStream_t st)
 {
-    list_check_kernel<R, 1024><<<kCheckBlocks, 1024, 0, st>>>(a, v, off, h, set_cond);
+    // at most 4 hot particles per warp (32 warps a block): fewer blocks for
+    // small handles, whose cap is lower
+    const int grid = std::max(1, std::min(kCheckBlocks, (v.hot_max + 127) / 128));
+    list_check_kernel<R, 1024><<<grid, 1024, 0, st>>>(a, v, off, h, set_cond);
 }
 
 // Inside a stream capture: the re-sort of a step becomes a conditional graph
