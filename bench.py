@@ -20,7 +20,9 @@ value: particle-steps/s with the state resident in HBM, device-timed with CUDA
        (2.45 M x 64 B = 157 MB read+written) exceeds the 126 MB L2.
 e2e:   the same metric through the C ABI with host buffers: every frame of
        100 steps uploads the particles from pinned host memory
-       (rdgpu_set_particles), steps, and downloads them (rdgpu_get_particles),
+       (rdgpu_set_particles, FP32 coordinates for the FP32C engine as the
+       reference's float frames, FP64 for the FP64 engine), steps, and
+       downloads them (rdgpu_get_particles),
        the per-frame traffic of the reference's JNI frame loop.
 plain_f64: the north star's denominator, the plain FP64 single-system path:
        32 of the workload's systems, each alone in its own FP64 handle.
@@ -316,8 +318,11 @@ def run_ours(args):
     if not args.no_e2e:
         frame = 100
         frames = max(1, min(20, args.steps // frame))
-        # pinned host buffers, as a host application would keep them
-        xh = torch.empty((w.n, 3), dtype=torch.float64, pin_memory=True).numpy()
+        # pinned host buffers, as a host application would keep them; FP32
+        # coordinates for the FP32C engine (the reference moves float frames,
+        # ReaDDyGPU.cpp:264-292), FP64 for the FP64 engine
+        xdt = torch.float32 if args.precision == "f32c" else torch.float64
+        xh = torch.empty((w.n, 3), dtype=xdt, pin_memory=True).numpy()
         th = torch.empty(w.n, dtype=torch.int32, pin_memory=True).numpy()
         eng.get_particles(xh, th)
         barrier()
@@ -329,11 +334,13 @@ def run_ours(args):
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         dt = replicas.max_over_ranks(dt, f"cuda:{local}")
-        h2d = w.n * (3 * 8 + 4) + (len(w.offsets) * 8 if w.offsets is not None else 0)
-        d2h = w.n * (3 * 8 + 4)
+        xb = xh.itemsize
+        h2d = w.n * (3 * xb + 4) + (len(w.offsets) * 8 if w.offsets is not None else 0)
+        d2h = w.n * (3 * xb + 4)
         e2e = {"value": n_all * frame * frames / dt, "unit": "particle-steps/s",
                "h2d_bytes_per_step": h2d / frame, "d2h_bytes_per_step": d2h / frame,
                "frame_steps": frame, "frames": frames,
+               "coords": "float32" if xb == 4 else "float64",
                "note": "per frame: pinned-host upload + re-binning, 100 steps, download"}
 
     cb = None

@@ -200,6 +200,15 @@ int rdgpu_set_particles(rdgpu_handle h, const int64_t* offsets, int64_t n_total,
    order.  Replaces copyPosFromDevice (CudaSimulation.cu:2309 ff).             */
 int rdgpu_get_particles(rdgpu_handle h, double* xyz, int32_t* types);
 
+/* The same with FP32 coordinates, as the reference moves them
+   (copyPosToDevice / copyPosFromDevice take float, CudaSimulation.cu:562-626,
+   and the JNI frame is float[], ReaDDyGPU.cpp:264-292): half the bytes over
+   PCIe.  Upload is exact into either precision (an FP32C handle starts with
+   zero compensation); download rounds each coordinate to FP32.              */
+int rdgpu_set_particles_f32(rdgpu_handle h, const int64_t* offsets, int64_t n_total,
+                            const float* xyz, const int32_t* types);
+int rdgpu_get_particles_f32(rdgpu_handle h, float* xyz, int32_t* types);
+
 int rdgpu_num_particles(rdgpu_handle h, int64_t* n_total);
 
 /* Bonded pairs of particle groups (ReaDDy group potentials): each bond

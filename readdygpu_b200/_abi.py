@@ -88,6 +88,7 @@ class Metrics(C.Structure):
 # C-ABI functions and their signatures: (name, restype, argtypes)
 P = C.c_void_p
 DP = C.POINTER(C.c_double)
+FP = C.POINTER(C.c_float)
 I32P = C.POINTER(C.c_int32)
 I64P = C.POINTER(C.c_int64)
 U64P = C.POINTER(C.c_uint64)
@@ -100,6 +101,8 @@ FUNCTIONS = [
     ("rdgpu_last_error", C.c_char_p, [P]),
     ("rdgpu_set_particles", C.c_int, [P, I64P, C.c_int64, DP, I32P]),
     ("rdgpu_get_particles", C.c_int, [P, DP, I32P]),
+    ("rdgpu_set_particles_f32", C.c_int, [P, I64P, C.c_int64, FP, I32P]),
+    ("rdgpu_get_particles_f32", C.c_int, [P, FP, I32P]),
     ("rdgpu_num_particles", C.c_int, [P, I64P]),
     ("rdgpu_step", C.c_int, [P, C.c_int64]),
     ("rdgpu_step_with_noise", C.c_int, [P, DP]),

@@ -1305,8 +1305,8 @@ template <class R> int set_bonds_impl(Engine* E, long long nb, const int* ij, co
     return rc;
 }
 
-template <class R> int set_particles_impl(Engine* E, const long long* offsets, long long ntot,
-                                          const double* xyz, const int* types)
+template <class R, class In> int set_particles_impl(Engine* E, const long long* offsets, long long ntot,
+                                                    const In* xyz, const int* types)
 {
     // validate the layout before touching the handle's state
     std::vector<long long> off;
@@ -1339,9 +1339,10 @@ template <class R> int set_particles_impl(Engine* E, const long long* offsets, l
     if (ntot > 0) {
         CK(cudaMemcpyAsync(E->off_d, off.data(), (E->nsys + 1) * sizeof(long long), cudaMemcpyHostToDevice, E->stream));
         sys_of_kernel<<<grid_for(ntot), 256, 0, E->stream>>>(E->off_d, E->nsys, ntot, E->sys_of);
-        CK(cudaMemcpyAsync(E->vec_d, xyz, ntot * 3 * sizeof(double), cudaMemcpyHostToDevice, E->stream));
+        // (the FP64 staging buffer holds FP32 coordinates in its first half)
+        CK(cudaMemcpyAsync(E->vec_d, xyz, ntot * 3 * sizeof(In), cudaMemcpyHostToDevice, E->stream));
         CK(cudaMemcpyAsync(E->ityp_d, types, ntot * sizeof(int), cudaMemcpyHostToDevice, E->stream));
-        ingest_kernel<R><<<grid_for(ntot), 256, 0, E->stream>>>(E->sys_d, E->sys_of, ntot, E->vec_d, E->ityp_d,
+        ingest_kernel<R, In><<<grid_for(ntot), 256, 0, E->stream>>>(E->sys_d, E->sys_of, ntot, (const In*)E->vec_d, E->ityp_d,
                                                                 E->desc.n_types, stg_state<R>(E),
                                                                 E->tcell, E->tslot, E->counts, E->x0_d, E->err);
         CK(cudaGetLastError());
@@ -1530,14 +1531,14 @@ template <class R> int apply_edits_impl(Engine* E, const float* ed, long long co
     return RDGPU_OK;
 }
 
-template <class R> int get_particles_impl(Engine* E, double* xyz, int* types)
+template <class R, class Out> int get_particles_impl(Engine* E, Out* xyz, int* types)
 {
     const long long N = E->npart_tot;
     if (N == 0) return RDGPU_OK;
-    emit_kernel<R><<<grid_for(N), 256, 0, E->stream>>>(E->sys_d, E->sys_of, N, cur_state<R>(E), E->vec_d,
-                                                       E->ityp_d);
+    emit_kernel<R, Out><<<grid_for(N), 256, 0, E->stream>>>(E->sys_d, E->sys_of, N, cur_state<R>(E), (Out*)E->vec_d,
+                                                            E->ityp_d);
     CK(cudaGetLastError());
-    if (xyz) CK(cudaMemcpyAsync(xyz, E->vec_d, N * 3 * sizeof(double), cudaMemcpyDeviceToHost, E->stream));
+    if (xyz) CK(cudaMemcpyAsync(xyz, E->vec_d, N * 3 * sizeof(Out), cudaMemcpyDeviceToHost, E->stream));
     if (types) CK(cudaMemcpyAsync(types, E->ityp_d, N * sizeof(int), cudaMemcpyDeviceToHost, E->stream));
     CK(cudaStreamSynchronize(E->stream));
     return RDGPU_OK;
@@ -1884,6 +1885,23 @@ int rdgpu_set_bonds(rdgpu_handle h, int64_t n_bonds, const int32_t* ij, const in
 }
 
 int rdgpu_get_particles(rdgpu_handle h, double* xyz, int32_t* types)
+{
+    Engine* E = (Engine*)h;
+    GUARD(E);
+    NEED_PARTICLES(E);
+    return DISPATCH(E, get_particles_impl, E, xyz, (int*)types);
+}
+
+int rdgpu_set_particles_f32(rdgpu_handle h, const int64_t* offsets, int64_t n_total, const float* xyz,
+                            const int32_t* types)
+{
+    Engine* E = (Engine*)h;
+    GUARD(E);
+    if (n_total < 0 || (n_total > 0 && (!xyz || !types))) return fail(E, RDGPU_ERR_ARG, "invalid particle arrays");
+    return DISPATCH(E, set_particles_impl, E, (const long long*)offsets, (long long)n_total, xyz, (const int*)types);
+}
+
+int rdgpu_get_particles_f32(rdgpu_handle h, float* xyz, int32_t* types)
 {
     Engine* E = (Engine*)h;
     GUARD(E);

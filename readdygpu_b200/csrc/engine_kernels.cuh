@@ -870,19 +870,19 @@ __device__ __forceinline__ void ingest_one(const SysDev& s, long long g, int id,
     tslot[g] = atomicAdd(counts + cell, 1);
 }
 
-// writes the particles (input order) into the staging arrays with their cell
-// and slot, ready for scan + scatter
-template <class R>
+// writes the particles (input order; FP64 or FP32 coordinates) into the
+// staging arrays with their cell and slot, ready for scan + scatter
+template <class R, class In>
 __global__ void ingest_kernel(const SysDev* __restrict__ sys, const unsigned short* __restrict__ sys_of, long long ntot,
-                              const double* __restrict__ xyz, const int* __restrict__ types, int ntypes, State<R> stg,
+                              const In* __restrict__ xyz, const int* __restrict__ types, int ntypes, State<R> stg,
                               int* __restrict__ tcell, int* __restrict__ tslot, int* __restrict__ counts,
                               double* __restrict__ x0, int* err)
 {
     for (long long g = blockIdx.x * (long long)blockDim.x + threadIdx.x; g < ntot;
          g += (long long)gridDim.x * blockDim.x) {
         const SysDev& s = sys[sys_of[g]];
-        ingest_one<R>(s, g, (int)(g - s.part_base), xyz + 3 * g, types[g], ntypes, stg, tcell, tslot, counts, x0,
-                      err);
+        const double xd[3] = {(double)xyz[3 * g], (double)xyz[3 * g + 1], (double)xyz[3 * g + 2]};
+        ingest_one<R>(s, g, (int)(g - s.part_base), xd, types[g], ntypes, stg, tcell, tslot, counts, x0, err);
     }
 }
 
@@ -950,10 +950,11 @@ __global__ void edit_append_kernel(const SysDev* __restrict__ sys, long long bas
                       x0n, err);
 }
 
-// sorted arrays -> absolute coordinates and types by global index
-template <class R>
+// sorted arrays -> absolute coordinates (FP64, or rounded to FP32) and types
+// by global index
+template <class R, class Out>
 __global__ void emit_kernel(const SysDev* __restrict__ sys, const unsigned short* __restrict__ sys_of, long long ntot,
-                            State<R> cur, double* __restrict__ xyz, int* __restrict__ types)
+                            State<R> cur, Out* __restrict__ xyz, int* __restrict__ types)
 {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ntot;
          i += (long long)gridDim.x * blockDim.x) {
@@ -961,16 +962,16 @@ __global__ void emit_kernel(const SysDev* __restrict__ sys, const unsigned short
         if constexpr (sizeof(R) == 4) {
             const float4 p = cur.pos[i], c = cur.aux[i];
             const long long g = s.part_base + __float_as_int(c.w);
-            xyz[3 * g + 0] = __dadd_rn(__dsub_rn((double)p.x, (double)c.x), s.lo[0]);
-            xyz[3 * g + 1] = __dadd_rn(__dsub_rn((double)p.y, (double)c.y), s.lo[1]);
-            xyz[3 * g + 2] = __dadd_rn(__dsub_rn((double)p.z, (double)c.z), s.lo[2]);
+            xyz[3 * g + 0] = (Out)__dadd_rn(__dsub_rn((double)p.x, (double)c.x), s.lo[0]);
+            xyz[3 * g + 1] = (Out)__dadd_rn(__dsub_rn((double)p.y, (double)c.y), s.lo[1]);
+            xyz[3 * g + 2] = (Out)__dadd_rn(__dsub_rn((double)p.z, (double)c.z), s.lo[2]);
             types[g] = __float_as_int(p.w) & 0xff;
         } else {
             const Rec64 r = cur.rec[i];
             const long long g = s.part_base + r.id;
-            xyz[3 * g + 0] = __dadd_rn(r.x, s.lo[0]);
-            xyz[3 * g + 1] = __dadd_rn(r.y, s.lo[1]);
-            xyz[3 * g + 2] = __dadd_rn(r.z, s.lo[2]);
+            xyz[3 * g + 0] = (Out)__dadd_rn(r.x, s.lo[0]);
+            xyz[3 * g + 1] = (Out)__dadd_rn(r.y, s.lo[1]);
+            xyz[3 * g + 2] = (Out)__dadd_rn(r.z, s.lo[2]);
             types[g] = r.w & 0xff;
         }
     }

@@ -70,6 +70,7 @@ extern "C" JNIEXPORT void JNICALL Java_readdy_impl_sim_top_TopGPU_cCreateSimulat
     rdgpu_inputs_desc(in, &desc, &run);
     int64_t n = rdgpu_inputs_count(in);
     std::vector<double> xyz(3 * n);
+    std::vector<float> xyzf;
     std::vector<int32_t> types(n), ids(n);
     rdgpu_inputs_particles(in, xyz.data(), types.data(), ids.data());
     // particle groups -> bonded pairs (the reference's groups kernel,
@@ -134,7 +135,9 @@ extern "C" JNIEXPORT void JNICALL Java_readdy_impl_sim_top_TopGPU_cCreateSimulat
             printf("error: %s\n", rdgpu_last_error(h));
             break;
         }
-        if (rdgpu_get_particles(h, xyz.data(), types.data()) != RDGPU_OK) {
+        // the frame is float[] (ReaDDyGPU.cpp:264-292): download FP32 directly
+        xyzf.resize(3 * n);
+        if (rdgpu_get_particles_f32(h, xyzf.data(), types.data()) != RDGPU_OK) {
             printf("error while copying positions from device: %s\n", rdgpu_last_error(h));
             break;
         }
@@ -147,9 +150,9 @@ extern "C" JNIEXPORT void JNICALL Java_readdy_impl_sim_top_TopGPU_cCreateSimulat
         if (!P) { printf("cant get array pointer\n"); break; }
         P[0] = (jfloat)n;
         for (int64_t j = 0; j < n; ++j) {
-            P[1 + 5 * j + 0] = (jfloat)xyz[3 * j + 0];
-            P[1 + 5 * j + 1] = (jfloat)xyz[3 * j + 1];
-            P[1 + 5 * j + 2] = (jfloat)xyz[3 * j + 2];
+            P[1 + 5 * j + 0] = xyzf[3 * j + 0];
+            P[1 + 5 * j + 1] = xyzf[3 * j + 1];
+            P[1 + 5 * j + 2] = xyzf[3 * j + 2];
             P[1 + 5 * j + 3] = (jfloat)j;
             P[1 + 5 * j + 4] = (jfloat)ids[j];
         }

@@ -110,7 +110,10 @@ class Engine:
 
     # -- state -----------------------------------------------------------
     def set_particles(self, xyz, types, offsets=None):
-        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        """Upload positions (n, 3) and types; float32 positions go through
+        rdgpu_set_particles_f32 (half the bytes), anything else as float64."""
+        f32 = isinstance(xyz, np.ndarray) and xyz.dtype == np.float32
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32 if f32 else np.float64).reshape(-1, 3)
         types = np.ascontiguousarray(types, dtype=np.int32).reshape(-1)
         n = types.size
         if offsets is not None:
@@ -118,19 +121,28 @@ class Engine:
             offp = _p(off, C.c_int64)
         else:
             offp = None
-        self._check(_lib().rdgpu_set_particles(self._h, offp, n, _p(xyz, C.c_double), _p(types, C.c_int32)))
+        if f32:
+            rc = _lib().rdgpu_set_particles_f32(self._h, offp, n, _p(xyz, C.c_float), _p(types, C.c_int32))
+        else:
+            rc = _lib().rdgpu_set_particles(self._h, offp, n, _p(xyz, C.c_double), _p(types, C.c_int32))
+        self._check(rc)
         self.n = n
 
     def get_particles(self, xyz=None, types=None):
         """Positions (n, 3) float64 and types; into the given C-contiguous
-        arrays when passed (e.g. pinned host buffers)."""
+        arrays when passed (e.g. pinned host buffers); a float32 xyz array
+        is filled through rdgpu_get_particles_f32."""
         if xyz is None:
             xyz = np.empty((self.n, 3))
         if types is None:
             types = np.empty(self.n, np.int32)
-        assert xyz.dtype == np.float64 and xyz.shape == (self.n, 3) and xyz.flags.c_contiguous
+        assert xyz.dtype in (np.float64, np.float32) and xyz.shape == (self.n, 3) and xyz.flags.c_contiguous
         assert types.dtype == np.int32 and types.shape == (self.n,) and types.flags.c_contiguous
-        self._check(_lib().rdgpu_get_particles(self._h, _p(xyz, C.c_double), _p(types, C.c_int32)))
+        if xyz.dtype == np.float32:
+            rc = _lib().rdgpu_get_particles_f32(self._h, _p(xyz, C.c_float), _p(types, C.c_int32))
+        else:
+            rc = _lib().rdgpu_get_particles(self._h, _p(xyz, C.c_double), _p(types, C.c_int32))
+        self._check(rc)
         return xyz, types
 
     def set_bonds(self, ij, pot, potentials):
