@@ -24,7 +24,7 @@ e2e:   the same metric through the C ABI with host buffers: every frame of
        reference's float frames, FP64 for the FP64 engine), steps, and
        downloads them (rdgpu_get_particles),
        the per-frame traffic of the reference's JNI frame loop.
-plain_f64: the north star's denominator, the plain FP64 single-system path:
+plain_f64: the metric's denominator, the plain FP64 single-system path:
        32 of the workload's systems, each alone in its own FP64 handle.
 --impl reference: the CPU path of the reference semantics (the C oracle port,
        all host threads, the reference's Java core cannot run here) on a
