@@ -22,6 +22,8 @@ using namespace rdgpu;
 namespace {
 thread_local std::string g_create_error;
 constexpr int kStepBlock = 128;
+// internal: do_steps_list stopped early so that do_steps re-tunes (never returned by the ABI)
+constexpr int RDGPU_OK_CONTINUE = 1;
 // hot particles (moved more than about skin/2 since the build) the list check
 // looks at after a step, at most (fewer for small handles); with more, the
 // step rebuilds the list instead
@@ -112,6 +114,8 @@ struct rdgpu_engine {
     double max_rc = 0.0;                 // largest pair cutoff
     double cell_cut = 0.0;               // lower bound of the cell edge of the current grid
     bool tuned = false;
+    bool tuning = false;                 // inside tune(): its trials do not re-tune
+    bool retune = false;                 // the lists outgrew their capacity: tune again
     ListCtl* ctl = nullptr;
     ListCtl* pinned_ctl = nullptr;
     int nbuild_h = 0;
@@ -927,6 +931,12 @@ template <class R> int do_steps_list(Engine* E, long long nsteps, const double* 
             if (rc) return rc;
             rc = resort<R>(E, true);
             if (rc) return rc;
+            // the particles gathered into denser clusters than the tuner saw:
+            // an AUTO handle times its options again on the new state
+            if (E->nb_req == RDGPU_NB_AUTO && !E->tuning && !noise_d) {
+                E->retune = true;
+                return RDGPU_OK_CONTINUE;
+            }
             continue;
         }
         rc = prepare_step_state(E, tf);
@@ -951,6 +961,8 @@ template <class R> int do_steps_mode(Engine* E, long long nsteps, const double* 
 template <class R> int tune(Engine* E)
 {
     E->tuned = true;
+    E->tuning = true;
+    struct Done { Engine* e; ~Done() { e->tuning = false; } } done_{E};
     const long long N = E->npart_tot;
     if (N == 0 || E->graph_steps <= 0) return RDGPU_OK;
     const size_t recA = sizeof(R) == 4 ? 16 : 32;
@@ -1020,11 +1032,19 @@ template <class R> int prepare_graph(Engine* E)
 
 template <class R> int do_steps(Engine* E, long long nsteps, const double* noise_d)
 {
-    if (E->nb_req == RDGPU_NB_AUTO && !E->tuned && !noise_d && nsteps >= 4LL * std::max(E->graph_steps, 1)) {
-        int rc = tune<R>(E);
-        if (rc) return rc;
+    const long long target = E->step_h + nsteps;
+    for (;;) {
+        const long long left = target - E->step_h;
+        if (left <= 0) return RDGPU_OK;
+        if (E->nb_req == RDGPU_NB_AUTO && (!E->tuned || E->retune) && !noise_d &&
+            left >= 4LL * std::max(E->graph_steps, 1)) {
+            E->retune = false;
+            int rc = tune<R>(E);
+            if (rc) return rc;
+        }
+        const int rc = do_steps_mode<R>(E, left, noise_d);
+        if (rc != RDGPU_OK_CONTINUE) return rc;
     }
-    return do_steps_mode<R>(E, nsteps, noise_d);
 }
 
 int setup_systems(Engine* E, std::string& why)
