@@ -25,7 +25,7 @@ e2e:   the same metric through the C ABI with host buffers: every frame of
        downloads them (rdgpu_get_particles),
        the per-frame traffic of the reference's JNI frame loop.
 plain_f64: the metric's denominator, the plain FP64 single-system path:
-       32 of the workload's systems, each alone in its own FP64 handle.
+       every system of the workload alone in its own FP64 handle.
 --impl reference: the CPU path of the reference semantics (the C oracle port,
        all host threads, the reference's Java core cannot run here) on a
        bounded sample of the same workload.
@@ -134,11 +134,25 @@ def dist_env():
     return replicas.env()
 
 
-def workload(config, rank):
+def workload(config, reference=False):
+    """The benchmark input.  Building it maps no library of the engine
+    (readdygpu_b200 loads libreaddy_b200.so on first use only); the reference
+    arm takes config 3's insertion from the oracle, which gives the same
+    coordinates as the engine package's generator."""
     from readdygpu_b200 import configs
-    if config == 4:
-        return configs.config4()
+    if config == 3 and reference:
+        from oracle import oracle as O
+        return configs.config3(rsa=O.rsa_spheres)
     return configs.CONFIGS[config]()
+
+
+def bench_config(w, ws):
+    """The `config` object of the JSON line, the same in both arms."""
+    alg = 64 * w.n
+    return {"workload": w.name, "particles": w.n, "systems": len(w.boxes) if w.boxes else 1,
+            "parallelism": f"replicas{ws}",
+            "l2": "inputs larger than L2 (state read+written per step exceeds 126 MB)" if alg > 126e6
+            else "state fits in L2"}
 
 
 def cpu_baseline(w, budget_s=12.0, threads=None):
@@ -203,18 +217,15 @@ def host_cpu_model():
     return "unknown"
 
 
-def plain_f64(w, local, steps=200, sample=32):
-    """The plain FP64 single-system GPU path (the drop-in): each sampled system
-    of the batch alone in its own FP64 handle with default options (autotuned
+def plain_f64(w, local, steps=200):
+    """The plain FP64 single-system GPU path (the drop-in): every system of the
+    batch alone in its own FP64 handle with default options (autotuned
     before timing), stepped `steps` steps after as many warm-up steps; the
     particle-steps/s of running them one after another, device-timed."""
     import numpy as np
     import torch
     import readdygpu_b200 as R
-    if w.boxes is None:
-        picks = [None]
-    else:
-        picks = sorted(set(np.linspace(0, len(w.boxes) - 1, sample).round().astype(int).tolist()))
+    picks = [None] if w.boxes is None else list(range(len(w.boxes)))
     ps, ms, npart = 0.0, 0.0, 0
     for k in picks:
         if k is None:
@@ -240,21 +251,21 @@ def plain_f64(w, local, steps=200, sample=32):
         eng.close()
     return {"value": ps / (ms / 1e3), "unit": "particle-steps/s", "systems": len(picks), "particles": npart,
             "steps": steps,
-            "sample": f"{len(picks)} of the workload's systems spread over its size range, each alone in an FP64 "
-                      f"handle, {steps} timed steps each"}
+            "sample": f"all {len(picks)} systems of the workload, each alone in an FP64 handle, {steps} timed "
+                      f"steps each"}
 
 
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return
-    w = workload(args.config, 0)
+    w = workload(args.config, reference=True)
     cb = cpu_baseline(w, budget_s=20.0)
     cb["cpu_model"] = host_cpu_model()
     line = {"impl": "reference", "metric": "particle-steps/s", "value": cb["value"], "unit": "particle-steps/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": w.name, "particles": w.n, "systems": len(w.boxes) if w.boxes else 1},
+            "config": bench_config(w, ws),
             "cpu_baseline": cb,
             "e2e": {"value": cb["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
@@ -272,7 +283,7 @@ def run_ours(args):
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
     replicas.init("nccl")
-    w = workload(args.config, rank)
+    w = workload(args.config)
     kw = {}
     if w.boxes is not None:
         # each rank owns its own replicate ensemble: shift the seeds
@@ -360,13 +371,8 @@ def run_ours(args):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32" if args.precision == "f32c" else "f64",
                 "data": "synthetic",
-                "config": {"workload": w.name, "particles": w.n,
-                           "systems": len(w.boxes) if w.boxes else 1, "precision": args.precision,
-                           "parallelism": f"replicas{ws}",
-                           "neighbour": {"mode": nb["neighbour_mode"], "skin_nm": nb["skin"],
-                                         "requested": args.neighbour},
-                           "l2": "inputs larger than L2 (state read+written per step exceeds 126 MB)"
-                           if alg > 126e6 else "state fits in L2"},
+                "config": bench_config(w, ws), "precision": args.precision,
+                "neighbour": {"mode": nb["neighbour_mode"], "skin_nm": nb["skin"], "requested": args.neighbour},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_kind": peak_kind,
                              "traffic": (tpp * w.n if tpp else None),

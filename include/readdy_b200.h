@@ -326,9 +326,12 @@ int64_t rdgpu_launch_count(rdgpu_handle h);
 /* Runs nsteps steps one launch at a time (no CUDA graph) with CUDA events on
    the handle's stream around the step kernel and around what follows it in
    the step: the counting sort (scan + scatter) of the cell walk, or the
-   re-sort and list build of the pair list (no-ops in steps that need no
-   rebuild).  Returns their mean duration per step in milliseconds.  The
-   state advances exactly as with rdgpu_step.  No reference counterpart
+   list check, re-sort and list build of the pair list (no-ops in steps that
+   need no rebuild).  Steps are queued in batches of 16 without a
+   synchronisation in between, so each event pair brackets a kernel that was
+   already queued; the first step of a batch (queued on an idle stream) is not
+   counted.  Returns the mean durations per step in milliseconds.  The state
+   advances exactly as with rdgpu_step.  No reference counterpart
    (measurement hook).                                                        */
 int rdgpu_step_profile(rdgpu_handle h, int64_t nsteps, double* step_kernel_ms, double* sort_ms);
 

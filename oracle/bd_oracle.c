@@ -602,6 +602,68 @@ void orc_neighbor_digest_f32(const rdgpu_system_desc* d, int64_t n, const float*
     }
 }
 
+/* The same digests from a cell list, OpenMP over particles: for the
+   benchmark configurations at their full sizes.  The cells (edge >= the
+   largest cutoff x (1 + 1e-4), so that a pair that rounds under its FP32
+   cutoff is still in adjacent cells) only select candidates; the predicate
+   and its arithmetic are the brute-force functions' above.                  */
+static void digest_cells(const rdgpu_system_desc* d, int64_t n, const double* xd, const float* xf,
+                         const int32_t* types, int32_t* counts, uint64_t* hashes, int n_threads)
+{
+    tables_t t;
+    make_tables(d, &t);
+    double* xc = (double*)xd;
+    if (xf) {
+        xc = (double*)malloc((size_t)(n > 0 ? n : 1) * 3 * sizeof(double));
+        for (int64_t i = 0; i < 3 * n; ++i) xc[i] = (double)xf[i];
+    }
+    cells_t c;
+    build_cells(&t, max_rc(&t) * (1.0 + 1e-4), n, xc, &c);
+    if (n_threads < 1) n_threads = 1;
+#pragma omp parallel for num_threads(n_threads) schedule(dynamic, 4096)
+    for (int64_t i = 0; i < n; ++i) {
+        int32_t cnt = 0;
+        uint64_t h = 0;
+        const int ti = types[i];
+        int64_t st[27], en[27];
+        int nr = neighbour_ranges(&c, &t, xc, i, n, st, en);
+        for (int rr = 0; rr < nr; ++rr) for (int64_t q = st[rr]; q < en[rr]; ++q) {
+            const int64_t j = NB_J(&c, q);
+            if (j == i) continue;
+            const int tj = types[j];
+            int in;
+            if (xf) {
+                float dx = mimgf(xf[3 * i + 0], xf[3 * j + 0], t.Lf[0], t.halff[0], t.per[0]);
+                float dy = mimgf(xf[3 * i + 1], xf[3 * j + 1], t.Lf[1], t.halff[1], t.per[1]);
+                float dz = mimgf(xf[3 * i + 2], xf[3 * j + 2], t.Lf[2], t.halff[2], t.per[2]);
+                in = ((dx * dx + dy * dy) + dz * dz) < t.rc2f[ti * MT + tj];
+            } else {
+                double dx = mimg(xd[3 * i + 0], xd[3 * j + 0], t.L[0], t.half[0], t.per[0]);
+                double dy = mimg(xd[3 * i + 1], xd[3 * j + 1], t.L[1], t.half[1], t.per[1]);
+                double dz = mimg(xd[3 * i + 2], xd[3 * j + 2], t.L[2], t.half[2], t.per[2]);
+                in = ((dx * dx + dy * dy) + dz * dz) < t.rc2[ti * MT + tj];
+            }
+            if (in) { cnt++; h += orc_splitmix64((uint64_t)j); }
+        }
+        counts[i] = cnt;
+        hashes[i] = h;
+    }
+    free_cells(&c);
+    if (xf) free(xc);
+}
+
+void orc_neighbor_digest_cells_f64(const rdgpu_system_desc* d, int64_t n, const double* xrel,
+                                   const int32_t* types, int32_t* counts, uint64_t* hashes, int n_threads)
+{
+    digest_cells(d, n, xrel, NULL, types, counts, hashes, n_threads);
+}
+
+void orc_neighbor_digest_cells_f32(const rdgpu_system_desc* d, int64_t n, const float* xrel,
+                                   const int32_t* types, int32_t* counts, uint64_t* hashes, int n_threads)
+{
+    digest_cells(d, n, NULL, xrel, types, counts, hashes, n_threads);
+}
+
 /* ------------------------------------------------------------------------ */
 /* Euler-Maruyama step.                                                     */
 /* ------------------------------------------------------------------------ */
@@ -826,4 +888,71 @@ int orc_max_threads(void)
 #else
     return 1;
 #endif
+}
+
+/* ------------------------------------------------------------------------ */
+/* Input generator of the config-3 workload for the benchmark's reference   */
+/* arm: random sequential insertion of non-overlapping spheres, the same    */
+/* proposals (SplitMix64 uniforms) and acceptance rule as the engine        */
+/* package's generator, so both arms step identical coordinates.            */
+/* ------------------------------------------------------------------------ */
+
+static double orc_sm_uniform(uint64_t* s)
+{
+    uint64_t z = (*s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+int64_t orc_rsa_spheres(int64_t n, double L, double diam, uint64_t seed, int64_t max_attempts, double* xyz)
+{
+    int nc = (int)floor(L / diam);
+    if (nc < 3) nc = 3 > (int)(L / diam) ? (int)(L / diam) : 3;
+    if (nc < 1) nc = 1;
+    const double c = L / nc;
+    const int cap = 16;
+    const size_t ncell = (size_t)nc * nc * nc;
+    int32_t* cnt = (int32_t*)calloc(ncell, sizeof(int32_t));
+    int64_t* slot = (int64_t*)malloc(ncell * cap * sizeof(int64_t));
+    uint64_t rs = seed;
+    const double d2 = diam * diam;
+    int64_t placed = 0;
+    for (int64_t att = 0; att < max_attempts && placed < n; ++att) {
+        double p[3];
+        for (int a = 0; a < 3; ++a) p[a] = orc_sm_uniform(&rs) * L;
+        int ci[3];
+        for (int a = 0; a < 3; ++a) {
+            int k = (int)(p[a] / c);
+            ci[a] = k >= nc ? nc - 1 : k;
+        }
+        int ok = 1;
+        for (int dz = -1; dz <= 1 && ok; ++dz)
+            for (int dy = -1; dy <= 1 && ok; ++dy)
+                for (int dx = -1; dx <= 1 && ok; ++dx) {
+                    int x = (ci[0] + dx + nc) % nc, y = (ci[1] + dy + nc) % nc, z = (ci[2] + dz + nc) % nc;
+                    size_t cell = ((size_t)z * nc + y) * nc + x;
+                    for (int q = 0; q < cnt[cell]; ++q) {
+                        const double* o = xyz + 3 * slot[cell * cap + q];
+                        double r2 = 0.0;
+                        for (int a = 0; a < 3; ++a) {
+                            double dd = p[a] - o[a];
+                            if (dd > 0.5 * L) dd -= L;
+                            else if (dd < -0.5 * L) dd += L;
+                            r2 += dd * dd;
+                        }
+                        if (r2 < d2) { ok = 0; break; }
+                    }
+                }
+        if (!ok) continue;
+        size_t cell = ((size_t)ci[2] * nc + ci[1]) * nc + ci[0];
+        if (cnt[cell] >= cap) continue;
+        slot[cell * cap + cnt[cell]++] = placed;
+        for (int a = 0; a < 3; ++a) xyz[3 * placed + a] = p[a];
+        ++placed;
+    }
+    free(cnt);
+    free(slot);
+    return placed;
 }

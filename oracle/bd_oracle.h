@@ -68,6 +68,15 @@ void orc_neighbor_digest_f32(const rdgpu_system_desc* d, int64_t n,
                              const float* xrel, const int32_t* types,
                              int32_t* counts, uint64_t* hashes);
 
+/* The same digests from a cell list, OpenMP over n_threads threads: for
+   large systems (the benchmark configurations at their full sizes).         */
+void orc_neighbor_digest_cells_f64(const rdgpu_system_desc* d, int64_t n,
+                                   const double* xrel, const int32_t* types,
+                                   int32_t* counts, uint64_t* hashes, int n_threads);
+void orc_neighbor_digest_cells_f32(const rdgpu_system_desc* d, int64_t n,
+                                   const float* xrel, const int32_t* types,
+                                   int32_t* counts, uint64_t* hashes, int n_threads);
+
 /* One Euler-Maruyama step with injected noise (3 per particle):
    x <- x + D dt/(kB T) F + sqrt(2 D dt) xi, then periodic wrap.
    Returns 0, or RDGPU_ERR_JUMP if a particle moved more than a box length.  */
@@ -110,6 +119,11 @@ int orc_run_steps_f64(const rdgpu_system_desc* d, int64_t n, double* xrel,
                       int64_t nsteps, int n_threads);
 
 int orc_max_threads(void);
+
+/* Config-3 input for the benchmark's reference arm: random sequential
+   insertion of n spheres of diameter diam into the periodic box [0,L)^3,
+   SplitMix64 proposals from `seed`; returns the number placed.              */
+int64_t orc_rsa_spheres(int64_t n, double L, double diam, uint64_t seed, int64_t max_attempts, double* xyz);
 
 #ifdef __cplusplus
 }

@@ -42,6 +42,9 @@ def lib():
             "orc_splitmix64": (C.c_uint64, [C.c_uint64]),
             "orc_run_steps_f64": (C.c_int, [SD, C.c_int64, DP, I32P, C.c_uint64, C.c_int64, C.c_int64, C.c_int]),
             "orc_max_threads": (C.c_int, []),
+            "orc_neighbor_digest_cells_f64": (None, [SD, C.c_int64, DP, I32P, I32P, U64P, C.c_int]),
+            "orc_neighbor_digest_cells_f32": (None, [SD, C.c_int64, FP, I32P, I32P, U64P, C.c_int]),
+            "orc_rsa_spheres": (C.c_int64, [C.c_int64, C.c_double, C.c_double, C.c_uint64, C.c_int64, DP]),
             "orc_bond_forces_f64": (C.c_int, [SD, C.c_int64, DP, I32P, C.c_int64, I32P, I32P, C.c_int32,
                                               C.POINTER(A.PairPot), DP, DP]),
         }
@@ -136,6 +139,35 @@ def neighbor_digest(desc, xrel, types, f32=False):
         lib().orc_neighbor_digest_f64(C.byref(desc), n, _p(x, C.c_double), _p(types, C.c_int32),
                                       _p(cnt, C.c_int32), _p(h, C.c_uint64))
     return cnt, h
+
+
+def neighbor_digest_cells(desc, xrel, types, f32=False, threads=None):
+    """neighbor_digest from a cell list with OpenMP (large systems)."""
+    types = _c(types, np.int32)
+    n = types.size
+    cnt = np.zeros(n, np.int32)
+    h = np.zeros(n, np.uint64)
+    threads = threads or max_threads()
+    if f32:
+        x = _c(xrel, np.float32)
+        lib().orc_neighbor_digest_cells_f32(C.byref(desc), n, _p(x, C.c_float), _p(types, C.c_int32),
+                                            _p(cnt, C.c_int32), _p(h, C.c_uint64), threads)
+    else:
+        x = _c(xrel, np.float64)
+        lib().orc_neighbor_digest_cells_f64(C.byref(desc), n, _p(x, C.c_double), _p(types, C.c_int32),
+                                            _p(cnt, C.c_int32), _p(h, C.c_uint64), threads)
+    return cnt, h
+
+
+def rsa_spheres(n, L, diam, seed, max_attempts=None):
+    """Random sequential insertion (the config-3 input) for the benchmark's
+    reference arm; the same coordinates as readdygpu_b200.configs.rsa_spheres."""
+    xyz = np.empty((n, 3))
+    got = lib().orc_rsa_spheres(n, L, diam, seed, 200 * n if max_attempts is None else max_attempts,
+                                _p(xyz, C.c_double))
+    if got < n:
+        raise RuntimeError(f"random sequential insertion placed only {got} of {n} spheres")
+    return xyz
 
 
 def step_f64(desc, xrel, types, noise, threads=1):

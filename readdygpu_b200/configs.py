@@ -107,17 +107,18 @@ def config2(n=100_000, steps=10_000):
     return Workload("config2_4species_100k", sys_, xyz, types, steps)
 
 
-def config3(n=1_000_000, steps=5_000, phi=0.30):
+def config3(n=1_000_000, steps=5_000, phi=0.30, rsa=None):
     """n identical spheres of radius 2 nm at volume fraction phi in a periodic
     cube (seeded random sequential insertion without overlap); D 1e6 nm^2/s;
     harmonic repulsion k=10 (cutoff 4 nm = cell size); RDF 200 bins over
-    0-20 nm every 100 steps."""
+    0-20 nm every 100 steps.  rsa: the insertion routine (default
+    rsa_spheres; any routine with its arguments and coordinates)."""
     r = 2.0
     L = float_exact_box((n * 4.0 / 3.0 * math.pi * r ** 3 / phi) ** (1.0 / 3.0))
     sys_ = System([ParticleType("A", 1e6, r)],
                   pair=[PairPotential(A.P2_HARMONIC, [(0, 0)], 10.0, "repulsive")],
                   kT=KT, dt=1e-9, lo=(0, 0, 0), hi=(L, L, L), periodic=(1, 1, 1), cell_size=4.0)
-    xyz = rsa_spheres(n, L, 2 * r, SEED0 + 3)
+    xyz = (rsa or rsa_spheres)(n, L, 2 * r, SEED0 + 3)
     return Workload(f"config3_rsa_{n}", sys_, xyz, np.zeros(n, np.int32), steps,
                     notes="RDF 200 bins 0-20 nm every 100 steps")
 

@@ -128,9 +128,12 @@ struct rdgpu_engine {
     int list_cap = 0;
     std::vector<double> rc_h;            // pair cutoff per type pair (0: no potential)
     void* rl2_d = nullptr;               // squared list radius per type pair, in the state precision
-    // CUDA graphs of graph_steps steps: cell walk, pair list
-    cudaGraphExec_t graph = nullptr;
-    cudaGraphExec_t lgraph = nullptr;
+    // captured step graphs by step count, cell walk and pair list: graph_steps
+    // steps and every power of two below it.  A call of n steps replays
+    // n / graph_steps full graphs and the rest as a sum of powers of two, so
+    // short calls run graphed too.
+    std::map<int, cudaGraphExec_t> cgraphs;
+    std::map<int, cudaGraphExec_t> lgraphs;
     int graph_steps = 100;
     long long launches = 0;
     std::string last_error;
@@ -291,17 +294,41 @@ template <class R> void build_ext(const rdgpu_system_desc& d, const rdgpu_box& b
 // ---------------------------------------------------------------------------
 // buffers
 // ---------------------------------------------------------------------------
-void drop_graphs(Engine* E)
+void drop_graph_map(std::map<int, cudaGraphExec_t>& m)
 {
-    if (E->graph) { cudaGraphExecDestroy(E->graph); E->graph = nullptr; }
-    if (E->lgraph) { cudaGraphExecDestroy(E->lgraph); E->lgraph = nullptr; }
+    for (auto& kv : m) cudaGraphExecDestroy(kv.second);
+    m.clear();
 }
 
-// the current state moved to buffer c; the cell-walk graph captured the old one
+void drop_graphs(Engine* E)
+{
+    drop_graph_map(E->cgraphs);
+    drop_graph_map(E->lgraphs);
+}
+
+// the current state moved to buffer c; the cell-walk graphs captured the old one
 void set_cur(Engine* E, int c)
 {
-    if (c != E->cur && E->graph) { cudaGraphExecDestroy(E->graph); E->graph = nullptr; }
+    if (c != E->cur) drop_graph_map(E->cgraphs);
     E->cur = c;
+}
+
+// The graph sizes a call of `remaining` steps replays, largest first: full
+// graphs of graph_steps steps, then the bits of the remainder.
+template <class F> int for_each_graph(const Engine* E, long long remaining, F&& f)
+{
+    const long long G = E->graph_steps;
+    for (long long g = 0; g < remaining / G; ++g) {
+        const int rc = f((int)G);
+        if (rc) return rc;
+    }
+    const long long r = remaining % G;
+    for (long long p = 1LL << 30; p >= 1; p >>= 1)
+        if (r & p) {
+            const int rc = f((int)p);
+            if (rc) return rc;
+        }
+    return RDGPU_OK;
 }
 
 void free_particles(Engine* E)
@@ -455,19 +482,25 @@ template <class R> int launch_steps(Engine* E, int n, const double* noise_d)
     return RDGPU_OK;
 }
 
-template <class R> int capture_graph(Engine* E)
+// the cell-walk graph of n steps (captured on first use)
+template <class R> int capture_graph(Engine* E, int n, cudaGraphExec_t* out)
 {
-    if (E->graph) return RDGPU_OK;
+    const auto it = E->cgraphs.find(n);
+    if (it != E->cgraphs.end()) { *out = it->second; return RDGPU_OK; }
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(E->stream, cudaStreamCaptureModeThreadLocal));
     long long l0 = E->launches;
-    int rc = launch_steps<R>(E, E->graph_steps, nullptr);
+    int rc = launch_steps<R>(E, n, nullptr);
     cudaError_t ce = cudaStreamEndCapture(E->stream, &g);
     E->launches = l0;
     if (rc) return rc;
     CK(ce);
-    CK(cudaGraphInstantiate(&E->graph, g, 0));
+    cudaGraphExec_t x = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&x, g, 0);
     cudaGraphDestroy(g);
+    CK(ie);
+    E->cgraphs[n] = x;
+    *out = x;
     return RDGPU_OK;
 }
 
@@ -475,16 +508,17 @@ template <class R> int do_steps_cells(Engine* E, long long nsteps, const double*
 {
     const long long target = E->step_h + nsteps;
     long long remaining = nsteps;
-    if (E->graph_steps > 0 && !noise_d && remaining >= E->graph_steps) {
-        int rc = capture_graph<R>(E);
+    if (E->graph_steps > 0 && !noise_d) {
+        int rc = for_each_graph(E, remaining, [&](int n) -> int {
+            cudaGraphExec_t x;
+            const int r = capture_graph<R>(E, n, &x);
+            if (r) return r;
+            CK(cudaGraphLaunch(x, E->stream));
+            E->launches += (long long)n * ((E->npart_tot > 0) ? 4 : 3) + 1;
+            return RDGPU_OK;
+        });
         if (rc) return rc;
-        const long long ng = remaining / E->graph_steps;
-        const long long per_graph = (long long)E->graph_steps * ((E->npart_tot > 0) ? 4 : 3) + 1;
-        for (long long g = 0; g < ng; ++g) {
-            CK(cudaGraphLaunch(E->graph, E->stream));
-            E->launches += per_graph;
-        }
-        remaining -= ng * E->graph_steps;
+        remaining = 0;
     }
     while (remaining > 0) {
         const int n = (int)std::min<long long>(remaining, 1000);
@@ -628,7 +662,7 @@ int ensure_list(Engine* E, int cap)
     // groups of 4 entries (one int4), at least two of them: the step kernel
     // requests the first 8 entries before it knows the list length
     cap = (std::max(std::max(cap, E->list_cap), 8) + 3) & ~3;
-    if (E->lgraph) { cudaGraphExecDestroy(E->lgraph); E->lgraph = nullptr; }
+    drop_graph_map(E->lgraphs);
     dfree(E->nbr); dfree(E->xref); dfree(E->hot);
     E->list_cap = 0;
     E->list_stride = 0;
@@ -825,7 +859,7 @@ template <class R> int enter_list(Engine* E, double skin)
         int rc = configure_cells(E, cut, why);
         if (rc) return fail(E, rc, why);
     }
-    if (E->skin != skin && E->lgraph) { cudaGraphExecDestroy(E->lgraph); E->lgraph = nullptr; }
+    if (E->skin != skin) drop_graph_map(E->lgraphs);
     E->skin = skin;
     E->nb_mode = RDGPU_NB_LIST;
     {
@@ -865,21 +899,27 @@ template <class R> int enter_cells(Engine* E)
     return RDGPU_OK;
 }
 
-template <class R> int capture_list_graph(Engine* E)
+// the pair-list graph of n steps (captured on first use)
+template <class R> int capture_list_graph(Engine* E, int n, cudaGraphExec_t* out)
 {
-    if (E->lgraph) return RDGPU_OK;
+    const auto it = E->lgraphs.find(n);
+    if (it != E->lgraphs.end()) { *out = it->second; return RDGPU_OK; }
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(E->stream, cudaStreamCaptureModeThreadLocal));
     long long l0 = E->launches;
     E->capturing = true;
-    int rc = launch_list_steps<R>(E, E->graph_steps, nullptr);
+    int rc = launch_list_steps<R>(E, n, nullptr);
     E->capturing = false;
     cudaError_t ce = cudaStreamEndCapture(E->stream, &g);
     E->launches = l0;
     if (rc) return rc;
     CK(ce);
-    CK(cudaGraphInstantiate(&E->lgraph, g, 0));
+    cudaGraphExec_t x = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&x, g, 0);
     cudaGraphDestroy(g);
+    CK(ie);
+    E->lgraphs[n] = x;
+    *out = x;
     return RDGPU_OK;
 }
 
@@ -890,23 +930,22 @@ template <class R> int do_steps_list(Engine* E, long long nsteps, const double* 
         long long remaining = target - E->step_h;
         int rc = write_ctl(E, 0);
         if (rc) return rc;
-        const long long per_graph = (long long)E->graph_steps * 2 + 1;
         const int nb0 = E->nbuild_h;
-        if (E->graph_steps > 0 && !noise_d && remaining >= E->graph_steps) {
-            rc = capture_list_graph<R>(E);
+        const bool graphed = E->graph_steps > 0 && !noise_d;
+        if (graphed) {
+            rc = for_each_graph(E, remaining, [&](int n) -> int {
+                cudaGraphExec_t x;
+                const int r = capture_list_graph<R>(E, n, &x);
+                if (r) return r;
+                CK(cudaGraphLaunch(x, E->stream));
+                E->launches += 2LL * n + 1;
+                return RDGPU_OK;
+            });
             if (rc) return rc;
-            const long long ng = remaining / E->graph_steps;
-            for (long long g = 0; g < ng; ++g) {
-                CK(cudaGraphLaunch(E->lgraph, E->stream));
-                E->launches += per_graph;
-            }
-            remaining -= ng * E->graph_steps;
-            // the re-sorts that ran inside the graphs (six kernels each)
-            rc = read_back(E);
-            if (rc) return rc;
-            E->launches += 6LL * std::max(0, E->nbuild_h - nb0);
+            remaining = 0;
         }
-        // the rest, after the graphs (the step counter and parity carry over on the device)
+        // without graphs (injected noise, or graphs off): kernel by kernel
+        // (the step counter and parity carry over on the device)
         while (remaining > 0) {
             const int n = (int)std::min<long long>(remaining, 1000);
             rc = launch_list_steps<R>(E, n, noise_d);
@@ -915,6 +954,8 @@ template <class R> int do_steps_list(Engine* E, long long nsteps, const double* 
         }
         rc = read_back(E);
         if (rc) return rc;
+        // the re-sorts that ran inside the graphs (six kernels each)
+        if (graphed) E->launches += 6LL * std::max(0, E->nbuild_h - nb0);
         const int ef = *E->pinned_err;
         const int nreb = E->pinned_ctl->nreb;
         if (ef == 0) {
@@ -965,6 +1006,9 @@ template <class R> int tune(Engine* E)
     struct Done { Engine* e; ~Done() { e->tuning = false; } } done_{E};
     const long long N = E->npart_tot;
     if (N == 0 || E->graph_steps <= 0) return RDGPU_OK;
+    // the trials' launches and list builds are not the run's
+    const long long launches0 = E->launches;
+    const int nbuild0 = E->nbuild_h;
     const size_t recA = sizeof(R) == 4 ? 16 : 32;
     void* snapA = nullptr;
     void* snapB = nullptr;
@@ -1018,16 +1062,26 @@ template <class R> int tune(Engine* E)
     if (snapB) cudaFree(snapB);
     if (rc) return rc;
     E->step_h = step0;
+    E->launches = launches0;
+    E->nbuild_h = nbuild0;
     rc = prepare_step_state(E, step0);
     if (rc) return rc;
     return best_skin > 0.0 ? enter_list<R>(E, best_skin) : (E->nb_mode = RDGPU_NB_LIST, enter_cells<R>(E));
 }
 
-// captures the step graph of the mode in effect (nothing runs)
+// captures the step graphs of the mode in effect, graph_steps steps and the
+// powers of two below it, so that no later call captures (nothing runs)
 template <class R> int prepare_graph(Engine* E)
 {
     if (E->graph_steps <= 0) return RDGPU_OK;
-    return E->nb_mode == RDGPU_NB_LIST ? capture_list_graph<R>(E) : capture_graph<R>(E);
+    std::vector<int> sizes = {E->graph_steps};
+    for (int p = 1; p < E->graph_steps; p <<= 1) sizes.push_back(p);
+    for (int n : sizes) {
+        cudaGraphExec_t x;
+        const int rc = E->nb_mode == RDGPU_NB_LIST ? capture_list_graph<R>(E, n, &x) : capture_graph<R>(E, n, &x);
+        if (rc) return rc;
+    }
+    return RDGPU_OK;
 }
 
 template <class R> int do_steps(Engine* E, long long nsteps, const double* noise_d)
@@ -1112,50 +1166,86 @@ int setup_systems(Engine* E, std::string& why)
     return 0;
 }
 
-template <class R> int profile_list(Engine* E, long long nsteps, double* kms, double* sms)
-{
-    int rc = write_ctl(E, 0);
-    if (rc) return rc;
-    cudaEvent_t e0, e1, e2;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
-    CK(cudaEventCreate(&e2));
-    Args<R> a = make_args<R>(E);
-    ListArgs<R> v = make_list_args<R>(E, true);
-    double tk = 0.0, ts = 0.0;
-    long long counted = 0;
-    const long long target = E->step_h + nsteps;
-    while (E->step_h < target) {
-        a.step_off = 0;
-        CK(cudaEventRecord(e0, E->stream));
-        launch_list_step_kernel<R>(E, a, v);
-        CK(cudaEventRecord(e1, E->stream));
-        launch_check<R>(E, a, v, 1, 0, 0, E->stream);
-        launch_chain<R>(E, a, v, 1, E->stream);
-        E->launches += 7;
-        CK(cudaEventRecord(e2, E->stream));
-        advance_kernel<<<1, 32, 0, E->stream>>>(E->step_d, E->err, 1);
-        ++E->launches;
-        CK(cudaMemcpyAsync(E->pinned_err, E->err, sizeof(int), cudaMemcpyDeviceToHost, E->stream));
-        CK(cudaStreamSynchronize(E->stream));
-        if (*E->pinned_err == 0) {
+// Event timing of the step kernel and of what follows it in a step.  Steps
+// go out in batches of kProfBatch without a synchronisation in between, so
+// that while the GPU runs one step the host has queued the next: an event
+// pair then brackets the kernel alone.  The first step of each batch starts
+// on an idle stream (its first event would also time the host's launch) and
+// is not counted.
+constexpr int kProfBatch = 16;
+
+struct ProfEvents {
+    cudaEvent_t ev[3 * kProfBatch] = {};
+    int made = 0;
+    ~ProfEvents()
+    {
+        for (int k = 0; k < made; ++k) cudaEventDestroy(ev[k]);
+    }
+    cudaError_t create()
+    {
+        for (; made < 3 * kProfBatch; ++made) {
+            const cudaError_t e = cudaEventCreate(&ev[made]);
+            if (e != cudaSuccess) return e;
+        }
+        return cudaSuccess;
+    }
+    // adds the batch's kernel and follower times (steps 1 .. nb-1)
+    void add(int nb, double& tk, double& ts, long long& counted) const
+    {
+        for (int k = 1; k < nb; ++k) {
             float m1 = 0.f, m2 = 0.f;
-            cudaEventElapsedTime(&m1, e0, e1);
-            cudaEventElapsedTime(&m2, e1, e2);
+            cudaEventElapsedTime(&m1, ev[3 * k], ev[3 * k + 1]);
+            cudaEventElapsedTime(&m2, ev[3 * k + 1], ev[3 * k + 2]);
             tk += m1;
             ts += m2;
             ++counted;
-            ++E->step_h;
-            continue;
         }
-        // a failed step (the step kernel, or the re-sort for the next one): the
-        // input of the failing step tf is intact; a list overflow grows the
-        // lists and re-sorts (the step is not timed), anything else is reported
+    }
+};
+
+template <class R> int profile_list(Engine* E, long long nsteps, double* kms, double* sms)
+{
+    ProfEvents pe;
+    CK(pe.create());
+    double tk = 0.0, ts = 0.0;
+    long long counted = 0;
+    const long long target = E->step_h + nsteps;
+    int rc = RDGPU_OK;
+    while (E->step_h < target) {
+        rc = write_ctl(E, 0);
+        if (rc) break;
+        Args<R> a = make_args<R>(E);
+        const ListArgs<R> v = make_list_args<R>(E, true);
+        const int nb = (int)std::min<long long>(kProfBatch, target - E->step_h);
+        for (int k = 0; k < nb; ++k) {
+            a.step_off = k;
+            CK(cudaEventRecord(pe.ev[3 * k], E->stream));
+            launch_list_step_kernel<R>(E, a, v);
+            CK(cudaEventRecord(pe.ev[3 * k + 1], E->stream));
+            launch_check<R>(E, a, v, k + 1, 0, 0, E->stream);
+            launch_chain<R>(E, a, v, k + 1, E->stream);
+            E->launches += 7;
+            CK(cudaEventRecord(pe.ev[3 * k + 2], E->stream));
+        }
+        advance_kernel<<<1, 32, 0, E->stream>>>(E->step_d, E->err, nb);
+        ++E->launches;
+        CK(cudaGetLastError());
         rc = read_back(E);
         if (rc) break;
         const int ef = *E->pinned_err;
+        const int nreb = E->pinned_ctl->nreb;
+        if (ef == 0) {
+            pe.add(nb, tk, ts, counted);
+            E->step_h += nb;
+            set_cur(E, (int)((E->step_h + nreb) & 1));
+            continue;
+        }
+        // a failed step (the step kernel, or the re-sort for the next one):
+        // the input of the failing step tf is intact; a list overflow grows
+        // the lists and re-sorts (the batch is not timed), anything else is
+        // reported
         E->step_h = *E->pinned_step;
-        set_cur(E, (int)((E->step_h + E->pinned_ctl->nreb) & 1));
+        set_cur(E, (int)((E->step_h + nreb) & 1));
         if (ef != EF_LISTOVF) {
             rc = prepare_step_state(E, E->step_h);
             if (!rc) rc = fail(E, (ef & EF_NONFINITE) ? RDGPU_ERR_NONFINITE : RDGPU_ERR_JUMP,
@@ -1164,18 +1254,9 @@ template <class R> int profile_list(Engine* E, long long nsteps, double* kms, do
         }
         rc = ensure_list(E, list_regrow_cap(E));
         if (!rc) rc = resort<R>(E, true);
-        if (!rc) rc = write_ctl(E, 0);
         if (rc) break;
-        a = make_args<R>(E);
-        v = make_list_args<R>(E, true);
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaEventDestroy(e2);
     if (rc) return rc;
-    rc = read_back(E);
-    if (rc) return rc;
-    set_cur(E, (int)((E->step_h + E->pinned_ctl->nreb) & 1));
     if (kms) *kms = counted > 0 ? tk / counted : 0.0;
     if (sms) *sms = counted > 0 ? ts / counted : 0.0;
     return RDGPU_OK;
@@ -1184,37 +1265,40 @@ template <class R> int profile_list(Engine* E, long long nsteps, double* kms, do
 template <class R> int profile_impl(Engine* E, long long nsteps, double* kms, double* sms)
 {
     if (E->nb_mode == RDGPU_NB_LIST) return profile_list<R>(E, nsteps, kms, sms);
-    cudaEvent_t e0, e1, e2;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
-    CK(cudaEventCreate(&e2));
-    Args<R> a = make_args<R>(E);
+    ProfEvents pe;
+    CK(pe.create());
     double tk = 0.0, ts = 0.0;
-    for (long long k = 0; k < nsteps; ++k) {
-        a.step_off = 0;
-        CK(cudaEventRecord(e0, E->stream));
-        launch_step_kernel<R>(E, a);
-        CK(cudaEventRecord(e1, E->stream));
-        launch_sort<R>(E);
-        CK(cudaEventRecord(e2, E->stream));
-        advance_kernel<<<1, 32, 0, E->stream>>>(E->step_d, E->err, 1);
+    long long counted = 0;
+    for (long long done = 0; done < nsteps;) {
+        const int nb = (int)std::min<long long>(kProfBatch, nsteps - done);
+        Args<R> a = make_args<R>(E);
+        for (int k = 0; k < nb; ++k) {
+            a.step_off = k;
+            CK(cudaEventRecord(pe.ev[3 * k], E->stream));
+            launch_step_kernel<R>(E, a);
+            CK(cudaEventRecord(pe.ev[3 * k + 1], E->stream));
+            launch_sort<R>(E);
+            CK(cudaEventRecord(pe.ev[3 * k + 2], E->stream));
+        }
+        advance_kernel<<<1, 32, 0, E->stream>>>(E->step_d, E->err, nb);
         ++E->launches;
-        CK(cudaEventSynchronize(e2));
-        float m1 = 0.f, m2 = 0.f;
-        cudaEventElapsedTime(&m1, e0, e1);
-        cudaEventElapsedTime(&m2, e1, e2);
-        tk += m1;
-        ts += m2;
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(E->pinned_err, E->err, sizeof(int), cudaMemcpyDeviceToHost, E->stream));
+        CK(cudaMemcpyAsync(E->pinned_step, E->err_step, sizeof(long long), cudaMemcpyDeviceToHost, E->stream));
+        CK(cudaStreamSynchronize(E->stream));
+        if (*E->pinned_err) {
+            // the failing step's input is the current sorted state (its sort was skipped)
+            const long long tf = *E->pinned_step;
+            const int rc = prepare_step_state(E, tf);
+            if (rc) return rc;
+            return fail(E, RDGPU_ERR_JUMP, "a step failed during profiling at step " + std::to_string(tf));
+        }
+        pe.add(nb, tk, ts, counted);
+        E->step_h += nb;
+        done += nb;
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaEventDestroy(e2);
-    CK(cudaMemcpyAsync(E->pinned_err, E->err, sizeof(int), cudaMemcpyDeviceToHost, E->stream));
-    CK(cudaStreamSynchronize(E->stream));
-    if (*E->pinned_err) return fail(E, RDGPU_ERR_JUMP, "a step failed during profiling");
-    E->step_h += nsteps;
-    if (kms) *kms = nsteps > 0 ? tk / nsteps : 0.0;
-    if (sms) *sms = nsteps > 0 ? ts / nsteps : 0.0;
+    if (kms) *kms = counted > 0 ? tk / counted : 0.0;
+    if (sms) *sms = counted > 0 ? ts / counted : 0.0;
     return RDGPU_OK;
 }
 

@@ -119,6 +119,14 @@ extern "C" JNIEXPORT void JNICALL Java_readdy_impl_sim_top_TopGPU_cCreateSimulat
         fflush(stdout);
         return;
     }
+    // choose the neighbour search and capture the step graphs once, before
+    // the frames (otherwise a handle tunes only on a call of >= 400 steps)
+    if (rdgpu_autotune(h) != RDGPU_OK) {
+        printf("error during initialization: %s\n", rdgpu_last_error(h));
+        rdgpu_destroy(h);
+        fflush(stdout);
+        return;
+    }
     jclass cls = env->GetObjectClass(obj);
     jmethodID mid = env->GetMethodID(cls, "frameCallback", "(I[F)Z");
     if (!mid) {

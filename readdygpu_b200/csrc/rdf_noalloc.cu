@@ -2,9 +2,8 @@
 // memory.
 //
 // Some hosts of this library cannot call cudaMalloc: a JVM or another
-// runtime that hands out device buffers from its own pool, a caller that
-// runs inside stream capture, or a plug-in that must not change the device's
-// memory footprint after start-up.  rdgpu_rdf_counts_noalloc computes the
+// runtime that hands out device buffers from its own pool, or a plug-in that
+// must not change the device's memory footprint after start-up.  rdgpu_rdf_counts_noalloc computes the
 // same counts as rdgpu_rdf, on positions and types the caller already has on
 // the device, and writes them to a caller-provided device buffer.  Its scratch
 // memory (cell binning) is the file-scope array below, which every GPU that
@@ -171,7 +170,10 @@ __global__ void na_rdf(const NaScratch* __restrict__ s, long long n, int S, int 
             const int cc[3] = {p.cell % b.n[0], (p.cell / b.n[0]) % b.n[1], p.cell / (b.n[0] * b.n[1])};
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-                int r = (int)ceil(rmax * b.invc[a]);
+                // half-width in cells; the margin keeps the outer layer when
+                // rmax / cell edge rounds onto an integer (the cell edge
+                // L / floor(L / rmax) can round to a hair below rmax)
+                int r = (int)ceil(rmax * b.invc[a] * (1.0 + 1e-12));
                 if (r < 1) r = 1;
                 if (b.per[a]) {
                     if (2 * r + 1 >= b.n[a]) { lo3[a] = 0; cntax[a] = b.n[a]; }

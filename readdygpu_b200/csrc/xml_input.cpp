@@ -310,8 +310,15 @@ int read_all(rdgpu_inputs* I, const char* pp, const char* tp, const char* pg, co
             q.consider_radius = rdxml::trim(at("considerParticleRadius", "true")) != "false";
             for (int t : tl)
                 if (t >= 0 && t < d.n_types) q.types[t] = 1;
+        } else if (type == "WEAK_INTERACTION_HARMONIC" || type == "WEAK_INTERACTION") {
+            // the cubic weak interaction (the reference GPU's
+            // CudaSimulation.cu:1021-1031, Java's P2_WeakInteraction) is not
+            // implemented here: refuse the input rather than run without it
+            I->error = "pair potential type " + type + " (cubic weak interaction) is not supported by this core; "
+                       "use WEAK_INTERACTION_PIECEWISE_HARMONIC";
+            return RDGPU_ERR_ARG;
         } else {
-            I->run.n_unsupported++;   // e.g. WEAK_INTERACTION_HARMONIC, LOLLIPOP
+            I->run.n_unsupported++;   // types neither the reference's GPU core nor this one knows
         }
     }
     // ---- param_global.xml (GlobalParametersHandler.cpp:73-143, XMLReader.cpp:67)

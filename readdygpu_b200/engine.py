@@ -21,8 +21,8 @@ class RdgpuError(RuntimeError):
 
 
 def _lib():
-    from . import lib
-    return lib
+    from . import load
+    return load()
 
 
 def _p(a, ct):

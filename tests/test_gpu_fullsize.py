@@ -42,3 +42,68 @@ def test_fp32c_force_error_full_size(cfg):
     r = precision.force_error(w)
     assert r["force_rel_err"] <= 1e-5, r
     assert r["energy_rel_err"] <= 1e-5, r
+
+
+def _per_system(w):
+    """(descriptor, particle slice) of every system of a workload."""
+    if w.boxes is None:
+        return [(w.system.to_desc(), slice(0, w.n))]
+    out = []
+    for k, (lo, hi, per, _) in enumerate(w.boxes):
+        d = w.system.to_desc()
+        for a in range(3):
+            d.lo[a], d.hi[a], d.periodic[a] = lo[a], hi[a], int(per[a])
+        out.append((d, slice(int(w.offsets[k]), int(w.offsets[k + 1]))))
+    return out
+
+
+def _stored(O, d, xyz, prec):
+    """The positions as the engine stores them (box-relative; FP32 for FP32C)."""
+    if prec == "f64":
+        return O.to_rel_f64(d, xyz).reshape(-1, 3)
+    hi, _ = O.to_rel_f32(d, xyz)
+    return hi.reshape(-1, 3)
+
+
+FULL = {2: configs.config2, 4: configs.config4, 5: configs.config5}
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32c"])
+@pytest.mark.parametrize("cfg", [2, 4, 5])
+def test_full_size_neighbours_and_forces_against_oracle(oracle, cfg, prec):
+    """Configs 2 (100,000, z open, weak interaction + disk), 4 (512 systems,
+    2,445,685 particles) and 5 (250,000, sphere + membrane) at full size,
+    engine against the oracle on the same stored positions:
+      * neighbour sets (count and hash of partner ids per particle): bit-exact,
+        with the FP64 and the FP32 predicate;
+      * FP64 forces ||dF||/||F|| <= 1e-12, energy 1e-10 relative;
+      * FP32C forces ||dF||/||F|| <= 1e-5, per particle 1e-4 max(|F_i|, F_rms),
+        energy 1e-5 relative."""
+    w = FULL[cfg]()
+    kw = {"boxes": w.boxes} if w.boxes is not None else {}
+    with Engine(w.system, precision=prec, **kw) as e:
+        e.set_particles(w.xyz, w.types, offsets=w.offsets)
+        cnt, h = e.neighbor_digest()
+        F, E = e.forces()
+    threads = oracle.max_threads()
+    Fo = np.zeros_like(F)
+    Eo = 0.0
+    for d, sl in _per_system(w):
+        x = _stored(oracle, d, w.xyz[sl], prec)
+        oc, oh = oracle.neighbor_digest_cells(d, x, w.types[sl], f32=(prec == "f32c"), threads=threads)
+        assert np.array_equal(cnt[sl], oc), (cfg, prec, "counts", int(np.abs(cnt[sl] - oc).max()))
+        assert np.array_equal(h[sl], oh), (cfg, prec, "hashes")
+        Fo[sl], e_ = oracle.forces_f64(d, x.astype(np.float64), w.types[sl], threads=threads)
+        Eo += e_
+    assert cnt.sum() > 0
+    rel = np.linalg.norm(F - Fo) / np.linalg.norm(Fo)
+    if prec == "f64":
+        assert rel <= 1e-12, rel
+        assert abs(E - Eo) <= 1e-10 * max(1.0, abs(Eo)), (E, Eo)
+    else:
+        assert rel <= 1e-5, rel
+        per = np.linalg.norm(F - Fo, axis=1)
+        mag = np.linalg.norm(Fo, axis=1)
+        rms = np.sqrt(np.mean(mag ** 2))
+        assert np.all(per <= 1e-4 * np.maximum(mag, rms)), (per / np.maximum(mag, rms)).max()
+        assert abs(E - Eo) <= 1e-5 * max(1.0, abs(Eo)), (E, Eo)

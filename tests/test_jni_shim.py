@@ -116,6 +116,21 @@ def test_input_errors(tmp_path):
     assert rc == A.ERR_ARG and "mismatched" in msg
 
 
+def test_input_refuses_cubic_weak_interaction(tmp_path):
+    """The reference GPU runs WEAK_INTERACTION_HARMONIC (CudaSimulation.cu:1021-1031);
+    this core does not implement it and refuses the input instead of skipping it."""
+    paths, _, _ = write_inputs(tmp_path, n=5)
+    for name in ("WEAK_INTERACTION_HARMONIC", "WEAK_INTERACTION"):
+        txt = open(paths["tplgy_potentials"]).read()
+        pot = (f'<pot name="cubic" type="{name}" forceConst="10" affectedParticleTypeIdPairs="[[0,1]]" '
+               'affectedParticleIdPairs="" />\n</tplgy_potentials>')
+        bad = dict(paths)
+        bad["tplgy_potentials"] = str(tmp_path / f"pots_{name}.xml")
+        open(bad["tplgy_potentials"], "w").write(txt.replace("</tplgy_potentials>", pot))
+        rc, msg, *_ = read_inputs(bad)
+        assert rc == A.ERR_ARG and name in msg and "not supported" in msg
+
+
 def test_jni_without_device_reports_and_returns(tmp_path, capfd):
     try:
         import torch

@@ -64,9 +64,24 @@ def _engine_counts(sys_, xyz, types, nbins, rmax):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("kind", ["periodic", "slab"])
-def test_noalloc_matches_rdgpu_rdf_twice(kind):
+@pytest.mark.parametrize("nbins,rmax", [(60, 12.0), (50, 10.0), (40, 30.0)])
+def test_noalloc_matches_rdgpu_rdf_twice(kind, nbins, rmax):
+    """rmax 12: cells of 12.5 / 13.3 nm; rmax 10 in the 50 nm box: L / rmax is
+    an integer, so the cell edge equals rmax up to rounding, with pairs placed
+    just under rmax across cell boundaries; rmax 30: beyond half the box."""
     sys_, xyz, types = _system(kind)
-    nbins, rmax = 60, 12.0
+    if rmax == 10.0:
+        # pairs just under rmax apart along each axis, straddling cell edges
+        ext = []
+        for a in range(3):
+            for c in (10.0, 20.0, 30.0):
+                p = np.array(sys_.lo, dtype=float) + 5.0
+                q = p.copy()
+                p[a] = sys_.lo[a] + c - 1e-7
+                q[a] = p[a] + 10.0 - 1e-6
+                ext += [p, q]
+        xyz = np.concatenate([xyz, np.array(ext)])
+        types = np.concatenate([types, np.zeros(len(ext), np.int32)])
     # two calls in a row, on different particles: the shared scratch keeps the
     # previous call's contents, which must not leak into the next result
     for shift in (0.0, 3.3):
