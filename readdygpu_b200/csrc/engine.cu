@@ -21,7 +21,11 @@ using namespace rdgpu;
 
 namespace {
 thread_local std::string g_create_error;
-constexpr int kStepBlock = 128;
+constexpr int kStepBlock = 128;    // cell-walk step kernel
+constexpr int kListBlock = 128;    // pair-list step kernel
+// FP32 pair-list steps spread each warp's listed pairs over its lanes
+// (list_step_kernel FLAT)
+constexpr bool kFlatPairs = false;
 // internal: do_steps_list stopped early so that do_steps re-tunes (never returned by the ABI)
 constexpr int RDGPU_OK_CONTINUE = 1;
 // hot particles (moved more than about skin/2 since the build) the list check
@@ -106,6 +110,16 @@ struct rdgpu_engine {
     int rdf_nbins = 0;
     double rdf_rmax = 0.0;
     long long rdf_frames = 0;
+    // RDF coarse grid (cells of edge >= rmax): grids per system, counting
+    // sort arrays, particles sorted by coarse cell
+    RdfGrid* rdf_grid_d = nullptr;
+    int rdf_grid_n = 0;
+    int* rdf_cnt = nullptr;
+    int* rdf_start = nullptr;
+    int* rdf_tsum = nullptr;
+    long long rdf_cells_cap = 0;
+    void* rdf_rec = nullptr;
+    long long rdf_rec_cap = 0;
     // neighbour search
     int nb_req = RDGPU_NB_AUTO;          // requested mode
     int nb_mode = RDGPU_NB_CELLS;        // mode in effect
@@ -757,18 +771,19 @@ template <class R> int add_conditional_chain(Engine* E, const Args<R>& a, const 
 
 template <class R> void launch_list_step_kernel(Engine* E, const Args<R>& a, const ListArgs<R>& v)
 {
-    const int grid = (int)((E->npart_tot + kStepBlock - 1) / kStepBlock);
+    const int grid = (int)((E->npart_tot + kListBlock - 1) / kListBlock);
     bool allper = true;
     for (int s = 0; s < E->nsys; ++s)
         for (int q = 0; q < 3; ++q) allper = allper && E->sys_h[s].per[q];
+    constexpr bool F = kFlatPairs && sizeof(R) == 4;
     if (E->hrep && allper)
-        list_step_kernel<R, true, true, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a, v);
+        list_step_kernel<R, true, true, kListBlock, F><<<grid, kListBlock, 0, E->stream>>>(a, v);
     else if (E->hrep)
-        list_step_kernel<R, true, false, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a, v);
+        list_step_kernel<R, true, false, kListBlock, F><<<grid, kListBlock, 0, E->stream>>>(a, v);
     else if (allper)
-        list_step_kernel<R, false, true, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a, v);
+        list_step_kernel<R, false, true, kListBlock, F><<<grid, kListBlock, 0, E->stream>>>(a, v);
     else
-        list_step_kernel<R, false, false, kStepBlock><<<grid, kStepBlock, 0, E->stream>>>(a, v);
+        list_step_kernel<R, false, false, kListBlock, F><<<grid, kListBlock, 0, E->stream>>>(a, v);
     ++E->launches;
 }
 
@@ -1724,12 +1739,108 @@ __global__ void rdf_norm_kernel(const unsigned long long* c, int S, int nbins, d
     g[i] = denom > 0 ? (double)c[i] / denom : 0.0;
 }
 
-template <class R> int rdf_impl(Engine* E, int nbins, double rmax, int accumulate, unsigned long long* out, long long* frames)
+// The RDF frame on the simulation's own cell grid (rdf_kernel): for boxes
+// whose coarse grid would have fewer than 3 cells along a periodic axis.
+template <class R> int rdf_fine(Engine* E, int nbins, double rmax)
 {
     const int S = E->desc.n_types;
     const int H = S * S * nbins;
     int rc = fresh_cells<R>(E);
     if (rc) return rc;
+    // the block's histogram and the bin edges in shared memory when they fit
+    const size_t smem = (size_t)((H + 1) & ~1) * 4 + (size_t)(nbins + 1) * 8;
+    const int use_smem = smem <= 48 * 1024 ? 1 : 0;
+    // one particle per thread: the per-particle work varies little
+    const int grid = (int)((E->npart_tot + 127) / 128);
+    rdf_kernel<R><<<grid, 128, use_smem ? smem : 0, E->stream>>>(
+        E->sys_d, E->sys_of, E->npart_tot, cur_state<R>(E), E->start, S, nbins, E->rdf_e2,
+        rmax / (double)nbins, use_smem, E->rdf_tmp);
+    CK(cudaGetLastError());
+    return RDGPU_OK;
+}
+
+// The RDF frame on a coarse grid of cells of edge >= rmax (rdf_tile_kernel),
+// from the current state in any order (no re-sort of the simulation's cells).
+// Returns RDGPU_OK_CONTINUE when some system's grid has fewer than 3 cells
+// along a periodic axis (rdf_fine then takes the frame).
+template <class R> int rdf_tiled(Engine* E, int nbins, double rmax)
+{
+    const int S = E->desc.n_types;
+    const int H = S * S * nbins;
+    std::vector<RdfGrid> gh(E->nsys);
+    long long nc = 0;
+    double lmax = 0.0;
+    for (int s = 0; s < E->nsys; ++s) {
+        RdfGrid& g = gh[s];
+        memset(&g, 0, sizeof(g));
+        long long m = 1;
+        for (int a = 0; a < 3; ++a) {
+            const double Lp = edge(E, s, a);
+            const int n = std::min(cells_along(Lp, rmax), 256);
+            if (E->sys_h[s].per[a] && n < 3) return RDGPU_OK_CONTINUE;
+            g.n[a] = n;
+            g.per[a] = E->sys_h[s].per[a];
+            g.L[a] = Lp;
+            g.invc[a] = (double)n / Lp;
+            lmax = std::max(lmax, Lp);
+            m *= n;
+        }
+        g.base = nc;
+        nc += m;
+    }
+    if (nc >= (1LL << 27)) return RDGPU_OK_CONTINUE;
+    const long long N = E->npart_tot;
+    const size_t recsz = sizeof(RdfRec<R>);
+    if (E->rdf_grid_n < E->nsys) {
+        dfree(E->rdf_grid_d);
+        CK(cudaMalloc(&E->rdf_grid_d, E->nsys * sizeof(RdfGrid)));
+        E->rdf_grid_n = E->nsys;
+    }
+    const int ntiles = (int)((nc + SCAN_TILE - 1) / SCAN_TILE);
+    if (nc > E->rdf_cells_cap) {
+        dfree(E->rdf_cnt); dfree(E->rdf_start); dfree(E->rdf_tsum);
+        CK(cudaMalloc(&E->rdf_cnt, nc * sizeof(int)));
+        CK(cudaMalloc(&E->rdf_start, (nc + 1) * sizeof(int)));
+        CK(cudaMalloc(&E->rdf_tsum, std::max(ntiles, 1) * sizeof(int)));
+        E->rdf_cells_cap = nc;
+    }
+    if (N * (long long)recsz > E->rdf_rec_cap) {
+        dfree(E->rdf_rec);
+        CK(cudaMalloc(&E->rdf_rec, E->cap_particles * recsz));
+        E->rdf_rec_cap = E->cap_particles * (long long)recsz;
+    }
+    CK(cudaMemcpyAsync(E->rdf_grid_d, gh.data(), E->nsys * sizeof(RdfGrid), cudaMemcpyHostToDevice, E->stream));
+    CK(cudaMemsetAsync(E->rdf_cnt, 0, nc * sizeof(int), E->stream));
+    const State<R> cur = cur_state<R>(E);
+    RdfRec<R>* rec = (RdfRec<R>*)E->rdf_rec;
+    // tcell / tslot are staging arrays of a step's sort, free between steps
+    rdf_count_kernel<R><<<grid_for(N), 256, 0, E->stream>>>(E->sys_of, N, cur, E->rdf_grid_d, E->tcell, E->tslot,
+                                                            E->rdf_cnt);
+    scan_tiles_kernel<<<ntiles, SCAN_BLOCK, 0, E->stream>>>(E->rdf_cnt, nc, E->rdf_tsum, E->err, nullptr);
+    scan_apply_kernel<<<ntiles, SCAN_BLOCK, 0, E->stream>>>(E->rdf_cnt, nc, E->rdf_tsum, ntiles, E->rdf_start,
+                                                            E->err, nullptr);
+    rdf_scatter_kernel<R><<<grid_for(N), 256, 0, E->stream>>>(N, cur, E->tcell, E->tslot, E->rdf_start, rec);
+    // FP32 pre-selection radius: rmax widened by the FP32 rounding of the
+    // coordinates (within a box length of the box) and of the distance
+    const double rpre = rmax + 64.0 * std::ldexp(1.0, -24) * lmax;
+    const float r2pre = (float)(rpre * rpre * (1.0 + 1e-5));
+    const size_t dyn = (size_t)(nbins + 1) * 8 + (size_t)H * 4;
+    const int use_smem = dyn <= 40 * 1024 ? 1 : 0;
+    const size_t smem = use_smem ? dyn : (size_t)(nbins + 1) * 8;
+    if (smem > 40 * 1024) return RDGPU_OK_CONTINUE;
+    const int grid = (int)std::min<long long>((nc + RDF_WARPS - 1) / RDF_WARPS, 148LL * 8);
+    rdf_tile_kernel<R><<<grid, RDF_WARPS * 32, smem, E->stream>>>(E->rdf_grid_d, E->nsys, nc, E->rdf_start, rec, S,
+                                                                  nbins, E->rdf_e2, rmax / (double)nbins, r2pre,
+                                                                  use_smem, E->rdf_tmp);
+    CK(cudaGetLastError());
+    return RDGPU_OK;
+}
+
+template <class R> int rdf_impl(Engine* E, int nbins, double rmax, int accumulate, unsigned long long* out, long long* frames)
+{
+    const int S = E->desc.n_types;
+    const int H = S * S * nbins;
+    int rc = RDGPU_OK;
     if (E->rdf_nbins != nbins || E->rdf_rmax != rmax) {
         dfree(E->rdf_acc); dfree(E->rdf_tmp); dfree(E->rdf_e2);
         CK(cudaMalloc(&E->rdf_acc, H * sizeof(unsigned long long)));
@@ -1746,16 +1857,14 @@ template <class R> int rdf_impl(Engine* E, int nbins, double rmax, int accumulat
         E->rdf_frames = 0;
     }
     CK(cudaMemsetAsync(E->rdf_tmp, 0, H * sizeof(unsigned long long), E->stream));
-    // the block's histogram and the bin edges in shared memory when they fit
-    const size_t smem = (size_t)((H + 1) & ~1) * 4 + (size_t)(nbins + 1) * 8;
-    const int use_smem = smem <= 48 * 1024 ? 1 : 0;
     if (E->npart_tot > 0) {
-        // one particle per thread: the per-particle work varies little
-        const int grid = (int)((E->npart_tot + 127) / 128);
-        rdf_kernel<R><<<grid, 128, use_smem ? smem : 0, E->stream>>>(
-            E->sys_d, E->sys_of, E->npart_tot, cur_state<R>(E), E->start, S, nbins, E->rdf_e2,
-            rmax / (double)nbins, use_smem, E->rdf_tmp);
-        CK(cudaGetLastError());
+        rc = rdf_tiled<R>(E, nbins, rmax);
+        if (rc != RDGPU_OK_CONTINUE) {
+            if (rc) return rc;
+        } else {
+            rc = rdf_fine<R>(E, nbins, rmax);
+            if (rc) return rc;
+        }
     }
     if (accumulate) {
         add_u64_kernel<<<(H + 255) / 256, 256, 0, E->stream>>>(E->rdf_acc, E->rdf_tmp, H);
@@ -1932,6 +2041,7 @@ int rdgpu_destroy(rdgpu_handle h)
     dfree(E->err); dfree(E->err_step); dfree(E->step_d); dfree(E->ctl); dfree(E->rl2_d);
     if (E->pinned_ctl) cudaFreeHost(E->pinned_ctl);
     dfree(E->red_d); dfree(E->redc_d); dfree(E->part_d); dfree(E->pcnt_d); dfree(E->ed_buf); dfree(E->off_d); dfree(E->rdf_acc); dfree(E->rdf_tmp); dfree(E->rdf_e2);
+    dfree(E->rdf_grid_d); dfree(E->rdf_cnt); dfree(E->rdf_start); dfree(E->rdf_tsum); dfree(E->rdf_rec);
     if (E->pinned_err) cudaFreeHost(E->pinned_err);
     if (E->pinned_step) cudaFreeHost(E->pinned_step);
     if (E->stream) cudaStreamDestroy(E->stream);

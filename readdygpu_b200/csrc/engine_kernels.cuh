@@ -26,6 +26,7 @@
 // (lib/ReaDDyGPU_Cpp/CudaKernels/CudaSimulation.cu:1034-1236, 1402-1782,
 // 1838-1919).
 #pragma once
+#include <type_traits>
 #include "engine_device.cuh"
 
 namespace rdgpu {
@@ -565,7 +566,7 @@ __global__ void inv_kernel(State<R> cur, long long ntot, int* __restrict__ inv)
 }
 
 template <class R, bool VALUE_IMAGE, bool HREP, int BLOCK>
-__global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) step_kernel(Args<R> a)
+__global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? 1024 : 768) / BLOCK) step_kernel(Args<R> a)
 {
     __shared__ R s_rc2[MAXT * MAXT];
     __shared__ R s_rmax2[MAXT];
@@ -1201,6 +1202,269 @@ __global__ void __launch_bounds__(128, 8) rdf_kernel(const SysDev* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
+// RDF on a coarse grid (rdf_tile_kernel and its counting sort).  The grid has
+// cells of edge >= rmax and at least 3 cells along every periodic axis, so
+// every pair closer than rmax sits in one cell or in two neighbouring ones,
+// and each unordered pair of neighbouring cells appears once among a cell's
+// 13 forward neighbours.  A warp takes the particles of one cell 32 at a time
+// (one per lane); the particles of each forward neighbour (and of the cell
+// itself, partners of higher index only) pass through a per-warp shared-memory
+// tile and are tested against all 32 lanes with an FP32 distance that
+// over-accepts (r2pre covers its rounding).  Accepted pairs queue in shared
+// memory and are evaluated 32 at a time, one per lane, with the exact FP64
+// predicate and bin rule of rdf_kernel: dx = (xi - xj) - sx, sx the periodic
+// shift of the neighbour cell, which is the symmetric minimum image
+// (mimg_sym) for every pair closer than rmax < L/2.  Each pair is counted
+// for both orientations, as in rdf_kernel.
+// ---------------------------------------------------------------------------
+struct RdfGrid {
+    int n[3];
+    int per[3];
+    long long base;      // first coarse cell of the system
+    double L[3];         // the engine's period per axis
+    double invc[3];      // n / L
+};
+
+template <class R> struct RdfRec;
+template <> struct RdfRec<float> { float4 p; };                                   // x, y, z, bits(type)
+template <> struct __align__(32) RdfRec<double> { double x, y, z; int t, pad; };
+
+template <class R>
+__device__ __forceinline__ long long rdf_cell_of(const RdfGrid& g, const R x[3])
+{
+    int c[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double q = floor((double)x[a] * g.invc[a]);
+        c[a] = q < 0.0 ? 0 : (q >= (double)g.n[a] ? g.n[a] - 1 : (int)q);
+    }
+    return g.base + ((long long)c[2] * g.n[1] + c[1]) * g.n[0] + c[0];
+}
+
+template <class R>
+__global__ void rdf_count_kernel(const unsigned short* __restrict__ sys_of, long long ntot, State<R> cur,
+                                 const RdfGrid* __restrict__ grids, int* __restrict__ tcell, int* __restrict__ tslot,
+                                 int* __restrict__ counts)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ntot;
+         i += (long long)gridDim.x * blockDim.x) {
+        R x[3];
+        int w;
+        load_pos(cur, i, x, w);
+        const long long c = rdf_cell_of(grids[sys_of[i]], x);
+        tslot[i] = atomicAdd(counts + c, 1);
+        tcell[i] = (int)c;
+    }
+}
+
+template <class R>
+__global__ void rdf_scatter_kernel(long long ntot, State<R> cur, const int* __restrict__ tcell,
+                                   const int* __restrict__ tslot, const int* __restrict__ start,
+                                   RdfRec<R>* __restrict__ rec)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < ntot;
+         i += (long long)gridDim.x * blockDim.x) {
+        R x[3];
+        int w;
+        load_pos(cur, i, x, w);
+        const long long d = start[tcell[i]] + tslot[i];
+        RdfRec<R> r;
+        if constexpr (sizeof(R) == 4) {
+            r.p = make_float4(x[0], x[1], x[2], __int_as_float(w & 0xff));
+        } else {
+            r.x = x[0]; r.y = x[1]; r.z = x[2]; r.t = w & 0xff; r.pad = 0;
+        }
+        rec[d] = r;
+    }
+}
+
+// forward neighbours (dx, dy, dz) of a cell; entry 0 is the cell itself
+__constant__ signed char c_rdf_nb[14][3] = {
+    {0, 0, 0},  {1, 0, 0},  {-1, 1, 0}, {0, 1, 0},  {1, 1, 0},
+    {-1, -1, 1}, {0, -1, 1}, {1, -1, 1}, {-1, 0, 1}, {0, 0, 1}, {1, 0, 1},
+    {-1, 1, 1}, {0, 1, 1},  {1, 1, 1}};
+
+constexpr int RDF_WARPS = 4;
+
+template <class R>
+__device__ __forceinline__ void rdf_exact(const double* __restrict__ ox, const int* __restrict__ ot,
+                                          const RdfRec<R>* __restrict__ rec, int2 e, const RdfGrid& g, int S,
+                                          int nbins, double rmax2, float inv_wf, const double* __restrict__ e2s,
+                                          int use_smem, unsigned* __restrict__ sh, unsigned long long* __restrict__ hist)
+{
+    const int o = e.y & 31, code = e.y >> 5;
+    double xj[3];
+    int tj;
+    if constexpr (sizeof(R) == 4) {
+        const float4 p = __ldg(&rec[e.x].p);
+        xj[0] = p.x; xj[1] = p.y; xj[2] = p.z;
+        tj = __float_as_int(p.w);
+    } else {
+        const RdfRec<double> q = rec[e.x];
+        xj[0] = q.x; xj[1] = q.y; xj[2] = q.z;
+        tj = q.t;
+    }
+    double d[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int sc = (code >> (2 * a)) & 3;
+        const double sx = sc == 1 ? g.L[a] : (sc == 2 ? -g.L[a] : 0.0);
+        d[a] = sub_rn(sub_rn(ox[3 * o + a], xj[a]), sx);
+    }
+    const double r2 = dist2(d[0], d[1], d[2]);
+    if (!(r2 < rmax2)) return;
+    const float r2f = (float)r2;
+    int k = r2f > 0.0f ? (int)(r2f * rsqrtf(r2f) * inv_wf) : 0;
+    k = min(max(k, 0), nbins - 1);
+    while (k > 0 && e2s[k] > r2) --k;
+    while (k < nbins - 1 && e2s[k + 1] <= r2) ++k;
+    const int ti = ot[o];
+    const int h1 = (ti * S + tj) * nbins + k, h2 = (tj * S + ti) * nbins + k;
+    if (use_smem) {
+        if (h1 == h2) atomicAdd(sh + h1, 2u);
+        else { atomicAdd(sh + h1, 1u); atomicAdd(sh + h2, 1u); }
+    } else {
+        if (h1 == h2) atomicAdd(hist + h1, 2ull);
+        else { atomicAdd(hist + h1, 1ull); atomicAdd(hist + h2, 1ull); }
+    }
+}
+
+template <class R>
+__global__ void __launch_bounds__(RDF_WARPS * 32) rdf_tile_kernel(const RdfGrid* __restrict__ grids, int nsys,
+        long long ncells, const int* __restrict__ start, const RdfRec<R>* __restrict__ rec, int S, int nbins,
+        const double* __restrict__ e2, double w, float r2pre, int use_smem, unsigned long long* __restrict__ hist)
+{
+    // shared memory: per warp a tile of 32 candidates, 64 queued pairs and
+    // the 32 lanes' own positions and types; then the squared bin edges and,
+    // with use_smem, the block's histogram
+    __shared__ float4 s_tile[RDF_WARPS][32];
+    __shared__ int2 s_queue[RDF_WARPS][64];
+    __shared__ double s_own[RDF_WARPS][96];
+    __shared__ int s_ot[RDF_WARPS][32];
+    extern __shared__ double s_dyn[];
+    double* e2s = s_dyn;
+    unsigned* sh = reinterpret_cast<unsigned*>(s_dyn + nbins + 1);
+    const int H = S * S * nbins;
+    for (int k = threadIdx.x; k <= nbins; k += blockDim.x) e2s[k] = e2[k];
+    if (use_smem)
+        for (int k = threadIdx.x; k < H; k += blockDim.x) sh[k] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+    float4* tile = s_tile[wp];
+    int2* queue = s_queue[wp];
+    double* ox = s_own[wp];
+    int* ot = s_ot[wp];
+    const double rmax2 = e2[nbins];
+    const float inv_wf = (float)(1.0 / w);
+    const unsigned lt = (1u << lane) - 1u;
+    for (long long c = (long long)blockIdx.x * RDF_WARPS + wp; c < ncells; c += (long long)gridDim.x * RDF_WARPS) {
+        const int a0 = start[c], a1 = start[c + 1];
+        if (a0 == a1) continue;
+        // the system of cell c: the last grid whose base is <= c
+        int lo = 0, hi = nsys - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (grids[mid].base <= c) lo = mid; else hi = mid - 1;
+        }
+        const RdfGrid& g = grids[lo];
+        const long long lc = c - g.base;
+        const int cc[3] = {(int)(lc % g.n[0]), (int)((lc / g.n[0]) % g.n[1]), (int)(lc / ((long long)g.n[0] * g.n[1]))};
+        for (int ob = a0; ob < a1; ob += 32) {
+            const int i = ob + lane;
+            const bool own = i < a1;
+            float xf[3] = {0.f, 0.f, 0.f};
+            if (own) {
+                double xd[3];
+                int t;
+                if constexpr (sizeof(R) == 4) {
+                    const float4 p = __ldg(&rec[i].p);
+                    xd[0] = p.x; xd[1] = p.y; xd[2] = p.z;
+                    t = __float_as_int(p.w);
+                } else {
+                    const RdfRec<double> q = rec[i];
+                    xd[0] = q.x; xd[1] = q.y; xd[2] = q.z;
+                    t = q.t;
+                }
+#pragma unroll
+                for (int a = 0; a < 3; ++a) { ox[3 * lane + a] = xd[a]; xf[a] = (float)xd[a]; }
+                ot[lane] = t;
+            }
+            int qn = 0;
+            for (int nb = 0; nb < 14; ++nb) {
+                int q[3];
+                int code = 0;
+                float sxf[3];
+                bool skip = false;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    q[a] = cc[a] + c_rdf_nb[nb][a];
+                    sxf[a] = 0.f;
+                    if (q[a] < 0) {
+                        if (!g.per[a]) skip = true;
+                        q[a] += g.n[a];
+                        sxf[a] = -(float)g.L[a];
+                        code |= 2 << (2 * a);
+                    } else if (q[a] >= g.n[a]) {
+                        if (!g.per[a]) skip = true;
+                        q[a] -= g.n[a];
+                        sxf[a] = (float)g.L[a];
+                        code |= 1 << (2 * a);
+                    }
+                }
+                if (skip) continue;
+                const long long nc = g.base + ((long long)q[2] * g.n[1] + q[1]) * g.n[0] + q[0];
+                const int b0 = nb == 0 ? a0 : start[nc], b1 = nb == 0 ? a1 : start[nc + 1];
+                for (int tb = b0; tb < b1; tb += 32) {
+                    const int m = min(32, b1 - tb);
+                    __syncwarp();
+                    if (lane < m) {
+                        if constexpr (sizeof(R) == 4) {
+                            tile[lane] = __ldg(&rec[tb + lane].p);
+                        } else {
+                            const RdfRec<double> r = rec[tb + lane];
+                            tile[lane] = make_float4((float)r.x, (float)r.y, (float)r.z, 0.f);
+                        }
+                    }
+                    __syncwarp();
+                    for (int k = 0; k < m; ++k) {
+                        const float4 p = tile[k];
+                        const float dx = (xf[0] - p.x) - sxf[0];
+                        const float dy = (xf[1] - p.y) - sxf[1];
+                        const float dz = (xf[2] - p.z) - sxf[2];
+                        const float r2f = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                        const bool acc = own && r2f < r2pre && (nb != 0 || tb + k > i);
+                        const unsigned bal = __ballot_sync(FULL, acc);
+                        if (bal) {
+                            if (acc) queue[qn + __popc(bal & lt)] = make_int2(tb + k, lane | (code << 5));
+                            qn += __popc(bal);
+                            if (qn >= 32) {
+                                __syncwarp();
+                                rdf_exact<R>(ox, ot, rec, queue[lane], g, S, nbins, rmax2, inv_wf, e2s, use_smem, sh,
+                                             hist);
+                                __syncwarp();
+                                if (lane < qn - 32) queue[lane] = queue[32 + lane];
+                                qn -= 32;
+                                __syncwarp();
+                            }
+                        }
+                    }
+                }
+            }
+            // what is left in the queue
+            __syncwarp();
+            if (lane < qn)
+                rdf_exact<R>(ox, ot, rec, queue[lane], g, S, nbins, rmax2, inv_wf, e2s, use_smem, sh, hist);
+            __syncwarp();
+        }
+    }
+    if (use_smem) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < H; k += blockDim.x)
+            if (sh[k]) atomicAdd(hist + k, (unsigned long long)sh[k]);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // MSD: squared unwrapped displacement per particle (FP64)
 // ---------------------------------------------------------------------------
 template <class R>
@@ -1381,13 +1645,135 @@ __device__ __forceinline__ void store_state(const State<double>& st, long long i
     st.rec[i] = r;
 }
 
-// one BD step of every particle over its pair list; ALLPER: every axis of
-// every system is periodic (the minimum image needs no per-axis test)
-template <class R, bool HREP, bool ALLPER, int BLOCK>
-__global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) list_step_kernel(Args<R> a, ListArgs<R> v)
+// The listed pairs of a warp's 32 particles spread over its 32 lanes (FP32).
+// Each lane's list goes to shared memory as (partner, owner lane) entries at
+// its place in the warp's concatenated lists, and the lanes then take the
+// entries 32 at a time, so the warp runs about (sum of the list lengths) / 32
+// pair evaluations rather than 32 times the longest list.  The owner's
+// operands come from shared memory; each pair term is converted to 2^-32
+// fixed point and added to the owner's sums with a shared-memory atomic, the
+// same integers the per-particle loop adds, so the sums are the same bit for
+// bit in any order.
+constexpr int FLAT_CAP = 256;    // entries per warp and round
+
+struct FlatWarpF {
+    float4 x[32];                    // the owner lane's position, bits(type)
+    float4 il[32];                   // 1/L per axis (0 on open axes), L_x
+    float2 l[32];                    // L_y, L_z
+    unsigned long long acc[3][32];   // 2^-32 fixed-point force sums
+    int2 pr[FLAT_CAP];               // (partner's sorted index, owner lane)
+};
+struct FlatNone {};
+
+__device__ __forceinline__ void flat_add(FlatWarpF& fw, int o, float pre, float dx, float dy, float dz)
 {
+    const float q = -pre * FX_SCALE;
+    atomicAdd(&fw.acc[0][o], (unsigned long long)__float2ll_rn(q * dx));
+    atomicAdd(&fw.acc[1][o], (unsigned long long)__float2ll_rn(q * dy));
+    atomicAdd(&fw.acc[2][o], (unsigned long long)__float2ll_rn(q * dz));
+}
+
+template <bool HREP>
+__device__ __forceinline__ void flat_pair(FlatWarpF& fw, int2 e, const float xj[3], int wj, const float* s_rc2,
+                                          const FastTab<float>& ft, const TypeTab<float>* tab)
+{
+    const float4 ox = fw.x[e.y], il4 = fw.il[e.y];
+    const float2 l2 = fw.l[e.y];
+    PairFrame pf;
+    pf.xy = f2_pack(ox.x, ox.y);
+    pf.il_xy = f2_pack(il4.x, il4.y);
+    pf.l_xy = f2_pack(il4.w, l2.x);
+    pf.z = ox.z;
+    pf.il_z = il4.z;
+    pf.l_z = l2.y;
+    float dx, dy, dz, r2;
+    pair_disp_x2(pf, xj[0], xj[1], xj[2], dx, dy, dz, r2);
+    const int pidx = __float_as_int(ox.w) * MAXT + (wj & 0xff);
+    if (!(r2 < s_rc2[pidx])) return;
+    if (HREP) {
+        // pre = k (r - r0) / r; r == 0 has no direction
+        if (r2 > 0.0f) flat_add(fw, e.y, ft.k[pidx] * (1.0f - ft.r0[pidx] * rsqrtf(r2)), dx, dy, dz);
+    } else {
+        const float r = sqrtf(r2);
+        const int nt = tab->nterm[pidx];
+        for (int m = 0; m < nt; ++m) {
+            float pre, en;
+            pair_term(tab->term[pidx * MAX_TERMS + m], r, pre, en);
+            flat_add(fw, e.y, pre, dx, dy, dz);
+        }
+    }
+}
+
+template <bool HREP>
+__device__ __forceinline__ void flat_pairs(FlatWarpF& fw, const State<float>& cur, const ListArgs<float>& v,
+                                           const float* s_rc2, const FastTab<float>& ft, const TypeTab<float>* tab,
+                                           int lane, int i, const float xi[3], int ti, const SysDev& s, int cnt,
+                                           const int4& q0, const int4& q1, Acc<float>& acc)
+{
+    // place of this lane's list in the warp's concatenated lists
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += t;
+    }
+    const int pre = incl - cnt;
+    const int P = __shfl_sync(FULL, incl, 31);
+    if (P == 0) return;
+    fw.x[lane] = make_float4(xi[0], xi[1], xi[2], __int_as_float(ti));
+    fw.il[lane] = make_float4(s.ilf[0], s.ilf[1], s.ilf[2], s.Lf[0]);
+    fw.l[lane] = make_float2(s.Lf[1], s.Lf[2]);
+    fw.acc[0][lane] = 0ull;
+    fw.acc[1][lane] = 0ull;
+    fw.acc[2][lane] = 0ull;
+    const int4* nb4 = reinterpret_cast<const int4*>(v.nbr) + i;
+    for (int base = 0; base < P; base += FLAT_CAP) {
+        // this lane's entries that fall into [base, base + FLAT_CAP)
+        const int k0 = max(0, base - pre), k1 = min(cnt, base + FLAT_CAP - pre);
+        for (int k = k0; k < k1; ++k) {
+            int j;
+            if (k < 8) {
+                const int4 q = k < 4 ? q0 : q1;
+                const int u = k & 3;
+                j = u == 0 ? q.x : (u == 1 ? q.y : (u == 2 ? q.z : q.w));
+            } else {
+                j = __ldg(reinterpret_cast<const int*>(nb4 + (long long)(k >> 2) * v.stride) + (k & 3));
+            }
+            fw.pr[pre + k - base] = make_int2(j, lane);
+        }
+        __syncwarp();
+        const int m = min(P - base, FLAT_CAP);
+        // two entries per lane and trip: both partner positions requested
+        // before either pair is evaluated
+        for (int s0 = lane; s0 < m; s0 += 64) {
+            const int s1 = s0 + 32;
+            const bool two = s1 < m;
+            const int2 e0 = fw.pr[s0];
+            const int2 e1 = two ? fw.pr[s1] : e0;
+            float x0[3], x1[3];
+            int w0, w1;
+            load_pos(cur, e0.x, x0, w0);
+            load_pos(cur, e1.x, x1, w1);
+            flat_pair<HREP>(fw, e0, x0, w0, s_rc2, ft, tab);
+            if (two) flat_pair<HREP>(fw, e1, x1, w1, s_rc2, ft, tab);
+        }
+        __syncwarp();
+    }
+    acc.fx = (long long)fw.acc[0][lane];
+    acc.fy = (long long)fw.acc[1][lane];
+    acc.fz = (long long)fw.acc[2][lane];
+}
+
+// one BD step of every particle over its pair list; ALLPER: every axis of
+// every system is periodic (the minimum image needs no per-axis test); FLAT
+// (FP32 only): the warp's listed pairs spread over its lanes (flat_pairs)
+template <class R, bool HREP, bool ALLPER, int BLOCK, bool FLAT = false>
+__global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? 1024 : 768) / BLOCK) list_step_kernel(Args<R> a, ListArgs<R> v)
+{
+    static_assert(!FLAT || sizeof(R) == 4, "the flat pair phase is FP32 only");
     __shared__ R s_rc2[MAXT * MAXT];
     __shared__ FastTab<R> s_ft;
+    __shared__ std::conditional_t<FLAT, FlatWarpF, FlatNone> s_flat[FLAT ? BLOCK / 32 : 1];
     if (*((volatile int*)a.err)) return;   // an earlier step failed: keep its input intact
     // rows of the S types in use (entries (ti, tj) with ti >= S are never read)
     for (int k = threadIdx.x; k < MAXT * a.tab->S; k += BLOCK) {
@@ -1402,8 +1788,12 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) list_step_kerne
     const int sel = list_sel(a, v, a.step_off);
     const State<R> cur = sel ? v.b1 : v.b0;
     const State<R> nxt = sel ? v.b0 : v.b1;
-    const int i = blockIdx.x * BLOCK + threadIdx.x;
-    if (i >= a.ntot) return;
+    const int i0 = blockIdx.x * BLOCK + threadIdx.x;
+    // the flat pair phase needs every lane of the warp: lanes past the last
+    // particle take part with an empty list and store nothing
+    const bool valid = i0 < a.ntot;
+    if (!FLAT && !valid) return;
+    const int i = valid ? i0 : (int)a.ntot - 1;
     const int si = a.sys_of[i];
     const SysDev& s = a.sys[si];
     R xi[3];
@@ -1425,7 +1815,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) list_step_kerne
     Acc<R> acc;
     acc.zero();
     const float4 xr = __ldg(v.xref + i);
-    const int cnt = __float_as_int(xr.w);
+    const int cnt = valid ? __float_as_int(xr.w) : 0;
     // the first 8 list entries (capacity >= 8) are requested together with
     // the particle's own state, before its list length is known; entries
     // past the length are never used
@@ -1435,10 +1825,14 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) list_step_kerne
     double il[3] = {0.0, 0.0, 0.0};
     if constexpr (sizeof(R) == 4) pf.load(s, xi);
     else { il[0] = s.il[0]; il[1] = s.il[1]; il[2] = s.il[2]; }
+    if constexpr (FLAT) {
+        flat_pairs<HREP>(s_flat[threadIdx.x >> 5], cur, v, s_rc2, s_ft, a.tab, threadIdx.x & 31, i, xi, ti, s, cnt,
+                         q0, q1, acc);
+    }
     // the partners in groups of 4: all their positions are requested before
     // the first pair is evaluated
     constexpr int LCHUNK = 4;
-    for (int k0 = 0; k0 < cnt; k0 += LCHUNK) {
+    for (int k0 = 0; k0 < (FLAT ? 0 : cnt); k0 += LCHUNK) {
         const int4 q = k0 == 0 ? q0 : (k0 == 4 ? q1 : __ldg(nb4 + (long long)(k0 >> 2) * v.stride));
         int jj[LCHUNK] = {q.x, q.y, q.z, q.w};
 #pragma unroll
@@ -1506,8 +1900,8 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) list_step_kerne
     const float d1 = mimg((float)xi[1], xr.y, s.Lf[1], s.halff[1], p1);
     const float d2 = mimg((float)xi[2], xr.z, s.Lf[2], s.halff[2], p2);
     const float dd = d0 * d0 + d1 * d1 + d2 * d2;
-    if (dd > v.cap2) *((volatile int*)&v.ctl->need) = 1;
-    const bool hot = dd > v.thr2;
+    if (valid && dd > v.cap2) *((volatile int*)&v.ctl->need) = 1;
+    const bool hot = valid && dd > v.thr2;
     const unsigned act = __activemask();
     const unsigned hm = __ballot_sync(act, hot);
     if (hm) {
@@ -1518,6 +1912,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(R) == 4 ? 8 : 6) list_step_kerne
         base = __shfl_sync(act, base, lead) + __popc(hm & ((1u << lane) - 1u));
         if (hot && base < v.hot_max) v.hot[base] = i;
     }
+    if (!valid) return;
     store_state(nxt, i, xi, wi, c, id);
     if (ef) {
         atomicOr(a.err, ef);

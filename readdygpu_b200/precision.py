@@ -134,6 +134,125 @@ def trajectory(w, steps, frames=10, seed=1, **kw):
     }
 
 
+def _block_mean(v, blocks=10):
+    """Mean of a time series and its standard error from block averages."""
+    v = np.asarray(v, dtype=np.float64)
+    nb = max(2, min(blocks, len(v)))
+    parts = np.array_split(v, nb)
+    m = np.array([p.mean() for p in parts])
+    return float(v.mean()), float(m.std(ddof=1) / np.sqrt(nb))
+
+
+def long_run(w, steps, samples=100, seed=1, rdf_bins=150, rdf_rmax=15.0, equil=0.1, **kw):
+    """The long-run precision study: the FP32C and the FP64 engine stepped side
+    by side from the same positions with the same Philox keys, sampled every
+    steps / samples steps.  At each sample:
+
+    * potential energy of both runs;
+    * MSD per species from the unwrapped displacement since the start
+      (MsdComputer.java:114-213 takes the first-seen position as the origin),
+      with its standard error over particles;
+    * the force error of the FP32C engine against the FP64 engine on the FP32C
+      run's current positions (snapped to the FP32 grid);
+    * one RDF frame of each run (accumulated counts).
+
+    Statistical comparison (the two runs share the noise, so their
+    differences are far below these bounds while the trajectories stay close,
+    and the bounds hold after they decorrelate):
+
+    * energy: the means over the samples after the first `equil` fraction,
+      |E32 - E64| <= 3 sqrt(se32^2 + se64^2) (block standard errors);
+    * D = MSD / 6t per species at the first sample and at the end:
+      |D32 - D64| <= 3 sqrt(se32^2 + se64^2) (standard errors over
+      particles);
+    * RDF: per bin |c32 - c64| <= 3 sqrt(c32 + c64) + 1 (counting error).
+    """
+    x0 = snap_to_f32(w)
+    every = max(1, steps // samples)
+    S = w.system.n_types
+    eng = {}
+    for prec in ("f32c", "f64"):
+        eng[prec] = _engine(w, prec, seed, **kw)
+        eng[prec].set_particles(x0, w.types, offsets=w.offsets)
+        eng[prec].autotune()
+    probe = {prec: _engine(w, prec, seed) for prec in ("f32c", "f64")}
+    rec = {p: {"t": [], "E": [], "msd": [], "msd_se": []} for p in eng}
+    ferr = []
+    ufirst = {}
+    done = 0
+    rdf_counts = {}
+    try:
+        while done < steps:
+            n = min(every, steps - done)
+            for prec, e in eng.items():
+                e.step(n)
+            done += n
+            for prec, e in eng.items():
+                m = e.metrics()
+                xe, _ = e.get_particles()
+                if w.boxes is not None or any(w.system.periodic):
+                    # periodic axes: the engine's image-unwrapped MSD (no per-particle spread)
+                    msd = np.array(m["msd"][:S])
+                    se = np.zeros(S)
+                else:
+                    # an open box: positions are unwrapped as they are
+                    d2 = ((xe - x0) ** 2).sum(axis=1)
+                    msd = np.array([d2[w.types == t].mean() for t in range(S)])
+                    se = np.array([d2[w.types == t].std(ddof=1) / np.sqrt(max(1, (w.types == t).sum()))
+                                   for t in range(S)])
+                r = rec[prec]
+                r["t"].append(done); r["E"].append(m["energy"]); r["msd"].append(msd); r["msd_se"].append(se)
+                c, _ = e.rdf(rdf_bins, rdf_rmax, accumulate=True)
+                rdf_counts[prec] = c
+                if prec == "f32c":
+                    xs = xe
+            # force error on the FP32C run's current positions
+            F = {}
+            xsn = snap_to_f32(_with_xyz(w, xs))
+            for prec, e in probe.items():
+                e.set_particles(xsn, w.types, offsets=w.offsets)
+                F[prec], _ = e.forces()
+            nrm = np.linalg.norm(F["f64"])
+            ferr.append(float(np.linalg.norm(F["f32c"] - F["f64"]) / nrm) if nrm > 0 else 0.0)
+    finally:
+        for e in list(eng.values()) + list(probe.values()):
+            e.close()
+    dt = w.system.dt
+    out = {"steps": steps, "sample_every": every, "samples": len(ferr),
+           "force_rel_err_max": max(ferr), "force_rel_err_mean": float(np.mean(ferr))}
+    k0 = int(equil * len(ferr))
+    E = {}
+    for prec in eng:
+        E[prec] = _block_mean(rec[prec]["E"][k0:])
+        t = np.array(rec[prec]["t"], dtype=np.float64)
+        out[f"energy_mean_{prec}"], out[f"energy_se_{prec}"] = E[prec]
+        out[f"energy_drift_per_step_{prec}"] = float(np.polyfit(t[k0:], rec[prec]["E"][k0:], 1)[0])
+    dE = abs(E["f32c"][0] - E["f64"][0])
+    out["energy_abs_dev"] = dE
+    out["energy_bound_3sigma"] = 3.0 * float(np.hypot(E["f32c"][1], E["f64"][1]))
+    for tag, k in (("first", 0), ("end", len(ferr) - 1)):
+        T = rec["f64"]["t"][k] * dt
+        D = {p: np.array(rec[p]["msd"][k]) / (6.0 * T) for p in eng}
+        se = {p: np.array(rec[p]["msd_se"][k]) / (6.0 * T) for p in eng}
+        out[f"D_{tag}_f32c"] = [float(v) for v in D["f32c"]]
+        out[f"D_{tag}_f64"] = [float(v) for v in D["f64"]]
+        out[f"D_{tag}_abs_dev"] = [float(v) for v in np.abs(D["f32c"] - D["f64"])]
+        out[f"D_{tag}_bound_3sigma"] = [float(v) for v in 3.0 * np.hypot(se["f32c"], se["f64"])]
+        out[f"D_{tag}_rel_dev"] = [float(v) for v in np.abs(D["f32c"] - D["f64"]) / np.maximum(np.abs(D["f64"]), 1e-300)]
+    c32 = rdf_counts["f32c"].astype(np.float64).reshape(-1)
+    c64 = rdf_counts["f64"].astype(np.float64).reshape(-1)
+    out["rdf_bins"] = rdf_bins
+    out["rdf_rmax_nm"] = rdf_rmax
+    out["rdf_pairs_counted"] = float(c64.sum())
+    out["rdf_max_dev_over_bound"] = float(np.max(np.abs(c32 - c64) / (3.0 * np.sqrt(c32 + c64) + 1.0)))
+    return out
+
+
+def _with_xyz(w, xyz):
+    from .configs import Workload
+    return Workload(w.name, w.system, xyz, w.types, w.steps, boxes=w.boxes, offsets=w.offsets)
+
+
 def study(config, particles=None, steps=1000, frames=10, seed=1, **kw):
     from . import configs
     if config == 4:
@@ -159,7 +278,21 @@ def main():
     p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--frames", type=int, default=10)
     p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--long", action="store_true",
+                   help="the long-run study (long_run): both precisions side by side, --frames samples")
     a = p.parse_args()
+    if a.long:
+        from . import configs
+        if a.config == 5 and a.particles:
+            w = configs.config5(n=a.particles, n_shell=max(1, round(0.06 * a.particles)))
+        elif a.particles:
+            w = configs.CONFIGS[a.config](n=a.particles)
+        else:
+            w = configs.CONFIGS[a.config]()
+        out = {"workload": w.name, "particles": int(len(w.types))}
+        out.update(long_run(w, a.steps, a.frames, a.seed))
+        print(json.dumps(out), flush=True)
+        return
     print(json.dumps(study(a.config, a.particles or None, a.steps, a.frames, a.seed)), flush=True)
 
 

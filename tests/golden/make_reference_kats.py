@@ -3,7 +3,7 @@ reference_kats.json.
 
 Run here, where the reference sources are readable:
 
-    python tests/golden/make_reference_kats.py /root/reference
+    python tests/golden/make_reference_kats.py <path of the reference checkout>
 
 It reads (as text) these test methods and records every expected gradient,
 energy and displacement they assert, with the file:line of the assertion
@@ -137,7 +137,9 @@ def displacement(ref):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_reference_kats.py <path of the reference checkout>")
+    ref = sys.argv[1]
     single, pair = displacement(ref)
     out = {
         "source": "reference JUnit tests (assertEquals tolerance 1e-4)",

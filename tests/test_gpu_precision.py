@@ -56,3 +56,21 @@ def test_precision_study_config5():
     assert r["energy_max_rel_dev"] <= 1e-4, r
     assert r["D_max_rel_dev"] <= 1e-3, r
     assert r["position_max_dev_nm"] <= 1e-2, r
+
+
+def test_long_run_statistics_config5():
+    """The long-run study (precision.long_run) at reduced size: config 5's
+    vesicle with 20,000 particles, 20,000 steps, sampled every 1,000.  Bars:
+    force error <= 1e-5 at every sample; mean potential energy, D per species
+    (at the first sample and at the end) and every RDF bin of the FP32C run
+    within 3 standard errors of the FP64 run's."""
+    w = configs.config5(n=20000, n_shell=1200)
+    r = precision.long_run(w, steps=20000, samples=20)
+    assert r["samples"] == 20
+    assert r["force_rel_err_max"] <= 1e-5, r
+    assert r["energy_abs_dev"] <= r["energy_bound_3sigma"], r
+    for tag in ("first", "end"):
+        for dev, bound in zip(r[f"D_{tag}_abs_dev"], r[f"D_{tag}_bound_3sigma"]):
+            assert dev <= bound, (tag, r)
+    assert r["rdf_pairs_counted"] > 0
+    assert r["rdf_max_dev_over_bound"] <= 1.0, r
