@@ -160,7 +160,9 @@ typedef struct {
                                            energy evaluation, which adds one)          */
     double   skin;                      /* pair-list skin in effect [nm], 0: cells   */
     int32_t  list_capacity;             /* pair-list slots per particle              */
-    int32_t  reserved;
+    int32_t  list_entry_bytes;          /* 2: partners as 16-bit offsets, 4: as 32-bit
+                                           indices (an offset did not fit 16 bits);
+                                           0 with the cell walk                       */
 } rdgpu_metrics;
 
 typedef struct rdgpu_engine* rdgpu_handle;

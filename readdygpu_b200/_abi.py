@@ -82,7 +82,7 @@ class Metrics(C.Structure):
     _fields_ = [("energy", C.c_double), ("msd", C.c_double * MAX_TYPES),
                 ("count", C.c_int64 * MAX_TYPES), ("step", C.c_int64),
                 ("neighbour_mode", C.c_int32), ("list_builds", C.c_int32), ("skin", C.c_double),
-                ("list_capacity", C.c_int32), ("reserved", C.c_int32)]
+                ("list_capacity", C.c_int32), ("list_entry_bytes", C.c_int32)]
 
 
 # C-ABI functions and their signatures: (name, restype, argtypes)

@@ -23,9 +23,6 @@ namespace {
 thread_local std::string g_create_error;
 constexpr int kStepBlock = 128;    // cell-walk step kernel
 constexpr int kListBlock = 128;    // pair-list step kernel
-// FP32 pair-list steps spread each warp's listed pairs over its lanes
-// (list_step_kernel FLAT)
-constexpr bool kFlatPairs = false;
 // internal: do_steps_list stopped early so that do_steps re-tunes (never returned by the ABI)
 constexpr int RDGPU_OK_CONTINUE = 1;
 // hot particles (moved more than about skin/2 since the build) the list check
@@ -133,8 +130,9 @@ struct rdgpu_engine {
     ListCtl* ctl = nullptr;
     ListCtl* pinned_ctl = nullptr;
     int nbuild_h = 0;
-    int* nbr = nullptr;                  // pair lists, list_cap x list_stride (groups of 4 per particle)
-    float4* xref = nullptr;              // positions at the build and list lengths
+    int4* nbr = nullptr;                 // pair-list entry groups (narrow: 8 offsets, wide: 4 indices)
+    uint2* head = nullptr;               // list heads: build position on a 16-bit lattice, list length
+    bool list_wide = false;              // 32-bit entries (a partner's offset did not fit 16 bits)
     int* hot = nullptr;                  // particles that moved more than about skin/2 since the build
     cudaStream_t stream2 = nullptr;      // captures the re-sort into conditional graph nodes
     bool capturing = false;
@@ -349,7 +347,7 @@ void free_particles(Engine* E)
 {
     for (int b = 0; b < 2; ++b) { dfree(E->bufA[b]); dfree(E->bufB[b]); }
     dfree(E->tcell); dfree(E->tslot);
-    dfree(E->nbr); dfree(E->xref); dfree(E->hot);
+    dfree(E->nbr); dfree(E->head); dfree(E->hot);
     E->list_stride = 0;
     E->list_cap = 0;
     dfree(E->sys_of); dfree(E->x0_d); dfree(E->vec_d); dfree(E->val_d); dfree(E->ityp_d); dfree(E->u64_d);
@@ -619,6 +617,27 @@ int configure_cells(Engine* E, double cut, std::string& why)
 // ---------------------------------------------------------------------------
 // pair-list mode (list_step_kernel and the re-sort chain; see the kernels)
 // ---------------------------------------------------------------------------
+double largest_edge(const Engine* E)
+{
+    double lmax = 0.0;
+    for (int s = 0; s < E->nsys; ++s)
+        for (int a = 0; a < 3; ++a) lmax = std::max(lmax, E->sys_h[s].L[a]);
+    return lmax;
+}
+
+// the hot-particle threshold th: skin/2 less the FP32 rounding of positions
+// and squared distances
+double list_threshold(const Engine* E, double skin)
+{
+    return 0.5 * skin * (1.0 - 2e-3) - 4.0 * largest_edge(E) * std::ldexp(1.0, -20);
+}
+
+// error bound of the lattice estimate of a displacement (2 bins per axis)
+double list_lattice_error(const Engine* E)
+{
+    return std::sqrt(3.0) * 2.0 * largest_edge(E) * std::ldexp(1.0, -16) * (1.0 + 1e-3);
+}
+
 template <class R> ListArgs<R> make_list_args(Engine* E, bool with_list)
 {
     ListArgs<R> v;
@@ -627,41 +646,41 @@ template <class R> ListArgs<R> make_list_args(Engine* E, bool with_list)
     v.b1 = state<R>(E->bufA[1], E->bufB[1]);
     v.ctl = E->ctl;
     v.nbr = with_list ? E->nbr : nullptr;
-    v.xref = E->xref;
+    v.head = E->head;
     v.hot = E->hot;
     v.stride = E->list_stride;
     v.cap = E->list_cap;
+    v.narrow = E->list_wide ? 0 : 1;
     // list radius and displacement thresholds.  A pair missing from the list
     // that is closer than its cutoff at a later step has moved by more than
     // 2 th together, th being kept below skin/2 by a margin for the FP32
     // rounding of positions (a few ulp of the largest box edge) and of the
     // squared distances: one of the two moved more than th (list_check_kernel
     // looks at those).  Beyond 2 th the check's cell walk may miss partners,
-    // and the step kernel asks for a rebuild outright.
+    // and the step kernel asks for a rebuild outright.  The step kernel
+    // estimates a displacement on the 16-bit lattice of the list heads, to
+    // within dq = 2 bins per axis (head_disp2), so it compares the estimate
+    // with th - sqrt(3) dq and 2 th - sqrt(3) dq.
     v.rl2t = (const R*)E->rl2_d;
     const double rl = E->max_rc + E->skin;
     v.rl2max = (R)(rl * rl * (1.0 + 1e-6));
-    double lmax = 0.0;
-    for (int s = 0; s < E->nsys; ++s)
-        for (int a = 0; a < 3; ++a) lmax = std::max(lmax, E->sys_h[s].L[a]);
-    const double th = 0.5 * E->skin * (1.0 - 2e-3) - 4.0 * lmax * std::ldexp(1.0, -20);
-    v.thr2 = (float)(th > 0 ? th * th : 0.0);
-    v.cap2 = (float)(th > 0 ? 4.0 * th * th : 0.0);
+    const double th = list_threshold(E, E->skin);
+    const double dq = list_lattice_error(E);
+    v.thr2 = (float)(th - dq > 0 ? (th - dq) * (th - dq) : 0.0);
+    v.cap2 = (float)(th - dq > 0 ? (2.0 * th - dq) * (2.0 * th - dq) : 0.0);
     // checking a hot particle's neighbourhood costs about what rebuilding
     // the lists of a thousand particles does
     v.hot_max = (int)std::min<long long>(kHotMax, std::max<long long>(8, E->npart_tot / 1000));
     return v;
 }
 
-// the skin is usable: positive rebuild threshold and >= 3 cells of edge
-// >= rc_max + skin on every periodic axis of every system
+// the skin is usable: the hot-particle threshold keeps half of skin/2 after
+// its margins, and >= 3 cells of edge >= rc_max + skin on every periodic
+// axis of every system
 bool list_eligible(Engine* E, double skin)
 {
     if (!(skin > 0.0) || !(E->max_rc > 0.0)) return false;
-    double lmax = 0.0;
-    for (int s = 0; s < E->nsys; ++s)
-        for (int a = 0; a < 3; ++a) lmax = std::max(lmax, E->sys_h[s].L[a]);
-    if (0.5 * skin * (1.0 - 2e-3) - 4.0 * lmax * std::ldexp(1.0, -20) < 0.25 * skin) return false;
+    if (list_threshold(E, skin) - list_lattice_error(E) < 0.25 * skin) return false;
     const double cut = std::max(E->desc.cell_size, E->max_rc + skin);
     for (int s = 0; s < E->nsys; ++s)
         for (int a = 0; a < 3; ++a)
@@ -669,24 +688,29 @@ bool list_eligible(Engine* E, double skin)
     return true;
 }
 
-int ensure_list(Engine* E, int cap)
+// list storage for cap entries per particle (wide: 32-bit entries)
+int ensure_list(Engine* E, int cap, bool wide)
 {
     const long long stride = std::max<long long>(E->cap_particles, 1);
-    if (cap <= E->list_cap && stride == E->list_stride && E->nbr) return RDGPU_OK;
-    // groups of 4 entries (one int4), at least two of them: the step kernel
-    // requests the first 8 entries before it knows the list length
-    cap = (std::max(std::max(cap, E->list_cap), 8) + 3) & ~3;
+    if (cap <= E->list_cap && stride == E->list_stride && wide == E->list_wide && E->nbr) return RDGPU_OK;
+    // whole groups of 8 entries (one int4 narrow, two wide): the step kernel
+    // requests the first 8 entries before it knows the list length; at most
+    // 2^16 - 1 (the list head's count field)
+    cap = std::min((std::max(std::max(cap, E->list_cap), 8) + 7) & ~7, 65528);
     drop_graph_map(E->lgraphs);
-    dfree(E->nbr); dfree(E->xref); dfree(E->hot);
+    dfree(E->nbr); dfree(E->head); dfree(E->hot);
     E->list_cap = 0;
     E->list_stride = 0;
-    CK(cudaMalloc(&E->nbr, (size_t)cap * stride * sizeof(int)));
-    CK(cudaMalloc(&E->xref, stride * sizeof(float4)));
+    const long long groups = wide ? cap / 4 : cap / 8;
+    CK(cudaMalloc(&E->nbr, (size_t)groups * stride * sizeof(int4)));
+    CK(cudaMalloc(&E->head, stride * sizeof(uint2)));
     CK(cudaMalloc(&E->hot, kHotMax * sizeof(int)));
     E->list_cap = cap;
     E->list_stride = stride;
+    E->list_wide = wide;
     return RDGPU_OK;
 }
+
 
 // capacity after an overflowing build: twice the longest list met, so that a
 // system that keeps clustering (attractive interactions) overflows a few
@@ -695,6 +719,14 @@ int list_regrow_cap(Engine* E)
 {
     const long long c = 2LL * E->pinned_ctl->maxcnt + 8;
     return (int)std::min<long long>(c, 1 << 20);
+}
+
+// storage after a build that failed with flags ef (EF_LISTOVF: a list longer
+// than the capacity; EF_LISTWIDE: an offset beyond 16 bits)
+int ensure_list_after(Engine* E, int ef)
+{
+    const int cap = (ef & EF_LISTOVF) ? list_regrow_cap(E) : E->list_cap;
+    return ensure_list(E, cap, E->list_wide || (ef & EF_LISTWIDE) != 0);
 }
 
 // list capacity from the densest system, x2 for fluctuations and clusters
@@ -769,21 +801,29 @@ template <class R> int add_conditional_chain(Engine* E, const Args<R>& a, const 
     return RDGPU_OK;
 }
 
+template <class R, bool NARROW>
+void launch_list_step_kernel_w(Engine* E, const Args<R>& a, const ListArgs<R>& v, int grid, bool allper)
+{
+    if (E->hrep && allper)
+        list_step_kernel<R, true, true, kListBlock, NARROW><<<grid, kListBlock, 0, E->stream>>>(a, v);
+    else if (E->hrep)
+        list_step_kernel<R, true, false, kListBlock, NARROW><<<grid, kListBlock, 0, E->stream>>>(a, v);
+    else if (allper)
+        list_step_kernel<R, false, true, kListBlock, NARROW><<<grid, kListBlock, 0, E->stream>>>(a, v);
+    else
+        list_step_kernel<R, false, false, kListBlock, NARROW><<<grid, kListBlock, 0, E->stream>>>(a, v);
+}
+
 template <class R> void launch_list_step_kernel(Engine* E, const Args<R>& a, const ListArgs<R>& v)
 {
     const int grid = (int)((E->npart_tot + kListBlock - 1) / kListBlock);
     bool allper = true;
     for (int s = 0; s < E->nsys; ++s)
         for (int q = 0; q < 3; ++q) allper = allper && E->sys_h[s].per[q];
-    constexpr bool F = kFlatPairs && sizeof(R) == 4;
-    if (E->hrep && allper)
-        list_step_kernel<R, true, true, kListBlock, F><<<grid, kListBlock, 0, E->stream>>>(a, v);
-    else if (E->hrep)
-        list_step_kernel<R, true, false, kListBlock, F><<<grid, kListBlock, 0, E->stream>>>(a, v);
-    else if (allper)
-        list_step_kernel<R, false, true, kListBlock, F><<<grid, kListBlock, 0, E->stream>>>(a, v);
+    if (v.narrow)
+        launch_list_step_kernel_w<R, true>(E, a, v, grid, allper);
     else
-        list_step_kernel<R, false, false, kListBlock, F><<<grid, kListBlock, 0, E->stream>>>(a, v);
+        launch_list_step_kernel_w<R, false>(E, a, v, grid, allper);
     ++E->launches;
 }
 
@@ -856,9 +896,9 @@ template <class R> int resort(Engine* E, bool with_list)
             set_cur(E, E->cur ^ 1);
             return reset_counters(E, E->step_h);
         }
-        if (ef != EF_LISTOVF) return fail(E, RDGPU_ERR_CUDA, "re-sort failed");
+        if (ef & ~(EF_LISTOVF | EF_LISTWIDE)) return fail(E, RDGPU_ERR_CUDA, "re-sort failed");
         // the scan cleared the counts; the current state is untouched
-        rc = ensure_list(E, list_regrow_cap(E));
+        rc = ensure_list_after(E, ef);
         if (rc) return rc;
     }
     return fail(E, RDGPU_ERR_CUDA, "pair-list build did not converge");
@@ -892,7 +932,7 @@ template <class R> int enter_list(Engine* E, double skin)
         }
     }
     if (E->part_off.empty() || E->npart_tot == 0) return RDGPU_OK;
-    int rc = ensure_list(E, list_cap_estimate(E));
+    int rc = ensure_list(E, list_cap_estimate(E), E->list_wide);
     if (rc) return rc;
     return resort<R>(E, true);
 }
@@ -982,14 +1022,14 @@ template <class R> int do_steps_list(Engine* E, long long nsteps, const double* 
         const long long tf = *E->pinned_step;
         E->step_h = tf;
         set_cur(E, (int)((tf + nreb) & 1));
-        if (ef == EF_LISTOVF) {
-            rc = ensure_list(E, list_regrow_cap(E));
+        if ((ef & ~(EF_LISTOVF | EF_LISTWIDE)) == 0) {
+            rc = ensure_list_after(E, ef);
             if (rc) return rc;
             rc = resort<R>(E, true);
             if (rc) return rc;
             // the particles gathered into denser clusters than the tuner saw:
             // an AUTO handle times its options again on the new state
-            if (E->nb_req == RDGPU_NB_AUTO && !E->tuning && !noise_d) {
+            if ((ef & EF_LISTOVF) && E->nb_req == RDGPU_NB_AUTO && !E->tuning && !noise_d) {
                 E->retune = true;
                 return RDGPU_OK_CONTINUE;
             }
@@ -1157,6 +1197,8 @@ int setup_systems(Engine* E, std::string& why)
             }
             v.per[a] = b.periodic[a] ? 1 : 0;
             v.Lf[a] = Lf;
+            v.qs[a] = (float)(65536.0 / Lp);
+            v.iqs[a] = (float)(Lp / 65536.0);
             v.halff[a] = 0.5f * Lf;
             v.ilf[a] = b.periodic[a] ? 1.0f / Lf : 0.0f;
             v.il[a] = b.periodic[a] ? 1.0 / L : 0.0;
@@ -1261,13 +1303,13 @@ template <class R> int profile_list(Engine* E, long long nsteps, double* kms, do
         // reported
         E->step_h = *E->pinned_step;
         set_cur(E, (int)((E->step_h + nreb) & 1));
-        if (ef != EF_LISTOVF) {
+        if (ef & ~(EF_LISTOVF | EF_LISTWIDE)) {
             rc = prepare_step_state(E, E->step_h);
             if (!rc) rc = fail(E, (ef & EF_NONFINITE) ? RDGPU_ERR_NONFINITE : RDGPU_ERR_JUMP,
                                "a step failed during profiling at step " + std::to_string(E->step_h));
             break;
         }
-        rc = ensure_list(E, list_regrow_cap(E));
+        rc = ensure_list_after(E, ef);
         if (!rc) rc = resort<R>(E, true);
         if (rc) break;
     }
@@ -1483,7 +1525,7 @@ template <class R, class In> int set_particles_impl(Engine* E, const long long* 
     if (rc) return rc;
     E->part_off = off;
     if (E->nb_mode == RDGPU_NB_LIST && ntot > 0) {
-        rc = ensure_list(E, list_cap_estimate(E));
+        rc = ensure_list(E, list_cap_estimate(E), E->list_wide);
         if (!rc) rc = resort<R>(E, true);
         if (rc) { E->part_off.clear(); return rc; }
     }
@@ -1643,7 +1685,7 @@ template <class R> int apply_edits_impl(Engine* E, const float* ed, long long co
     rc = reset_counters(E, E->step_h);
     if (rc) return rc;
     if (E->nb_mode == RDGPU_NB_LIST && N2 > 0) {
-        rc = ensure_list(E, list_cap_estimate(E));
+        rc = ensure_list(E, list_cap_estimate(E), E->list_wide);
         if (!rc) rc = resort<R>(E, true);
         if (rc) { E->part_off.clear(); return rc; }
     }
@@ -1759,14 +1801,20 @@ template <class R> int rdf_fine(Engine* E, int nbins, double rmax)
     return RDGPU_OK;
 }
 
-// The RDF frame on a coarse grid of cells of edge >= rmax (rdf_tile_kernel),
-// from the current state in any order (no re-sort of the simulation's cells).
-// Returns RDGPU_OK_CONTINUE when some system's grid has fewer than 3 cells
-// along a periodic axis (rdf_fine then takes the frame).
+// The RDF frame on a grid of its own (rdf_tile_kernel), from the current
+// state in any order (no re-sort of the simulation's cells): cells of edge
+// >= rmax / 2 with a stencil of half-width 2 when every periodic axis of
+// every system has >= 5 of them, else cells of edge >= rmax with half-width
+// 1 (>= 3 cells).  Returns RDGPU_OK_CONTINUE when neither fits (rdf_fine
+// then takes the frame).
 template <class R> int rdf_tiled(Engine* E, int nbins, double rmax)
 {
     const int S = E->desc.n_types;
     const int H = S * S * nbins;
+    int hw = 2;
+    for (int s = 0; s < E->nsys && hw == 2; ++s)
+        for (int a = 0; a < 3; ++a)
+            if (E->sys_h[s].per[a] && std::min(cells_along(edge(E, s, a), 0.5 * rmax), 512) < 5) hw = 1;
     std::vector<RdfGrid> gh(E->nsys);
     long long nc = 0;
     double lmax = 0.0;
@@ -1776,8 +1824,8 @@ template <class R> int rdf_tiled(Engine* E, int nbins, double rmax)
         long long m = 1;
         for (int a = 0; a < 3; ++a) {
             const double Lp = edge(E, s, a);
-            const int n = std::min(cells_along(Lp, rmax), 256);
-            if (E->sys_h[s].per[a] && n < 3) return RDGPU_OK_CONTINUE;
+            const int n = std::min(cells_along(Lp, rmax / hw), 256 * hw);
+            if (E->sys_h[s].per[a] && n < 2 * hw + 1) return RDGPU_OK_CONTINUE;
             g.n[a] = n;
             g.per[a] = E->sys_h[s].per[a];
             g.L[a] = Lp;
@@ -1829,8 +1877,8 @@ template <class R> int rdf_tiled(Engine* E, int nbins, double rmax)
     const size_t smem = use_smem ? dyn : (size_t)(nbins + 1) * 8;
     if (smem > 40 * 1024) return RDGPU_OK_CONTINUE;
     const int grid = (int)std::min<long long>((nc + RDF_WARPS - 1) / RDF_WARPS, 148LL * 8);
-    rdf_tile_kernel<R><<<grid, RDF_WARPS * 32, smem, E->stream>>>(E->rdf_grid_d, E->nsys, nc, E->rdf_start, rec, S,
-                                                                  nbins, E->rdf_e2, rmax / (double)nbins, r2pre,
+    rdf_tile_kernel<R><<<grid, RDF_WARPS * 32, smem, E->stream>>>(E->rdf_grid_d, E->nsys, nc, hw, E->rdf_start, rec,
+                                                                  S, nbins, E->rdf_e2, rmax / (double)nbins, r2pre,
                                                                   use_smem, E->rdf_tmp);
     CK(cudaGetLastError());
     return RDGPU_OK;
@@ -2249,6 +2297,7 @@ int rdgpu_metrics_get(rdgpu_handle h, rdgpu_metrics* m)
     m->list_builds = E->nbuild_h;
     m->skin = E->nb_mode == RDGPU_NB_LIST ? E->skin : 0.0;
     m->list_capacity = E->nb_mode == RDGPU_NB_LIST ? E->list_cap : 0;
+    m->list_entry_bytes = E->nb_mode == RDGPU_NB_LIST ? (E->list_wide ? 4 : 2) : 0;
     if (E->npart_tot == 0) return RDGPU_OK;
     int rc = rdgpu_forces(h, nullptr, &m->energy);
     if (rc) return rc;

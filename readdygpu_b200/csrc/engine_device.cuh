@@ -45,6 +45,8 @@ struct SysDev {
     double il[3];     // 1/L on periodic axes, 0 on open ones (image by rounding)
     double lo[3];
     unsigned long long seed;
+    float qs[3];      // 2^16 / L: bins of the 16-bit build-position lattice per unit length
+    float iqs[3];     // L / 2^16
 };
 
 template <class R> struct PairTerm {

@@ -26,7 +26,6 @@
 // (lib/ReaDDyGPU_Cpp/CudaKernels/CudaSimulation.cu:1034-1236, 1402-1782,
 // 1838-1919).
 #pragma once
-#include <type_traits>
 #include "engine_device.cuh"
 
 namespace rdgpu {
@@ -1206,16 +1205,18 @@ __global__ void __launch_bounds__(128, 8) rdf_kernel(const SysDev* __restrict__ 
 // cells of edge >= rmax and at least 3 cells along every periodic axis, so
 // every pair closer than rmax sits in one cell or in two neighbouring ones,
 // and each unordered pair of neighbouring cells appears once among a cell's
-// 13 forward neighbours.  A warp takes the particles of one cell 32 at a time
-// (one per lane); the particles of each forward neighbour (and of the cell
-// itself, partners of higher index only) pass through a per-warp shared-memory
-// tile and are tested against all 32 lanes with an FP32 distance that
-// over-accepts (r2pre covers its rounding).  Accepted pairs queue in shared
-// memory and are evaluated 32 at a time, one per lane, with the exact FP64
-// predicate and bin rule of rdf_kernel: dx = (xi - xj) - sx, sx the periodic
-// shift of the neighbour cell, which is the symmetric minimum image
-// (mimg_sym) for every pair closer than rmax < L/2.  Each pair is counted
-// for both orientations, as in rdf_kernel.
+// 13 forward neighbours.  A warp takes one cell: its particles (up to 128 at
+// a time) and then the particles of each forward neighbour (and of the cell
+// itself, partners of higher index only), moved to their periodic image next
+// to the cell, go to per-warp shared memory.  The own x candidate tests are
+// spread over the lanes, consecutive tests on consecutive lanes, with an
+// FP32 distance that over-accepts (r2pre covers its rounding); each lane
+// collects its accepted tests of a window as bits, and one warp scan
+// compacts them into a queue.  Queued pairs are evaluated 32 at a time, one
+// per lane, with the exact FP64 predicate and bin rule of rdf_kernel: dx =
+// (xi - xj) - sx, sx the periodic shift of the neighbour cell, which is the
+// symmetric minimum image (mimg_sym) for every pair closer than rmax < L/2.
+// Each pair is counted for both orientations, as in rdf_kernel.
 // ---------------------------------------------------------------------------
 struct RdfGrid {
     int n[3];
@@ -1278,21 +1279,50 @@ __global__ void rdf_scatter_kernel(long long ntot, State<R> cur, const int* __re
     }
 }
 
-// forward neighbours (dx, dy, dz) of a cell; entry 0 is the cell itself
-__constant__ signed char c_rdf_nb[14][3] = {
-    {0, 0, 0},  {1, 0, 0},  {-1, 1, 0}, {0, 1, 0},  {1, 1, 0},
-    {-1, -1, 1}, {0, -1, 1}, {1, -1, 1}, {-1, 0, 1}, {0, 0, 1}, {1, 0, 1},
-    {-1, 1, 1}, {0, 1, 1},  {1, 1, 1}};
-
 constexpr int RDF_WARPS = 4;
+constexpr int RDF_OWN = 64;       // own particles per pass of a cell
+constexpr int RDF_WIN = 16;       // own particles tested per lane between two compactions
+constexpr int RDF_QUEUE = 32 * RDF_WIN + 32;
+constexpr int RDF_NBMAX = 63;     // forward neighbours of a stencil of half-width 2, and the cell
 
-template <class R>
-__device__ __forceinline__ void rdf_exact(const double* __restrict__ ox, const int* __restrict__ ot,
-                                          const RdfRec<R>* __restrict__ rec, int2 e, const RdfGrid& g, int S,
-                                          int nbins, double rmax2, float inv_wf, const double* __restrict__ e2s,
-                                          int use_smem, unsigned* __restrict__ sh, unsigned long long* __restrict__ hist)
+// per-warp shared memory of rdf_tile_kernel
+struct RdfWarp {
+    float4 own[RDF_OWN];          // own particles as floats, bits(type) in w
+    double ox[3 * RDF_OWN];       // own particles as stored (widened FP32 or FP64)
+    int nbase[RDF_NBMAX];         // first candidate of each neighbour cell
+    int npre[RDF_NBMAX + 1];      // exclusive prefix of the neighbour cells' counts
+    int ncode[RDF_NBMAX];         // periodic shift code of each neighbour cell (2 bits per axis)
+    int2 queue[RDF_QUEUE];        // accepted pairs: (candidate index, own | shift code << 8)
+};
+
+// The q-th offset of the half-shell of a stencil of half-width hw (1 or 2):
+// offset 0 is the cell itself, then the offsets (dx, dy, dz) with dz > 0, or
+// dz == 0 and dy > 0, or dz == dy == 0 and dx > 0, in lexicographic order.
+__device__ __forceinline__ void rdf_offset(int q, int hw, int d[3])
 {
-    const int o = e.y & 31, code = e.y >> 5;
+    if (q == 0) { d[0] = d[1] = d[2] = 0; return; }
+    const int w = 2 * hw + 1;
+    // offsets with dz == dy == 0, dx > 0: hw of them; then dz == 0, dy > 0:
+    // hw * w; then dz > 0: hw * w * w
+    int k = q - 1;
+    if (k < hw) { d[0] = 1 + k; d[1] = 0; d[2] = 0; return; }
+    k -= hw;
+    if (k < hw * w) { d[2] = 0; d[1] = 1 + k / w; d[0] = k % w - hw; return; }
+    k -= hw * w;
+    d[2] = 1 + k / (w * w);
+    k %= w * w;
+    d[1] = k / w - hw;
+    d[0] = k % w - hw;
+}
+
+// the exact FP64 predicate and bin of one queued pair (rdf_kernel's rule)
+template <class R>
+__device__ __forceinline__ void rdf_exact(const RdfWarp& w, const RdfRec<R>* __restrict__ rec, int2 e,
+                                          const RdfGrid& g, int S, int nbins, double rmax2, float inv_wf,
+                                          const double* __restrict__ e2s, int use_smem, unsigned* __restrict__ sh,
+                                          unsigned long long* __restrict__ hist)
+{
+    const int o = e.y & 0xff, code = e.y >> 8;
     double xj[3];
     int tj;
     if constexpr (sizeof(R) == 4) {
@@ -1309,7 +1339,7 @@ __device__ __forceinline__ void rdf_exact(const double* __restrict__ ox, const i
     for (int a = 0; a < 3; ++a) {
         const int sc = (code >> (2 * a)) & 3;
         const double sx = sc == 1 ? g.L[a] : (sc == 2 ? -g.L[a] : 0.0);
-        d[a] = sub_rn(sub_rn(ox[3 * o + a], xj[a]), sx);
+        d[a] = sub_rn(sub_rn(w.ox[3 * o + a], xj[a]), sx);
     }
     const double r2 = dist2(d[0], d[1], d[2]);
     if (!(r2 < rmax2)) return;
@@ -1318,7 +1348,7 @@ __device__ __forceinline__ void rdf_exact(const double* __restrict__ ox, const i
     k = min(max(k, 0), nbins - 1);
     while (k > 0 && e2s[k] > r2) --k;
     while (k < nbins - 1 && e2s[k + 1] <= r2) ++k;
-    const int ti = ot[o];
+    const int ti = __float_as_int(w.own[o].w);
     const int h1 = (ti * S + tj) * nbins + k, h2 = (tj * S + ti) * nbins + k;
     if (use_smem) {
         if (h1 == h2) atomicAdd(sh + h1, 2u);
@@ -1331,16 +1361,13 @@ __device__ __forceinline__ void rdf_exact(const double* __restrict__ ox, const i
 
 template <class R>
 __global__ void __launch_bounds__(RDF_WARPS * 32) rdf_tile_kernel(const RdfGrid* __restrict__ grids, int nsys,
-        long long ncells, const int* __restrict__ start, const RdfRec<R>* __restrict__ rec, int S, int nbins,
-        const double* __restrict__ e2, double w, float r2pre, int use_smem, unsigned long long* __restrict__ hist)
+        long long ncells, int hw, const int* __restrict__ start, const RdfRec<R>* __restrict__ rec, int S,
+        int nbins, const double* __restrict__ e2, double w, float r2pre, int use_smem,
+        unsigned long long* __restrict__ hist)
 {
-    // shared memory: per warp a tile of 32 candidates, 64 queued pairs and
-    // the 32 lanes' own positions and types; then the squared bin edges and,
+    // shared memory: the warps' RdfWarp, then the squared bin edges and,
     // with use_smem, the block's histogram
-    __shared__ float4 s_tile[RDF_WARPS][32];
-    __shared__ int2 s_queue[RDF_WARPS][64];
-    __shared__ double s_own[RDF_WARPS][96];
-    __shared__ int s_ot[RDF_WARPS][32];
+    __shared__ RdfWarp s_w[RDF_WARPS];
     extern __shared__ double s_dyn[];
     double* e2s = s_dyn;
     unsigned* sh = reinterpret_cast<unsigned*>(s_dyn + nbins + 1);
@@ -1350,13 +1377,11 @@ __global__ void __launch_bounds__(RDF_WARPS * 32) rdf_tile_kernel(const RdfGrid*
         for (int k = threadIdx.x; k < H; k += blockDim.x) sh[k] = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
-    float4* tile = s_tile[wp];
-    int2* queue = s_queue[wp];
-    double* ox = s_own[wp];
-    int* ot = s_ot[wp];
+    RdfWarp& W = s_w[wp];
     const double rmax2 = e2[nbins];
     const float inv_wf = (float)(1.0 / w);
-    const unsigned lt = (1u << lane) - 1u;
+    const int wd = 2 * hw + 1;
+    const int nnb = 1 + (wd * wd * wd - 1) / 2;
     for (long long c = (long long)blockIdx.x * RDF_WARPS + wp; c < ncells; c += (long long)gridDim.x * RDF_WARPS) {
         const int a0 = start[c], a1 = start[c + 1];
         if (a0 == a1) continue;
@@ -1369,92 +1394,144 @@ __global__ void __launch_bounds__(RDF_WARPS * 32) rdf_tile_kernel(const RdfGrid*
         const RdfGrid& g = grids[lo];
         const long long lc = c - g.base;
         const int cc[3] = {(int)(lc % g.n[0]), (int)((lc / g.n[0]) % g.n[1]), (int)(lc / ((long long)g.n[0] * g.n[1]))};
-        for (int ob = a0; ob < a1; ob += 32) {
-            const int i = ob + lane;
-            const bool own = i < a1;
-            float xf[3] = {0.f, 0.f, 0.f};
-            if (own) {
-                double xd[3];
-                int t;
-                if constexpr (sizeof(R) == 4) {
-                    const float4 p = __ldg(&rec[i].p);
-                    xd[0] = p.x; xd[1] = p.y; xd[2] = p.z;
-                    t = __float_as_int(p.w);
-                } else {
-                    const RdfRec<double> q = rec[i];
-                    xd[0] = q.x; xd[1] = q.y; xd[2] = q.z;
-                    t = q.t;
-                }
-#pragma unroll
-                for (int a = 0; a < 3; ++a) { ox[3 * lane + a] = xd[a]; xf[a] = (float)xd[a]; }
-                ot[lane] = t;
-            }
-            int qn = 0;
-            for (int nb = 0; nb < 14; ++nb) {
-                int q[3];
-                int code = 0;
-                float sxf[3];
+        // the neighbour cells: first candidate, count (0 beyond an open
+        // bound) and periodic shift code; exclusive prefix of the counts
+        __syncwarp();
+        int run = 0;
+        for (int q0 = 0; q0 < nnb; q0 += 32) {
+            const int q = q0 + lane;
+            int cnt = 0, base = 0, code = 0;
+            if (q < nnb) {
+                int d[3];
+                rdf_offset(q, hw, d);
                 bool skip = false;
+                int z[3];
 #pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    q[a] = cc[a] + c_rdf_nb[nb][a];
-                    sxf[a] = 0.f;
-                    if (q[a] < 0) {
-                        if (!g.per[a]) skip = true;
-                        q[a] += g.n[a];
-                        sxf[a] = -(float)g.L[a];
-                        code |= 2 << (2 * a);
-                    } else if (q[a] >= g.n[a]) {
-                        if (!g.per[a]) skip = true;
-                        q[a] -= g.n[a];
-                        sxf[a] = (float)g.L[a];
-                        code |= 1 << (2 * a);
+                for (int ax = 0; ax < 3; ++ax) {
+                    z[ax] = cc[ax] + d[ax];
+                    if (z[ax] < 0) {
+                        if (!g.per[ax]) skip = true;
+                        z[ax] += g.n[ax];
+                        code |= 2 << (2 * ax);
+                    } else if (z[ax] >= g.n[ax]) {
+                        if (!g.per[ax]) skip = true;
+                        z[ax] -= g.n[ax];
+                        code |= 1 << (2 * ax);
                     }
                 }
-                if (skip) continue;
-                const long long nc = g.base + ((long long)q[2] * g.n[1] + q[1]) * g.n[0] + q[0];
-                const int b0 = nb == 0 ? a0 : start[nc], b1 = nb == 0 ? a1 : start[nc + 1];
-                for (int tb = b0; tb < b1; tb += 32) {
-                    const int m = min(32, b1 - tb);
-                    __syncwarp();
-                    if (lane < m) {
-                        if constexpr (sizeof(R) == 4) {
-                            tile[lane] = __ldg(&rec[tb + lane].p);
-                        } else {
-                            const RdfRec<double> r = rec[tb + lane];
-                            tile[lane] = make_float4((float)r.x, (float)r.y, (float)r.z, 0.f);
+                if (!skip) {
+                    const long long nc = g.base + ((long long)z[2] * g.n[1] + z[1]) * g.n[0] + z[0];
+                    base = start[nc];
+                    cnt = start[nc + 1] - base;
+                }
+                W.nbase[q] = base;
+                W.ncode[q] = code;
+            }
+            int incl = cnt;
+#pragma unroll
+            for (int sft = 1; sft < 32; sft <<= 1) {
+                const int t = __shfl_up_sync(FULL, incl, sft);
+                if (lane >= sft) incl += t;
+            }
+            if (q < nnb) W.npre[q] = run + incl - cnt;
+            run += __shfl_sync(FULL, incl, 31);
+        }
+        if (lane == 0) W.npre[nnb] = run;
+        const int C = run;     // candidates of all neighbour cells
+        for (int ob = a0; ob < a1; ob += RDF_OWN) {
+            const int m = min(RDF_OWN, a1 - ob);
+            __syncwarp();
+            for (int t = lane; t < m; t += 32) {
+                double xd[3];
+                int ty;
+                if constexpr (sizeof(R) == 4) {
+                    const float4 p = __ldg(&rec[ob + t].p);
+                    xd[0] = p.x; xd[1] = p.y; xd[2] = p.z;
+                    ty = __float_as_int(p.w);
+                } else {
+                    const RdfRec<double> q = rec[ob + t];
+                    xd[0] = q.x; xd[1] = q.y; xd[2] = q.z;
+                    ty = q.t;
+                }
+                W.own[t] = make_float4((float)xd[0], (float)xd[1], (float)xd[2], __int_as_float(ty));
+                W.ox[3 * t] = xd[0]; W.ox[3 * t + 1] = xd[1]; W.ox[3 * t + 2] = xd[2];
+            }
+            __syncwarp();
+            int qn = 0;
+            // one candidate per lane, 32 at a time over all neighbour cells
+            for (int cb = 0; cb < C; cb += 32) {
+                const int t = cb + lane;
+                const bool have = t < C;
+                // its neighbour cell: the last q with npre[q] <= t
+                int ql = 0, qh = nnb - 1;
+                while (ql < qh) {
+                    const int mid = (ql + qh + 1) >> 1;
+                    if (W.npre[mid] <= t) ql = mid; else qh = mid - 1;
+                }
+                const int j = W.nbase[ql] + (t - W.npre[ql]);
+                const int code = W.ncode[ql];
+                float cx = 3e30f, cy = 3e30f, cz = 3e30f;     // no candidate: never accepted
+                if (have) {
+                    float4 p;
+                    if constexpr (sizeof(R) == 4) {
+                        p = __ldg(&rec[j].p);
+                    } else {
+                        const RdfRec<double> r = rec[j];
+                        p = make_float4((float)r.x, (float)r.y, (float)r.z, 0.f);
+                    }
+                    // the candidate's image next to the own cell
+                    const int s0 = code & 3, s1 = (code >> 2) & 3, s2 = (code >> 4) & 3;
+                    cx = p.x + (s0 == 1 ? (float)g.L[0] : (s0 == 2 ? -(float)g.L[0] : 0.f));
+                    cy = p.y + (s1 == 1 ? (float)g.L[1] : (s1 == 2 ? -(float)g.L[1] : 0.f));
+                    cz = p.z + (s2 == 1 ? (float)g.L[2] : (s2 == 2 ? -(float)g.L[2] : 0.f));
+                }
+                // partners in the own cell itself (q == 0) count from a higher index only
+                const int jmin = ql == 0 ? j - ob : RDF_OWN;   // own o tests j only when o < j - ob
+                for (int o0 = 0; o0 < m; o0 += RDF_WIN) {
+                    unsigned bits = 0;
+#pragma unroll
+                    for (int it = 0; it < RDF_WIN; ++it) {
+                        const int o = o0 + it;
+                        if (o < m) {
+                            const float4 a = W.own[o];
+                            const float dx = a.x - cx, dy = a.y - cy, dz = a.z - cz;
+                            const float r2f = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                            const bool acc = r2f < r2pre && o < jmin;
+                            bits |= (unsigned)acc << it;
                         }
                     }
+                    const int cntl = __popc(bits);
+                    int incl = cntl;
+#pragma unroll
+                    for (int sft = 1; sft < 32; sft <<= 1) {
+                        const int tt = __shfl_up_sync(FULL, incl, sft);
+                        if (lane >= sft) incl += tt;
+                    }
+                    const int tot = __shfl_sync(FULL, incl, 31);
+                    if (tot == 0) continue;
+                    int slot = qn + incl - cntl;
+                    while (bits) {
+                        const int it = __ffs(bits) - 1;
+                        bits &= bits - 1;
+                        W.queue[slot++] = make_int2(j, (o0 + it) | (code << 8));
+                    }
+                    qn += tot;
                     __syncwarp();
-                    for (int k = 0; k < m; ++k) {
-                        const float4 p = tile[k];
-                        const float dx = (xf[0] - p.x) - sxf[0];
-                        const float dy = (xf[1] - p.y) - sxf[1];
-                        const float dz = (xf[2] - p.z) - sxf[2];
-                        const float r2f = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                        const bool acc = own && r2f < r2pre && (nb != 0 || tb + k > i);
-                        const unsigned bal = __ballot_sync(FULL, acc);
-                        if (bal) {
-                            if (acc) queue[qn + __popc(bal & lt)] = make_int2(tb + k, lane | (code << 5));
-                            qn += __popc(bal);
-                            if (qn >= 32) {
-                                __syncwarp();
-                                rdf_exact<R>(ox, ot, rec, queue[lane], g, S, nbins, rmax2, inv_wf, e2s, use_smem, sh,
-                                             hist);
-                                __syncwarp();
-                                if (lane < qn - 32) queue[lane] = queue[32 + lane];
-                                qn -= 32;
-                                __syncwarp();
-                            }
-                        }
+                    // evaluate full batches of 32
+                    int done = 0;
+                    for (; done + 32 <= qn; done += 32)
+                        rdf_exact<R>(W, rec, W.queue[done + lane], g, S, nbins, rmax2, inv_wf, e2s, use_smem, sh, hist);
+                    __syncwarp();
+                    if (done > 0) {
+                        if (lane < qn - done) W.queue[lane] = W.queue[done + lane];
+                        qn -= done;
+                        __syncwarp();
                     }
                 }
             }
             // what is left in the queue
             __syncwarp();
-            if (lane < qn)
-                rdf_exact<R>(ox, ot, rec, queue[lane], g, S, nbins, rmax2, inv_wf, e2s, use_smem, sh, hist);
-            __syncwarp();
+            if (lane < qn) rdf_exact<R>(W, rec, W.queue[lane], g, S, nbins, rmax2, inv_wf, e2s, use_smem, sh, hist);
         }
     }
     if (use_smem) {
@@ -1592,6 +1669,51 @@ __global__ void __launch_bounds__(TSUM_BLOCK) typed_final_kernel(const double* _
 // bit nreb flips at every re-sort.
 // ---------------------------------------------------------------------------
 constexpr int EF_LISTOVF = 16;
+constexpr int EF_LISTWIDE = 32;   // a partner's offset needs the 32-bit list entries
+
+// List head of particle i (8 bytes): its position at the build on a lattice
+// of 2^16 bins per box edge, wrapping (x: bits 0-15 of .x, y: bits 16-31, z:
+// bits 0-15 of .y), and its list length (bits 16-31 of .y).  The lattice
+// coordinate of any x (also beyond an open axis' bounds) is floor(x 2^16/L)
+// mod 2^16; a displacement shorter than L/2 is the wrapped 16-bit difference
+// of two lattice coordinates, within 2 bins (the floors and a periodic wrap
+// whose L 2^16/L rounds off the integer) of the exact one.
+__device__ __forceinline__ unsigned qcoord(float x, float q) { return (unsigned)__float2int_rd(x * q) & 0xffffu; }
+
+template <class R>
+__device__ __forceinline__ uint2 make_head(const R x[3], const SysDev& s, int cnt)
+{
+    const unsigned qx = qcoord((float)x[0], s.qs[0]), qy = qcoord((float)x[1], s.qs[1]);
+    const unsigned qz = qcoord((float)x[2], s.qs[2]);
+    return make_uint2(qx | (qy << 16), qz | ((unsigned)cnt << 16));
+}
+
+__device__ __forceinline__ int head_count(uint2 h) { return (int)(h.y >> 16); }
+
+// squared displacement since the build, lattice estimate
+template <class R>
+__device__ __forceinline__ float head_disp2(uint2 h, const R x[3], const SysDev& s)
+{
+    const int dx = (short)(qcoord((float)x[0], s.qs[0]) - (h.x & 0xffffu));
+    const int dy = (short)(qcoord((float)x[1], s.qs[1]) - (h.x >> 16));
+    const int dz = (short)(qcoord((float)x[2], s.qs[2]) - (h.y & 0xffffu));
+    const float ex = (float)dx * s.iqs[0], ey = (float)dy * s.iqs[1], ez = (float)dz * s.iqs[2];
+    return ex * ex + ey * ey + ez * ez;
+}
+
+// List entries in int4 groups, column-major over i (group g of particle i
+// at nbr4[g stride + i]): narrow lists hold 8 signed 16-bit offsets j - i
+// per group, wide ones 4 sorted indices j.
+__device__ __forceinline__ int group_word(const int4& g, int u)
+{
+    return u == 0 ? g.x : (u == 1 ? g.y : (u == 2 ? g.z : g.w));
+}
+__device__ __forceinline__ int list_entry(const int4& g, int u, bool narrow, int i)
+{
+    if (!narrow) return group_word(g, u);
+    const int wd = group_word(g, u >> 1);
+    return i + ((u & 1) ? (wd >> 16) : (int)(short)(wd & 0xffff));
+}
 
 struct ListCtl {
     int need;        // 1: re-sort and rebuild after this step
@@ -1605,11 +1727,11 @@ struct ListCtl {
 template <class R> struct ListArgs {
     State<R> b0, b1;     // the two state buffers
     ListCtl* ctl;
-    int* nbr;            // k-th partner of sorted particle i at nbr[4 ((k/4) stride + i) + k%4]: groups
-                         // of 4 as one int4, column-major over i; null: sort only
-    float4* xref;        // position of particle i at the build; w: bits of its list length
+    int4* nbr;           // list entries in groups (list_entry); null: sort only
+    uint2* head;         // list heads (make_head)
     long long stride;
-    int cap;             // list capacity per particle
+    int cap;             // list capacity per particle (a multiple of 8)
+    int narrow;          // 16-bit offsets, 8 per group (else 32-bit indices, 4 per group)
     const R* rl2t;       // squared list radius (rc + skin) per type pair; 0: no potential, never listed
     R rl2max;            // the largest of them
     float thr2;          // squared displacement since the build above which the list check looks at a particle
@@ -1645,135 +1767,32 @@ __device__ __forceinline__ void store_state(const State<double>& st, long long i
     st.rec[i] = r;
 }
 
-// The listed pairs of a warp's 32 particles spread over its 32 lanes (FP32).
-// Each lane's list goes to shared memory as (partner, owner lane) entries at
-// its place in the warp's concatenated lists, and the lanes then take the
-// entries 32 at a time, so the warp runs about (sum of the list lengths) / 32
-// pair evaluations rather than 32 times the longest list.  The owner's
-// operands come from shared memory; each pair term is converted to 2^-32
-// fixed point and added to the owner's sums with a shared-memory atomic, the
-// same integers the per-particle loop adds, so the sums are the same bit for
-// bit in any order.
-constexpr int FLAT_CAP = 256;    // entries per warp and round
-
-struct FlatWarpF {
-    float4 x[32];                    // the owner lane's position, bits(type)
-    float4 il[32];                   // 1/L per axis (0 on open axes), L_x
-    float2 l[32];                    // L_y, L_z
-    unsigned long long acc[3][32];   // 2^-32 fixed-point force sums
-    int2 pr[FLAT_CAP];               // (partner's sorted index, owner lane)
-};
-struct FlatNone {};
-
-__device__ __forceinline__ void flat_add(FlatWarpF& fw, int o, float pre, float dx, float dy, float dz)
+// The partners of list entries k0 .. k0 + 3 (k0 a multiple of 4) of sorted
+// particle i, from the group q that holds them: NARROW, two 32-bit words of
+// 16-bit offsets j - i; wide, the 4 indices.
+template <bool NARROW>
+__device__ __forceinline__ void chunk_entries(const int4& q, int k0, int i, int jj[4])
 {
-    const float q = -pre * FX_SCALE;
-    atomicAdd(&fw.acc[0][o], (unsigned long long)__float2ll_rn(q * dx));
-    atomicAdd(&fw.acc[1][o], (unsigned long long)__float2ll_rn(q * dy));
-    atomicAdd(&fw.acc[2][o], (unsigned long long)__float2ll_rn(q * dz));
-}
-
-template <bool HREP>
-__device__ __forceinline__ void flat_pair(FlatWarpF& fw, int2 e, const float xj[3], int wj, const float* s_rc2,
-                                          const FastTab<float>& ft, const TypeTab<float>* tab)
-{
-    const float4 ox = fw.x[e.y], il4 = fw.il[e.y];
-    const float2 l2 = fw.l[e.y];
-    PairFrame pf;
-    pf.xy = f2_pack(ox.x, ox.y);
-    pf.il_xy = f2_pack(il4.x, il4.y);
-    pf.l_xy = f2_pack(il4.w, l2.x);
-    pf.z = ox.z;
-    pf.il_z = il4.z;
-    pf.l_z = l2.y;
-    float dx, dy, dz, r2;
-    pair_disp_x2(pf, xj[0], xj[1], xj[2], dx, dy, dz, r2);
-    const int pidx = __float_as_int(ox.w) * MAXT + (wj & 0xff);
-    if (!(r2 < s_rc2[pidx])) return;
-    if (HREP) {
-        // pre = k (r - r0) / r; r == 0 has no direction
-        if (r2 > 0.0f) flat_add(fw, e.y, ft.k[pidx] * (1.0f - ft.r0[pidx] * rsqrtf(r2)), dx, dy, dz);
+    if constexpr (NARROW) {
+        const bool hi = (k0 & 4) != 0;
+        const int w0 = hi ? q.z : q.x, w1 = hi ? q.w : q.y;
+        jj[0] = i + (int)(short)w0;
+        jj[1] = i + (w0 >> 16);
+        jj[2] = i + (int)(short)w1;
+        jj[3] = i + (w1 >> 16);
     } else {
-        const float r = sqrtf(r2);
-        const int nt = tab->nterm[pidx];
-        for (int m = 0; m < nt; ++m) {
-            float pre, en;
-            pair_term(tab->term[pidx * MAX_TERMS + m], r, pre, en);
-            flat_add(fw, e.y, pre, dx, dy, dz);
-        }
+        jj[0] = q.x; jj[1] = q.y; jj[2] = q.z; jj[3] = q.w;
     }
-}
-
-template <bool HREP>
-__device__ __forceinline__ void flat_pairs(FlatWarpF& fw, const State<float>& cur, const ListArgs<float>& v,
-                                           const float* s_rc2, const FastTab<float>& ft, const TypeTab<float>* tab,
-                                           int lane, int i, const float xi[3], int ti, const SysDev& s, int cnt,
-                                           const int4& q0, const int4& q1, Acc<float>& acc)
-{
-    // place of this lane's list in the warp's concatenated lists
-    int incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(FULL, incl, o);
-        if (lane >= o) incl += t;
-    }
-    const int pre = incl - cnt;
-    const int P = __shfl_sync(FULL, incl, 31);
-    if (P == 0) return;
-    fw.x[lane] = make_float4(xi[0], xi[1], xi[2], __int_as_float(ti));
-    fw.il[lane] = make_float4(s.ilf[0], s.ilf[1], s.ilf[2], s.Lf[0]);
-    fw.l[lane] = make_float2(s.Lf[1], s.Lf[2]);
-    fw.acc[0][lane] = 0ull;
-    fw.acc[1][lane] = 0ull;
-    fw.acc[2][lane] = 0ull;
-    const int4* nb4 = reinterpret_cast<const int4*>(v.nbr) + i;
-    for (int base = 0; base < P; base += FLAT_CAP) {
-        // this lane's entries that fall into [base, base + FLAT_CAP)
-        const int k0 = max(0, base - pre), k1 = min(cnt, base + FLAT_CAP - pre);
-        for (int k = k0; k < k1; ++k) {
-            int j;
-            if (k < 8) {
-                const int4 q = k < 4 ? q0 : q1;
-                const int u = k & 3;
-                j = u == 0 ? q.x : (u == 1 ? q.y : (u == 2 ? q.z : q.w));
-            } else {
-                j = __ldg(reinterpret_cast<const int*>(nb4 + (long long)(k >> 2) * v.stride) + (k & 3));
-            }
-            fw.pr[pre + k - base] = make_int2(j, lane);
-        }
-        __syncwarp();
-        const int m = min(P - base, FLAT_CAP);
-        // two entries per lane and trip: both partner positions requested
-        // before either pair is evaluated
-        for (int s0 = lane; s0 < m; s0 += 64) {
-            const int s1 = s0 + 32;
-            const bool two = s1 < m;
-            const int2 e0 = fw.pr[s0];
-            const int2 e1 = two ? fw.pr[s1] : e0;
-            float x0[3], x1[3];
-            int w0, w1;
-            load_pos(cur, e0.x, x0, w0);
-            load_pos(cur, e1.x, x1, w1);
-            flat_pair<HREP>(fw, e0, x0, w0, s_rc2, ft, tab);
-            if (two) flat_pair<HREP>(fw, e1, x1, w1, s_rc2, ft, tab);
-        }
-        __syncwarp();
-    }
-    acc.fx = (long long)fw.acc[0][lane];
-    acc.fy = (long long)fw.acc[1][lane];
-    acc.fz = (long long)fw.acc[2][lane];
 }
 
 // one BD step of every particle over its pair list; ALLPER: every axis of
-// every system is periodic (the minimum image needs no per-axis test); FLAT
-// (FP32 only): the warp's listed pairs spread over its lanes (flat_pairs)
-template <class R, bool HREP, bool ALLPER, int BLOCK, bool FLAT = false>
+// every system is periodic (the minimum image needs no per-axis test);
+// NARROW: list entries are 16-bit offsets (the handle's list format)
+template <class R, bool HREP, bool ALLPER, int BLOCK, bool NARROW>
 __global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? 1024 : 768) / BLOCK) list_step_kernel(Args<R> a, ListArgs<R> v)
 {
-    static_assert(!FLAT || sizeof(R) == 4, "the flat pair phase is FP32 only");
     __shared__ R s_rc2[MAXT * MAXT];
     __shared__ FastTab<R> s_ft;
-    __shared__ std::conditional_t<FLAT, FlatWarpF, FlatNone> s_flat[FLAT ? BLOCK / 32 : 1];
     if (*((volatile int*)a.err)) return;   // an earlier step failed: keep its input intact
     // rows of the S types in use (entries (ti, tj) with ti >= S are never read)
     for (int k = threadIdx.x; k < MAXT * a.tab->S; k += BLOCK) {
@@ -1788,20 +1807,14 @@ __global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? 1024 : 768) / BLOCK) 
     const int sel = list_sel(a, v, a.step_off);
     const State<R> cur = sel ? v.b1 : v.b0;
     const State<R> nxt = sel ? v.b0 : v.b1;
-    const int i0 = blockIdx.x * BLOCK + threadIdx.x;
-    // the flat pair phase needs every lane of the warp: lanes past the last
-    // particle take part with an empty list and store nothing
-    const bool valid = i0 < a.ntot;
-    if (!FLAT && !valid) return;
-    const int i = valid ? i0 : (int)a.ntot - 1;
+    const int i = blockIdx.x * BLOCK + threadIdx.x;
+    if (i >= a.ntot) return;
     const int si = a.sys_of[i];
-    const SysDev& s = a.sys[si];
     R xi[3];
     int wi;
-    load_pos(cur, i, xi, wi);
-    const int ti = wi & 0xff;
     R c[3] = {R(0), R(0), R(0)};
     int id;
+    load_pos(cur, i, xi, wi);
     if constexpr (sizeof(R) == 4) {
         const float4 q = __ldg(cur.aux + i);
         c[0] = q.x; c[1] = q.y; c[2] = q.z;
@@ -1809,32 +1822,32 @@ __global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? 1024 : 768) / BLOCK) 
     } else {
         id = __ldg(&cur.rec[i].id);
     }
+    const uint2 hd = __ldg(v.head + i);
+    // the first 8 list entries (one narrow group, two wide ones; capacity
+    // >= 8) are requested together with the particle's own state, before its
+    // list length is known; entries past the length are never used
+    const int4 q0 = __ldg(v.nbr + i);
+    const int4 q1 = NARROW ? q0 : __ldg(v.nbr + i + v.stride);
+    const SysDev& s = a.sys[si];
+    const int ti = wi & 0xff;
     Box<R> bx;
     bx.load(s);
-    const int p0 = s.per[0], p1 = s.per[1], p2 = s.per[2];
     Acc<R> acc;
     acc.zero();
-    const float4 xr = __ldg(v.xref + i);
-    const int cnt = valid ? __float_as_int(xr.w) : 0;
-    // the first 8 list entries (capacity >= 8) are requested together with
-    // the particle's own state, before its list length is known; entries
-    // past the length are never used
-    const int4* nb4 = reinterpret_cast<const int4*>(v.nbr) + i;
-    const int4 q0 = __ldg(nb4), q1 = __ldg(nb4 + v.stride);
+    const int cnt = head_count(hd);
+    const int4* nb4 = v.nbr + i;
     PairFrame pf;
     double il[3] = {0.0, 0.0, 0.0};
     if constexpr (sizeof(R) == 4) pf.load(s, xi);
     else { il[0] = s.il[0]; il[1] = s.il[1]; il[2] = s.il[2]; }
-    if constexpr (FLAT) {
-        flat_pairs<HREP>(s_flat[threadIdx.x >> 5], cur, v, s_rc2, s_ft, a.tab, threadIdx.x & 31, i, xi, ti, s, cnt,
-                         q0, q1, acc);
-    }
     // the partners in groups of 4: all their positions are requested before
     // the first pair is evaluated
     constexpr int LCHUNK = 4;
-    for (int k0 = 0; k0 < (FLAT ? 0 : cnt); k0 += LCHUNK) {
-        const int4 q = k0 == 0 ? q0 : (k0 == 4 ? q1 : __ldg(nb4 + (long long)(k0 >> 2) * v.stride));
-        int jj[LCHUNK] = {q.x, q.y, q.z, q.w};
+    for (int k0 = 0; k0 < cnt; k0 += LCHUNK) {
+        const int gi = NARROW ? (k0 >> 3) : (k0 >> 2);
+        const int4 q = gi == 0 ? q0 : ((gi == 1 && !NARROW) ? q1 : __ldg(nb4 + (long long)gi * v.stride));
+        int jj[LCHUNK];
+        chunk_entries<NARROW>(q, k0, i, jj);
 #pragma unroll
         for (int u = 0; u < LCHUNK; ++u) jj[u] = (k0 + u < cnt) ? jj[u] : -1;
         R xj[LCHUNK][3];
@@ -1895,13 +1908,11 @@ __global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? 1024 : 768) / BLOCK) 
         bd_normals(s.seed, t, (long long)id, xn);
     }
     const int ef = em_update(xi, c, wi, F, xn, a.tab->a[ti], a.tab->b[ti], s);
-    // displacement since the build, minimum image
-    const float d0 = mimg((float)xi[0], xr.x, s.Lf[0], s.halff[0], p0);
-    const float d1 = mimg((float)xi[1], xr.y, s.Lf[1], s.halff[1], p1);
-    const float d2 = mimg((float)xi[2], xr.z, s.Lf[2], s.halff[2], p2);
-    const float dd = d0 * d0 + d1 * d1 + d2 * d2;
-    if (valid && dd > v.cap2) *((volatile int*)&v.ctl->need) = 1;
-    const bool hot = valid && dd > v.thr2;
+    // displacement since the build (lattice estimate; the thresholds
+    // allow for its error)
+    const float dd = head_disp2(hd, xi, s);
+    if (dd > v.cap2) *((volatile int*)&v.ctl->need) = 1;
+    const bool hot = dd > v.thr2;
     const unsigned act = __activemask();
     const unsigned hm = __ballot_sync(act, hot);
     if (hm) {
@@ -1912,7 +1923,6 @@ __global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? 1024 : 768) / BLOCK) 
         base = __shfl_sync(act, base, lead) + __popc(hm & ((1u << lane) - 1u));
         if (hot && base < v.hot_max) v.hot[base] = i;
     }
-    if (!valid) return;
     store_state(nxt, i, xi, wi, c, id);
     if (ef) {
         atomicOr(a.err, ef);
@@ -1964,11 +1974,30 @@ __global__ void list_scatter_kernel(Args<R> a, ListArgs<R> v, long long off)
     }
 }
 
+// writes the entries of one particle's list (list_entry's layouts); an
+// offset that 16 bits cannot hold marks the build as needing wide entries
+struct ListWriter {
+    int4* nbr;
+    long long stride;
+    int i, cap;
+    bool narrow, wide_need;
+    __device__ __forceinline__ void put(int k, int j)
+    {
+        if (k >= cap) return;
+        if (narrow) {
+            const int d = j - i;
+            if (d < -32768 || d > 32767) { wide_need = true; return; }
+            reinterpret_cast<short*>(nbr + (long long)(k >> 3) * stride + i)[k & 7] = (short)d;
+        } else {
+            reinterpret_cast<int*>(nbr + (long long)(k >> 2) * stride + i)[k & 3] = j;
+        }
+    }
+};
+
 // appends the pairs of one candidate range closer than their list radius
 template <class R>
 __device__ __forceinline__ void list_range(const State<R>& st, int j0, int j1, int self, const R xi[3], R sx, R sy,
-                                           R sz, const R* __restrict__ rl2, int* __restrict__ nb, long long stride4,
-                                           int cap, int& cnt)
+                                           R sz, const R* __restrict__ rl2, ListWriter& lw, int& cnt)
 {
     for (int j = j0; j < j1; ++j) {
         R xj[3];
@@ -1978,7 +2007,7 @@ __device__ __forceinline__ void list_range(const State<R>& st, int j0, int j1, i
         const R dy = sub_rn(xi[1], add_rn(xj[1], sy));
         const R dz = sub_rn(xi[2], add_rn(xj[2], sz));
         if (dist2(dx, dy, dz) < rl2[wj & 0xff] && j != self) {
-            if (cnt < cap) nb[(long long)(cnt >> 2) * stride4 + (cnt & 3)] = j;
+            lw.put(cnt, j);
             ++cnt;
         }
     }
@@ -2060,8 +2089,13 @@ __device__ __forceinline__ void list_build_one(const Args<R>& a, const ListArgs<
     int wi;
     load_pos(st, i, xi, wi);
     const R* rl2 = s_rl2 + (wi & 0xff) * MAXT;
-    int* nb = v.nbr + 4LL * i;
-    const long long stride4 = 4 * v.stride;
+    ListWriter lw;
+    lw.nbr = v.nbr;
+    lw.stride = v.stride;
+    lw.i = i;
+    lw.cap = v.cap;
+    lw.narrow = v.narrow != 0;
+    lw.wide_need = false;
     int cnt = 0;
     ListCell<R> g;
     g.locate(s, xi);
@@ -2069,12 +2103,12 @@ __device__ __forceinline__ void list_build_one(const Args<R>& a, const ListArgs<
     for (int dz = -1; dz <= 1; ++dz)
         for (int dy = -1; dy <= 1; ++dy)
             list_row_ranges<R>(a, s, g, lim, dz, dy, [&](int j0, int j1, R sx, R sy, R sz) {
-                list_range<R>(st, j0, j1, i, xi, sx, sy, sz, rl2, nb, stride4, v.cap, cnt);
+                list_range<R>(st, j0, j1, i, xi, sx, sy, sz, rl2, lw, cnt);
             });
-    v.xref[i] = make_float4((float)xi[0], (float)xi[1], (float)xi[2], __int_as_float(min(cnt, v.cap)));
-    if (cnt > v.cap) {
-        atomicMax(&v.ctl->maxcnt, cnt);
-        atomicOr(a.err, EF_LISTOVF);
+    v.head[i] = make_head(xi, s, min(cnt, v.cap));
+    if (cnt > v.cap || lw.wide_need) {
+        if (cnt > v.cap) atomicMax(&v.ctl->maxcnt, cnt);
+        atomicOr(a.err, (cnt > v.cap ? EF_LISTOVF : 0) | (lw.wide_need ? EF_LISTWIDE : 0));
         atomicMin((unsigned long long*)a.err_step, (unsigned long long)(*a.step_ptr + off));
     }
 }
@@ -2102,12 +2136,13 @@ __global__ void __launch_bounds__(BLOCK) list_build_kernel(Args<R> a, ListArgs<R
 template <class R>
 __device__ __forceinline__ bool listed(const ListArgs<R>& v, int i, int j)
 {
-    const int cnt = __float_as_int(__ldg(&v.xref[i].w));
-    const int4* nb4 = reinterpret_cast<const int4*>(v.nbr) + i;
-    for (int k0 = 0; k0 < cnt; k0 += 4) {
-        const int4 q = __ldg(nb4 + (long long)(k0 >> 2) * v.stride);
-        if (q.x == j || (k0 + 1 < cnt && q.y == j) || (k0 + 2 < cnt && q.z == j) || (k0 + 3 < cnt && q.w == j))
-            return true;
+    const int cnt = head_count(__ldg(v.head + i));
+    const int4* nb4 = v.nbr + i;
+    const int epg = v.narrow ? 8 : 4;
+    for (int k0 = 0; k0 < cnt; k0 += epg) {
+        const int4 q = __ldg(nb4 + (long long)(k0 / epg) * v.stride);
+        for (int u = 0; u < epg && k0 + u < cnt; ++u)
+            if (list_entry(q, u, v.narrow != 0, i) == j) return true;
     }
     return false;
 }

@@ -215,4 +215,5 @@ class Engine:
         S = self.system.n_types
         return {"energy": m.energy, "msd": list(m.msd[:S]), "count": list(m.count[:S]),
                 "step": m.step, "neighbour_mode": {A.NB_CELLS: "cells", A.NB_LIST: "list"}.get(m.neighbour_mode),
-                "list_builds": m.list_builds, "skin": m.skin, "list_capacity": m.list_capacity}
+                "list_builds": m.list_builds, "skin": m.skin, "list_capacity": m.list_capacity,
+                "list_entry_bytes": m.list_entry_bytes}

@@ -165,7 +165,13 @@ def long_run(w, steps, samples=100, seed=1, rdf_bins=150, rdf_rmax=15.0, equil=0
     * D = MSD / 6t per species at the first sample and at the end:
       |D32 - D64| <= 3 sqrt(se32^2 + se64^2) (standard errors over
       particles);
-    * RDF: per bin |c32 - c64| <= 3 sqrt(c32 + c64) + 1 (counting error).
+    * RDF: the per-frame counts of every bin, averaged in blocks of frames;
+      chi2 / dof = mean over bins of (m32 - m64)^2 / (se32^2 + se64^2) (block
+      standard errors, bins with counts) <= 1.5.  Under the hypothesis
+      that both runs sample the same distribution, with 10 blocks, chi2 / dof
+      is 1.29 on average (t statistics with 9 degrees of freedom) and 1.5 is
+      more than 3 standard deviations above that for >= 100 bins; the
+      largest |z| of a single bin is reported too.
     """
     x0 = snap_to_f32(w)
     every = max(1, steps // samples)
@@ -178,9 +184,8 @@ def long_run(w, steps, samples=100, seed=1, rdf_bins=150, rdf_rmax=15.0, equil=0
     probe = {prec: _engine(w, prec, seed) for prec in ("f32c", "f64")}
     rec = {p: {"t": [], "E": [], "msd": [], "msd_se": []} for p in eng}
     ferr = []
-    ufirst = {}
     done = 0
-    rdf_counts = {}
+    rdf_frames = {p: [] for p in eng}
     try:
         while done < steps:
             n = min(every, steps - done)
@@ -202,8 +207,8 @@ def long_run(w, steps, samples=100, seed=1, rdf_bins=150, rdf_rmax=15.0, equil=0
                                    for t in range(S)])
                 r = rec[prec]
                 r["t"].append(done); r["E"].append(m["energy"]); r["msd"].append(msd); r["msd_se"].append(se)
-                c, _ = e.rdf(rdf_bins, rdf_rmax, accumulate=True)
-                rdf_counts[prec] = c
+                c, _ = e.rdf(rdf_bins, rdf_rmax, accumulate=False)
+                rdf_frames[prec].append(c.reshape(-1).astype(np.float64))
                 if prec == "f32c":
                     xs = xe
             # force error on the FP32C run's current positions
@@ -239,12 +244,24 @@ def long_run(w, steps, samples=100, seed=1, rdf_bins=150, rdf_rmax=15.0, equil=0
         out[f"D_{tag}_abs_dev"] = [float(v) for v in np.abs(D["f32c"] - D["f64"])]
         out[f"D_{tag}_bound_3sigma"] = [float(v) for v in 3.0 * np.hypot(se["f32c"], se["f64"])]
         out[f"D_{tag}_rel_dev"] = [float(v) for v in np.abs(D["f32c"] - D["f64"]) / np.maximum(np.abs(D["f64"]), 1e-300)]
-    c32 = rdf_counts["f32c"].astype(np.float64).reshape(-1)
-    c64 = rdf_counts["f64"].astype(np.float64).reshape(-1)
     out["rdf_bins"] = rdf_bins
     out["rdf_rmax_nm"] = rdf_rmax
-    out["rdf_pairs_counted"] = float(c64.sum())
-    out["rdf_max_dev_over_bound"] = float(np.max(np.abs(c32 - c64) / (3.0 * np.sqrt(c32 + c64) + 1.0)))
+    out["rdf_pairs_counted"] = float(np.sum(rdf_frames["f64"]))
+    mb, sb = {}, {}
+    for prec in eng:
+        fr = np.array(rdf_frames[prec])
+        nb = max(2, min(10, len(fr)))
+        blocks = np.array([b.mean(axis=0) for b in np.array_split(fr, nb)])
+        mb[prec] = fr.mean(axis=0)
+        sb[prec] = blocks.std(axis=0, ddof=1) / np.sqrt(nb)
+    var = sb["f32c"] ** 2 + sb["f64"] ** 2
+    sel = var > 0
+    z2 = (mb["f32c"][sel] - mb["f64"][sel]) ** 2 / var[sel]
+    out["rdf_bins_compared"] = int(sel.sum())
+    out["rdf_chi2_per_dof"] = float(z2.mean()) if z2.size else 0.0
+    out["rdf_max_abs_z"] = float(np.sqrt(z2.max())) if z2.size else 0.0
+    both_zero = (~sel) & (mb["f32c"] != mb["f64"])
+    out["rdf_bins_differing_without_spread"] = int(both_zero.sum())
     return out
 
 

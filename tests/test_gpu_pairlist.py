@@ -281,3 +281,32 @@ def test_list_check_overflow_of_hot_particles_rebuilds(prec):
     assert out["list"][1]["neighbour_mode"] == "list"
     assert out["list"][1]["list_builds"] >= 2
     same(prec, out["cells"][0], out["list"][0])
+
+
+@pytest.mark.parametrize("prec", ["f32c", "f64"])
+def test_wide_list_entries_when_offsets_exceed_16_bits(prec):
+    """A thin slab of 200,000 particles (4 cell layers of 50,000) whose
+    z-neighbour cells lie more than 32767 sorted places apart: the first
+    build finds an offset that 16 bits cannot hold and the handle switches to
+    32-bit list entries; the trajectory is still the cell walk's (bit for bit
+    in FP32C)."""
+    rng = np.random.default_rng(4)
+    n = 200_000
+    sys_ = System([ParticleType("A", 1e6, 1.0)], pair=[PairPotential(A.P2_HARMONIC, [(0, 0)], 10.0, "repulsive")],
+                  kT=2.437, dt=1e-9, lo=(0, 0, 0), hi=(600, 600, 12), periodic=(1, 1, 1))
+    xyz = rng.uniform((0, 0, 0), (600, 600, 12), (n, 3))
+    types = np.zeros(n, np.int32)
+    xc, _, _ = run(sys_, xyz, types, prec, 60, neighbour_mode="cells")
+    xl, _, ml = run(sys_, xyz, types, prec, 60, neighbour_mode="list", skin=1.0)
+    assert ml["neighbour_mode"] == "list" and ml["list_entry_bytes"] == 4
+    same(prec, xc, xl)
+
+
+def test_narrow_list_entries_by_default():
+    """Config 4's systems (at most 20,000 particles each) keep 16-bit entries."""
+    from readdygpu_b200 import configs
+    w = configs.config4(n_systems=12, nmin=200, nmax=3000)
+    with Engine(w.system, precision="f32c", boxes=w.boxes, neighbour_mode="list", skin=0.6) as e:
+        e.set_particles(w.xyz, w.types, offsets=w.offsets)
+        e.step(50)
+        assert e.metrics()["list_entry_bytes"] == 2
