@@ -1803,18 +1803,12 @@ template <class R> int rdf_fine(Engine* E, int nbins, double rmax)
 
 // The RDF frame on a grid of its own (rdf_tile_kernel), from the current
 // state in any order (no re-sort of the simulation's cells): cells of edge
-// >= rmax / 2 with a stencil of half-width 2 when every periodic axis of
-// every system has >= 5 of them, else cells of edge >= rmax with half-width
-// 1 (>= 3 cells).  Returns RDGPU_OK_CONTINUE when neither fits (rdf_fine
-// then takes the frame).
+// >= rmax.  Returns RDGPU_OK_CONTINUE when some system has fewer than 3 of
+// them along a periodic axis (rdf_fine then takes the frame).
 template <class R> int rdf_tiled(Engine* E, int nbins, double rmax)
 {
     const int S = E->desc.n_types;
     const int H = S * S * nbins;
-    int hw = 2;
-    for (int s = 0; s < E->nsys && hw == 2; ++s)
-        for (int a = 0; a < 3; ++a)
-            if (E->sys_h[s].per[a] && std::min(cells_along(edge(E, s, a), 0.5 * rmax), 512) < 5) hw = 1;
     std::vector<RdfGrid> gh(E->nsys);
     long long nc = 0;
     double lmax = 0.0;
@@ -1824,8 +1818,8 @@ template <class R> int rdf_tiled(Engine* E, int nbins, double rmax)
         long long m = 1;
         for (int a = 0; a < 3; ++a) {
             const double Lp = edge(E, s, a);
-            const int n = std::min(cells_along(Lp, rmax / hw), 256 * hw);
-            if (E->sys_h[s].per[a] && n < 2 * hw + 1) return RDGPU_OK_CONTINUE;
+            const int n = std::min(cells_along(Lp, rmax), 256);
+            if (E->sys_h[s].per[a] && n < 3) return RDGPU_OK_CONTINUE;
             g.n[a] = n;
             g.per[a] = E->sys_h[s].per[a];
             g.L[a] = Lp;
@@ -1872,13 +1866,26 @@ template <class R> int rdf_tiled(Engine* E, int nbins, double rmax)
     // coordinates (within a box length of the box) and of the distance
     const double rpre = rmax + 64.0 * std::ldexp(1.0, -24) * lmax;
     const float r2pre = (float)(rpre * rpre * (1.0 + 1e-5));
-    const size_t dyn = (size_t)(nbins + 1) * 8 + (size_t)H * 4;
-    const int use_smem = dyn <= 40 * 1024 ? 1 : 0;
-    const size_t smem = use_smem ? dyn : (size_t)(nbins + 1) * 8;
-    if (smem > 40 * 1024) return RDGPU_OK_CONTINUE;
+    // Bound on |FP32 r^2 - FP64 r^2| of a pair closer than the pre-selection
+    // radius (rdf_bin): each FP32 displacement is within eps of the exact one
+    // (the FP32 conversion of the two coordinates of an FP64 state, the
+    // shifted candidate and the difference, each within 2^-24 of values below
+    // 2 lmax + rmax), so r^2 within 2 sqrt(3) rmax eps + 3 eps^2; the FP32
+    // squares and sums, the FP32 bin edges and the comparisons round by
+    // 2^-24 rmax^2 each (8 allowed), the FP64 distance by 2^-53 rmax^2 each.
+    const double eps = std::ldexp(1.0, -24) * (3.0 * lmax + 4.0 * rmax) * 1.01;
+    const double rr = rpre;
+    const float dlt = (float)((2.0 * std::sqrt(3.0) * rr * eps + 3.0 * eps * eps +
+                               8.0 * std::ldexp(1.0, -24) * rr * rr + 8.0 * std::ldexp(1.0, -53) * rr * rr) *
+                              (1.0 + 1e-3));
+    const size_t edges = (size_t)(nbins + 1) * 8 + (size_t)((nbins + 2) & ~1) * 4;
+    const size_t dyn = edges + (size_t)H * 4;
+    const int use_smem = dyn <= 16 * 1024 ? 1 : 0;
+    const size_t smem = use_smem ? dyn : edges;
+    if (smem > 16 * 1024) return RDGPU_OK_CONTINUE;
     const int grid = (int)std::min<long long>((nc + RDF_WARPS - 1) / RDF_WARPS, 148LL * 8);
-    rdf_tile_kernel<R><<<grid, RDF_WARPS * 32, smem, E->stream>>>(E->rdf_grid_d, E->nsys, nc, hw, E->rdf_start, rec,
-                                                                  S, nbins, E->rdf_e2, rmax / (double)nbins, r2pre,
+    rdf_tile_kernel<R><<<grid, RDF_WARPS * 32, smem, E->stream>>>(E->rdf_grid_d, E->nsys, nc, E->rdf_start, rec, S,
+                                                                  nbins, E->rdf_e2, rmax / (double)nbins, r2pre, dlt,
                                                                   use_smem, E->rdf_tmp);
     CK(cudaGetLastError());
     return RDGPU_OK;

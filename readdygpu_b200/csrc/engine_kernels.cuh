@@ -1205,19 +1205,19 @@ __global__ void __launch_bounds__(128, 8) rdf_kernel(const SysDev* __restrict__ 
 // cells of edge >= rmax and at least 3 cells along every periodic axis, so
 // every pair closer than rmax sits in one cell or in two neighbouring ones,
 // and each unordered pair of neighbouring cells appears once among a cell's
-// 13 forward neighbours.  A warp takes one cell: its particles (up to 128 at
-// a time) and then the particles of each forward neighbour (and of the cell
-// itself, partners of higher index only), moved to their periodic image next
-// to the cell, go to per-warp shared memory.  The own x candidate tests are
-// spread over the lanes, consecutive tests on consecutive lanes, with an
-// FP32 distance that over-accepts (r2pre covers its rounding); each lane
-// collects its accepted tests of a window as bits, and one warp scan
-// compacts them into a queue.  Queued pairs are evaluated 32 at a time, one
-// per lane, with the exact FP64 predicate and bin rule of rdf_kernel: dx =
+// 13 forward neighbours.  A warp takes one cell: its particles (up to 96 at
+// a time) go to per-warp shared memory, and the candidates of the cell and
+// its forward neighbours (partners of higher index only in the cell itself),
+// moved to their periodic image next to the cell, are taken one per lane, 32
+// at a time, each tested against all own particles with an FP32 distance
+// that over-accepts (r2pre covers its rounding).  Each lane collects its
+// accepted tests of a window as bits, and one warp scan compacts them into a
+// queue.  Queued pairs are binned 32 at a time, one per lane (rdf_bin): by
+// the FP32 distance when it is farther than a stated bound from every bin
+// edge, else by the exact FP64 predicate and bin rule of rdf_kernel: dx =
 // (xi - xj) - sx, sx the periodic shift of the neighbour cell, which is the
 // symmetric minimum image (mimg_sym) for every pair closer than rmax < L/2.
 // Each pair is counted for both orientations, as in rdf_kernel.
-// ---------------------------------------------------------------------------
 struct RdfGrid {
     int n[3];
     int per[3];
@@ -1280,75 +1280,39 @@ __global__ void rdf_scatter_kernel(long long ntot, State<R> cur, const int* __re
 }
 
 constexpr int RDF_WARPS = 4;
-constexpr int RDF_OWN = 64;       // own particles per pass of a cell
-constexpr int RDF_WIN = 16;       // own particles tested per lane between two compactions
+constexpr int RDF_OWN = 96;       // own particles per pass of a cell
+constexpr int RDF_WIN = 8;        // own particles tested per lane between two compactions
 constexpr int RDF_QUEUE = 32 * RDF_WIN + 32;
-constexpr int RDF_NBMAX = 63;     // forward neighbours of a stencil of half-width 2, and the cell
+constexpr int RDF_NB = 14;        // the cell and its 13 forward neighbours
 
 // per-warp shared memory of rdf_tile_kernel
 struct RdfWarp {
     float4 own[RDF_OWN];          // own particles as floats, bits(type) in w
     double ox[3 * RDF_OWN];       // own particles as stored (widened FP32 or FP64)
-    int nbase[RDF_NBMAX];         // first candidate of each neighbour cell
-    int npre[RDF_NBMAX + 1];      // exclusive prefix of the neighbour cells' counts
-    int ncode[RDF_NBMAX];         // periodic shift code of each neighbour cell (2 bits per axis)
+    int nbase[RDF_NB];            // first candidate of each neighbour cell
+    int npre[RDF_NB + 1];         // exclusive prefix of the neighbour cells' counts
+    int ncode[RDF_NB];            // periodic shift code of each neighbour cell (2 bits per axis)
     int2 queue[RDF_QUEUE];        // accepted pairs: (candidate index, own | shift code << 8)
+    float qr2[RDF_QUEUE];         // their FP32 squared distance
 };
 
-// The q-th offset of the half-shell of a stencil of half-width hw (1 or 2):
-// offset 0 is the cell itself, then the offsets (dx, dy, dz) with dz > 0, or
-// dz == 0 and dy > 0, or dz == dy == 0 and dx > 0, in lexicographic order.
-__device__ __forceinline__ void rdf_offset(int q, int hw, int d[3])
+// offset q of the half-shell: the cell itself, then the 13 offsets (dx, dy,
+// dz) with dz > 0, or dz == 0 and dy > 0, or dz == dy == 0 and dx > 0
+__device__ __forceinline__ void rdf_offset(int q, int d[3])
 {
     if (q == 0) { d[0] = d[1] = d[2] = 0; return; }
-    const int w = 2 * hw + 1;
-    // offsets with dz == dy == 0, dx > 0: hw of them; then dz == 0, dy > 0:
-    // hw * w; then dz > 0: hw * w * w
-    int k = q - 1;
-    if (k < hw) { d[0] = 1 + k; d[1] = 0; d[2] = 0; return; }
-    k -= hw;
-    if (k < hw * w) { d[2] = 0; d[1] = 1 + k / w; d[0] = k % w - hw; return; }
-    k -= hw * w;
-    d[2] = 1 + k / (w * w);
-    k %= w * w;
-    d[1] = k / w - hw;
-    d[0] = k % w - hw;
+    if (q == 1) { d[0] = 1; d[1] = 0; d[2] = 0; return; }
+    if (q < 5) { d[2] = 0; d[1] = 1; d[0] = q - 3; return; }
+    const int k = q - 5;
+    d[2] = 1;
+    d[1] = k / 3 - 1;
+    d[0] = k % 3 - 1;
 }
 
-// the exact FP64 predicate and bin of one queued pair (rdf_kernel's rule)
 template <class R>
-__device__ __forceinline__ void rdf_exact(const RdfWarp& w, const RdfRec<R>* __restrict__ rec, int2 e,
-                                          const RdfGrid& g, int S, int nbins, double rmax2, float inv_wf,
-                                          const double* __restrict__ e2s, int use_smem, unsigned* __restrict__ sh,
-                                          unsigned long long* __restrict__ hist)
+__device__ __forceinline__ void rdf_count(int ti, int tj, int k, int S, int nbins, int use_smem,
+                                          unsigned* __restrict__ sh, unsigned long long* __restrict__ hist)
 {
-    const int o = e.y & 0xff, code = e.y >> 8;
-    double xj[3];
-    int tj;
-    if constexpr (sizeof(R) == 4) {
-        const float4 p = __ldg(&rec[e.x].p);
-        xj[0] = p.x; xj[1] = p.y; xj[2] = p.z;
-        tj = __float_as_int(p.w);
-    } else {
-        const RdfRec<double> q = rec[e.x];
-        xj[0] = q.x; xj[1] = q.y; xj[2] = q.z;
-        tj = q.t;
-    }
-    double d[3];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const int sc = (code >> (2 * a)) & 3;
-        const double sx = sc == 1 ? g.L[a] : (sc == 2 ? -g.L[a] : 0.0);
-        d[a] = sub_rn(sub_rn(w.ox[3 * o + a], xj[a]), sx);
-    }
-    const double r2 = dist2(d[0], d[1], d[2]);
-    if (!(r2 < rmax2)) return;
-    const float r2f = (float)r2;
-    int k = r2f > 0.0f ? (int)(r2f * rsqrtf(r2f) * inv_wf) : 0;
-    k = min(max(k, 0), nbins - 1);
-    while (k > 0 && e2s[k] > r2) --k;
-    while (k < nbins - 1 && e2s[k + 1] <= r2) ++k;
-    const int ti = __float_as_int(w.own[o].w);
     const int h1 = (ti * S + tj) * nbins + k, h2 = (tj * S + ti) * nbins + k;
     if (use_smem) {
         if (h1 == h2) atomicAdd(sh + h1, 2u);
@@ -1359,20 +1323,69 @@ __device__ __forceinline__ void rdf_exact(const RdfWarp& w, const RdfRec<R>* __r
     }
 }
 
+// Bins one queued pair.  The FP64 squared distance r2 of rdf_kernel's rule
+// lies within dlt of the FP32 one (dlt covers the FP32 rounding of the
+// coordinates, the periodic shift, the distance and the FP32 bin edges
+// e2f): when r2f +- dlt falls inside one bin, that is r2's bin; otherwise
+// the FP64 predicate decides from the stored coordinates.
+template <class R>
+__device__ __forceinline__ void rdf_bin(const RdfWarp& w, const RdfRec<R>* __restrict__ rec, int2 e, float r2f,
+                                        float dlt, const RdfGrid& g, int S, int nbins, double rmax2, float inv_wf,
+                                        const double* __restrict__ e2s, const float* __restrict__ e2f,
+                                        int use_smem, unsigned* __restrict__ sh, unsigned long long* __restrict__ hist)
+{
+    const int o = e.y & 0xff, code = e.y >> 8;
+    if (r2f - dlt >= e2f[nbins]) return;                  // beyond rmax
+    int k = r2f > 0.0f ? (int)(r2f * rsqrtf(r2f) * inv_wf) : 0;
+    k = min(max(k, 0), nbins - 1);
+    const int ti = __float_as_int(w.own[o].w);
+    int tj;
+    if constexpr (sizeof(R) == 4) tj = __float_as_int(__ldg(&rec[e.x].p.w));
+    else tj = __ldg(&rec[e.x].t);
+    if (r2f - dlt >= e2f[k] && r2f + dlt < e2f[k + 1]) {
+        rdf_count<R>(ti, tj, k, S, nbins, use_smem, sh, hist);
+        return;
+    }
+    double xj[3];
+    if constexpr (sizeof(R) == 4) {
+        const float4 p = __ldg(&rec[e.x].p);
+        xj[0] = p.x; xj[1] = p.y; xj[2] = p.z;
+    } else {
+        const RdfRec<double> q = rec[e.x];
+        xj[0] = q.x; xj[1] = q.y; xj[2] = q.z;
+    }
+    double d[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int sc = (code >> (2 * a)) & 3;
+        const double sx = sc == 1 ? g.L[a] : (sc == 2 ? -g.L[a] : 0.0);
+        d[a] = sub_rn(sub_rn(w.ox[3 * o + a], xj[a]), sx);
+    }
+    const double r2 = dist2(d[0], d[1], d[2]);
+    if (!(r2 < rmax2)) return;
+    while (k > 0 && e2s[k] > r2) --k;
+    while (k < nbins - 1 && e2s[k + 1] <= r2) ++k;
+    rdf_count<R>(ti, tj, k, S, nbins, use_smem, sh, hist);
+}
+
 template <class R>
 __global__ void __launch_bounds__(RDF_WARPS * 32) rdf_tile_kernel(const RdfGrid* __restrict__ grids, int nsys,
-        long long ncells, int hw, const int* __restrict__ start, const RdfRec<R>* __restrict__ rec, int S,
-        int nbins, const double* __restrict__ e2, double w, float r2pre, int use_smem,
+        long long ncells, const int* __restrict__ start, const RdfRec<R>* __restrict__ rec, int S, int nbins,
+        const double* __restrict__ e2, double w, float r2pre, float dlt, int use_smem,
         unsigned long long* __restrict__ hist)
 {
-    // shared memory: the warps' RdfWarp, then the squared bin edges and,
-    // with use_smem, the block's histogram
+    // shared memory: the warps' RdfWarp, then the squared bin edges (FP64,
+    // then FP32) and, with use_smem, the block's histogram
     __shared__ RdfWarp s_w[RDF_WARPS];
     extern __shared__ double s_dyn[];
     double* e2s = s_dyn;
-    unsigned* sh = reinterpret_cast<unsigned*>(s_dyn + nbins + 1);
+    float* e2f = reinterpret_cast<float*>(s_dyn + nbins + 1);
+    unsigned* sh = reinterpret_cast<unsigned*>(e2f + ((nbins + 2) & ~1));
     const int H = S * S * nbins;
-    for (int k = threadIdx.x; k <= nbins; k += blockDim.x) e2s[k] = e2[k];
+    for (int k = threadIdx.x; k <= nbins; k += blockDim.x) {
+        e2s[k] = e2[k];
+        e2f[k] = (float)e2[k];
+    }
     if (use_smem)
         for (int k = threadIdx.x; k < H; k += blockDim.x) sh[k] = 0;
     __syncthreads();
@@ -1380,8 +1393,6 @@ __global__ void __launch_bounds__(RDF_WARPS * 32) rdf_tile_kernel(const RdfGrid*
     RdfWarp& W = s_w[wp];
     const double rmax2 = e2[nbins];
     const float inv_wf = (float)(1.0 / w);
-    const int wd = 2 * hw + 1;
-    const int nnb = 1 + (wd * wd * wd - 1) / 2;
     for (long long c = (long long)blockIdx.x * RDF_WARPS + wp; c < ncells; c += (long long)gridDim.x * RDF_WARPS) {
         const int a0 = start[c], a1 = start[c + 1];
         if (a0 == a1) continue;
@@ -1397,47 +1408,42 @@ __global__ void __launch_bounds__(RDF_WARPS * 32) rdf_tile_kernel(const RdfGrid*
         // the neighbour cells: first candidate, count (0 beyond an open
         // bound) and periodic shift code; exclusive prefix of the counts
         __syncwarp();
-        int run = 0;
-        for (int q0 = 0; q0 < nnb; q0 += 32) {
-            const int q = q0 + lane;
-            int cnt = 0, base = 0, code = 0;
-            if (q < nnb) {
-                int d[3];
-                rdf_offset(q, hw, d);
-                bool skip = false;
-                int z[3];
+        int cnt = 0;
+        if (lane < RDF_NB) {
+            int d[3], z[3];
+            int code = 0, base = 0;
+            bool skip = false;
+            rdf_offset(lane, d);
 #pragma unroll
-                for (int ax = 0; ax < 3; ++ax) {
-                    z[ax] = cc[ax] + d[ax];
-                    if (z[ax] < 0) {
-                        if (!g.per[ax]) skip = true;
-                        z[ax] += g.n[ax];
-                        code |= 2 << (2 * ax);
-                    } else if (z[ax] >= g.n[ax]) {
-                        if (!g.per[ax]) skip = true;
-                        z[ax] -= g.n[ax];
-                        code |= 1 << (2 * ax);
-                    }
+            for (int ax = 0; ax < 3; ++ax) {
+                z[ax] = cc[ax] + d[ax];
+                if (z[ax] < 0) {
+                    if (!g.per[ax]) skip = true;
+                    z[ax] += g.n[ax];
+                    code |= 2 << (2 * ax);
+                } else if (z[ax] >= g.n[ax]) {
+                    if (!g.per[ax]) skip = true;
+                    z[ax] -= g.n[ax];
+                    code |= 1 << (2 * ax);
                 }
-                if (!skip) {
-                    const long long nc = g.base + ((long long)z[2] * g.n[1] + z[1]) * g.n[0] + z[0];
-                    base = start[nc];
-                    cnt = start[nc + 1] - base;
-                }
-                W.nbase[q] = base;
-                W.ncode[q] = code;
             }
-            int incl = cnt;
-#pragma unroll
-            for (int sft = 1; sft < 32; sft <<= 1) {
-                const int t = __shfl_up_sync(FULL, incl, sft);
-                if (lane >= sft) incl += t;
+            if (!skip) {
+                const long long nc = g.base + ((long long)z[2] * g.n[1] + z[1]) * g.n[0] + z[0];
+                base = start[nc];
+                cnt = start[nc + 1] - base;
             }
-            if (q < nnb) W.npre[q] = run + incl - cnt;
-            run += __shfl_sync(FULL, incl, 31);
+            W.nbase[lane] = base;
+            W.ncode[lane] = code;
         }
-        if (lane == 0) W.npre[nnb] = run;
-        const int C = run;     // candidates of all neighbour cells
+        int incl = cnt;
+#pragma unroll
+        for (int sft = 1; sft < 32; sft <<= 1) {
+            const int t = __shfl_up_sync(FULL, incl, sft);
+            if (lane >= sft) incl += t;
+        }
+        if (lane < RDF_NB) W.npre[lane] = incl - cnt;
+        const int C = __shfl_sync(FULL, incl, RDF_NB - 1);     // candidates of all neighbour cells
+        if (lane == 0) W.npre[RDF_NB] = C;
         for (int ob = a0; ob < a1; ob += RDF_OWN) {
             const int m = min(RDF_OWN, a1 - ob);
             __syncwarp();
@@ -1461,17 +1467,15 @@ __global__ void __launch_bounds__(RDF_WARPS * 32) rdf_tile_kernel(const RdfGrid*
             // one candidate per lane, 32 at a time over all neighbour cells
             for (int cb = 0; cb < C; cb += 32) {
                 const int t = cb + lane;
-                const bool have = t < C;
                 // its neighbour cell: the last q with npre[q] <= t
-                int ql = 0, qh = nnb - 1;
-                while (ql < qh) {
-                    const int mid = (ql + qh + 1) >> 1;
-                    if (W.npre[mid] <= t) ql = mid; else qh = mid - 1;
-                }
+                int ql = 0;
+#pragma unroll
+                for (int step = 8; step > 0; step >>= 1)
+                    if (ql + step < RDF_NB && W.npre[ql + step] <= t) ql += step;
                 const int j = W.nbase[ql] + (t - W.npre[ql]);
                 const int code = W.ncode[ql];
                 float cx = 3e30f, cy = 3e30f, cz = 3e30f;     // no candidate: never accepted
-                if (have) {
+                if (t < C) {
                     float4 p;
                     if constexpr (sizeof(R) == 4) {
                         p = __ldg(&rec[j].p);
@@ -1485,45 +1489,56 @@ __global__ void __launch_bounds__(RDF_WARPS * 32) rdf_tile_kernel(const RdfGrid*
                     cy = p.y + (s1 == 1 ? (float)g.L[1] : (s1 == 2 ? -(float)g.L[1] : 0.f));
                     cz = p.z + (s2 == 1 ? (float)g.L[2] : (s2 == 2 ? -(float)g.L[2] : 0.f));
                 }
-                // partners in the own cell itself (q == 0) count from a higher index only
+                // partners in the own cell itself (ql == 0) count from a higher index only
                 const int jmin = ql == 0 ? j - ob : RDF_OWN;   // own o tests j only when o < j - ob
                 for (int o0 = 0; o0 < m; o0 += RDF_WIN) {
                     unsigned bits = 0;
+                    float r2k[RDF_WIN];
+                    const int nw = min(RDF_WIN, m - o0);
 #pragma unroll
                     for (int it = 0; it < RDF_WIN; ++it) {
-                        const int o = o0 + it;
-                        if (o < m) {
+                        r2k[it] = 0.f;
+                        if (it < nw) {
+                            const int o = o0 + it;
                             const float4 a = W.own[o];
                             const float dx = a.x - cx, dy = a.y - cy, dz = a.z - cz;
                             const float r2f = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+                            r2k[it] = r2f;
                             const bool acc = r2f < r2pre && o < jmin;
                             bits |= (unsigned)acc << it;
                         }
                     }
                     const int cntl = __popc(bits);
-                    int incl = cntl;
+                    int inc2 = cntl;
 #pragma unroll
                     for (int sft = 1; sft < 32; sft <<= 1) {
-                        const int tt = __shfl_up_sync(FULL, incl, sft);
-                        if (lane >= sft) incl += tt;
+                        const int tt = __shfl_up_sync(FULL, inc2, sft);
+                        if (lane >= sft) inc2 += tt;
                     }
-                    const int tot = __shfl_sync(FULL, incl, 31);
+                    const int tot = __shfl_sync(FULL, inc2, 31);
                     if (tot == 0) continue;
-                    int slot = qn + incl - cntl;
-                    while (bits) {
-                        const int it = __ffs(bits) - 1;
-                        bits &= bits - 1;
-                        W.queue[slot++] = make_int2(j, (o0 + it) | (code << 8));
+                    int slot = qn + inc2 - cntl;
+#pragma unroll
+                    for (int it = 0; it < RDF_WIN; ++it) {
+                        if ((bits >> it) & 1u) {
+                            W.queue[slot] = make_int2(j, (o0 + it) | (code << 8));
+                            W.qr2[slot] = r2k[it];
+                            ++slot;
+                        }
                     }
                     qn += tot;
                     __syncwarp();
-                    // evaluate full batches of 32
+                    // bin full batches of 32
                     int done = 0;
                     for (; done + 32 <= qn; done += 32)
-                        rdf_exact<R>(W, rec, W.queue[done + lane], g, S, nbins, rmax2, inv_wf, e2s, use_smem, sh, hist);
+                        rdf_bin<R>(W, rec, W.queue[done + lane], W.qr2[done + lane], dlt, g, S, nbins, rmax2, inv_wf,
+                                   e2s, e2f, use_smem, sh, hist);
                     __syncwarp();
                     if (done > 0) {
-                        if (lane < qn - done) W.queue[lane] = W.queue[done + lane];
+                        if (lane < qn - done) {
+                            W.queue[lane] = W.queue[done + lane];
+                            W.qr2[lane] = W.qr2[done + lane];
+                        }
                         qn -= done;
                         __syncwarp();
                     }
@@ -1531,7 +1546,9 @@ __global__ void __launch_bounds__(RDF_WARPS * 32) rdf_tile_kernel(const RdfGrid*
             }
             // what is left in the queue
             __syncwarp();
-            if (lane < qn) rdf_exact<R>(W, rec, W.queue[lane], g, S, nbins, rmax2, inv_wf, e2s, use_smem, sh, hist);
+            if (lane < qn)
+                rdf_bin<R>(W, rec, W.queue[lane], W.qr2[lane], dlt, g, S, nbins, rmax2, inv_wf, e2s, e2f, use_smem, sh,
+                           hist);
         }
     }
     if (use_smem) {
