@@ -107,3 +107,24 @@ def test_full_size_neighbours_and_forces_against_oracle(oracle, cfg, prec):
         rms = np.sqrt(np.mean(mag ** 2))
         assert np.all(per <= 1e-4 * np.maximum(mag, rms)), (per / np.maximum(mag, rms)).max()
         assert abs(E - Eo) <= 1e-5 * max(1.0, abs(Eo)), (E, Eo)
+
+
+@pytest.mark.parametrize("mode", ["cells", "list"])
+def test_config3_rdf_frames_over_a_run(oracle, mode):
+    """Config 3's RDF (200 bins over 0-20 nm) at every 100th step of a
+    1,000-step FP64 run on 100,000 RSA spheres: each frame's counts equal the
+    oracle's counts of the positions the engine holds at that step, bit for
+    bit.  (FP64 only: the FP32C engine bins its stored FP32 coordinates,
+    which a download returns compensated; its frames are checked at upload
+    in test_config3_rdf_full_size_bit_exact.)"""
+    w = configs.config3(n=100_000)
+    d = w.system.to_desc()
+    with Engine(w.system, precision="f64", seed=9, neighbour_mode=mode, skin=1.0) as e:
+        e.set_particles(w.xyz, w.types)
+        for frame in range(10):
+            e.step(100)
+            c, _ = e.rdf(200, 20.0, accumulate=False)
+            x, _ = e.get_particles()
+            co = oracle.rdf_counts(d, oracle.to_rel_f64(d, x).reshape(-1, 3), w.types, 200, 20.0)
+            assert np.array_equal(c.reshape(-1), co), (frame, int(np.abs(c.reshape(-1).astype(np.int64) - co.astype(np.int64)).max()))
+        assert e.metrics()["step"] == 1000
