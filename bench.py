@@ -194,8 +194,9 @@ def cpu_baseline(w, budget_s=12.0, threads=None):
 
 def rdf_frames(eng, nbins=200, rmax=20.0, frames=5, every=100):
     """The RDF of config 3 (200 bins over 0-20 nm, one frame every 100 steps)
-    through the C ABI: re-sort on fresh cells, histogram kernel, counts to the
-    host; wall time of whole synchronous calls after one untimed frame."""
+    through the C ABI: the particles sorted into the RDF's grid, histogram
+    kernel, counts to the host; wall time of whole synchronous calls after one
+    untimed frame."""
     eng.rdf(nbins, rmax)
     t0 = time.perf_counter()
     for _ in range(frames):
@@ -203,7 +204,7 @@ def rdf_frames(eng, nbins=200, rmax=20.0, frames=5, every=100):
     ms = (time.perf_counter() - t0) * 1e3 / frames
     return {"bins": nbins, "rmax_nm": rmax, "every_steps": every, "ms_per_frame": ms,
             "ms_per_step_amortized": ms / every,
-            "note": "rdgpu_rdf: re-sort and list build, rdf_kernel, uint64 counts to the host"}
+            "note": "rdgpu_rdf: particles sorted into the RDF grid, rdf_tile_kernel, uint64 counts to the host"}
 
 
 def host_cpu_model():

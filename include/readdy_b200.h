@@ -278,7 +278,11 @@ int rdgpu_debug_noise(rdgpu_handle h, int64_t step, double* noise);
    increment of [ti][tj] and [tj][ti] (CudaSimulation.cu:1815-1818).
    accumulate != 0 adds to the device accumulator (one "frame"); the host
    array then receives the accumulated counts; accumulate == 0 returns only
-   this frame's counts and leaves the accumulator alone.                      */
+   this frame's counts and leaves the accumulator alone.  The frame sorts
+   copies of the particles into a grid of its own (cells of edge >= rmax)
+   and leaves the simulation's state and lists as they are; when a periodic
+   box edge holds fewer than 3 such cells it re-sorts the simulation's
+   particles on their own cells instead (a list build in pair-list mode).    */
 int rdgpu_rdf(rdgpu_handle h, int32_t nbins, double rmax, int32_t accumulate,
               uint64_t* counts, int64_t* frames);
 
