@@ -60,7 +60,8 @@ struct rdgpu_engine {
     // particles
     long long npart_tot = 0, cap_particles = 0;
     std::vector<long long> part_off;     // n_sys + 1
-    std::vector<int> types_h;            // by global index
+    std::vector<int> types_h;            // by global index (host copy, see sync_types)
+    bool types_h_valid = false;          // types_h matches the device state
     void* bufA[2] = {nullptr, nullptr};  // two state buffers; FP32: pos, FP64: records
     void* bufB[2] = {nullptr, nullptr};  // FP32: aux
     int cur = 0;                         // the buffer that holds the current state
@@ -154,6 +155,8 @@ struct rdgpu_engine {
 namespace {
 
 using Engine = rdgpu_engine;
+
+template <class R> int sync_types(Engine* E);
 
 #define CK(call)                                                                   \
     do {                                                                           \
@@ -1385,6 +1388,10 @@ template <class R> int upload_bonds(Engine* E)
     free_bonds(E);
     const long long nb = (long long)E->bond_pot_h.size();
     if (nb == 0 || E->npart_tot == 0) return RDGPU_OK;
+    {
+        const int rc = sync_types<R>(E);
+        if (rc) return rc;
+    }
     const long long N = E->npart_tot;
     const int M = RDGPU_MAX_TYPES;
     std::vector<int> start(N + 1, 0), part(2 * nb), term(2 * nb);
@@ -1513,8 +1520,17 @@ template <class R, class In> int set_particles_impl(Engine* E, const long long* 
             return fail(E, RDGPU_ERR_ARG, "particle type out of range, non-finite coordinate, or a coordinate "
                                           "more than 64 box lengths outside the box");
     }
-    E->types_h.assign(types, types + ntot);
-    launch_sort<R>(E);
+    // the host copy of the types is downloaded when needed (sync_types)
+    E->types_h_valid = false;
+    const bool list_mode = E->nb_mode == RDGPU_NB_LIST && ntot > 0;
+    if (list_mode) {
+        // the list re-sort below sorts the ingested particles itself: the
+        // staging buffer becomes the current state (its counts are cleared
+        // by prepare_step_state)
+        set_cur(E, E->cur ^ 1);
+    } else {
+        launch_sort<R>(E);
+    }
     CK(cudaGetLastError());
     E->rdf_frames = 0;
     if (E->rdf_acc && E->rdf_nbins > 0) {
@@ -1524,7 +1540,7 @@ template <class R, class In> int set_particles_impl(Engine* E, const long long* 
     rc = prepare_step_state(E, 0);
     if (rc) return rc;
     E->part_off = off;
-    if (E->nb_mode == RDGPU_NB_LIST && ntot > 0) {
+    if (list_mode) {
         rc = ensure_list(E, list_cap_estimate(E), E->list_wide);
         if (!rc) rc = resort<R>(E, true);
         if (rc) { E->part_off.clear(); return rc; }
@@ -1566,6 +1582,10 @@ template <class R> int grow_preserving(Engine* E, long long n)
 // the appended ones follow; ids are renumbered 0 .. n-1 in that order.
 template <class R> int apply_edits_impl(Engine* E, const float* ed, long long count)
 {
+    {
+        const int rc = sync_types<R>(E);
+        if (rc) return rc;
+    }
     const long long N = E->npart_tot;
     const int S = E->desc.n_types;
     std::vector<char> gone(std::max<long long>(N, 1), 0);
@@ -1663,6 +1683,7 @@ template <class R> int apply_edits_impl(Engine* E, const float* ed, long long co
         if (!gone[i]) nt.push_back(E->types_h[i]);
     for (int t : atype) nt.push_back(t);
     E->types_h.swap(nt);
+    E->types_h_valid = true;
     // bonds: those of deleted particles go, the rest follow the new ids
     if (!E->bond_pot_h.empty()) {
         std::vector<int> nid(std::max<long long>(N, 1), -1);
@@ -1702,6 +1723,20 @@ template <class R, class Out> int get_particles_impl(Engine* E, Out* xyz, int* t
     if (xyz) CK(cudaMemcpyAsync(xyz, E->vec_d, N * 3 * sizeof(Out), cudaMemcpyDeviceToHost, E->stream));
     if (types) CK(cudaMemcpyAsync(types, E->ityp_d, N * sizeof(int), cudaMemcpyDeviceToHost, E->stream));
     CK(cudaStreamSynchronize(E->stream));
+    return RDGPU_OK;
+}
+
+// the host copy of the types by global index, downloaded after an upload
+// (bonds, reaction edits and the RDF normalisation read it)
+template <class R> int sync_types(Engine* E)
+{
+    if (E->types_h_valid) return RDGPU_OK;
+    E->types_h.resize(E->npart_tot);
+    if (E->npart_tot > 0) {
+        const int rc = get_particles_impl<R, double>(E, nullptr, E->types_h.data());
+        if (rc) return rc;
+    }
+    E->types_h_valid = true;
     return RDGPU_OK;
 }
 
@@ -2273,6 +2308,8 @@ int rdgpu_rdf_normalized(rdgpu_handle h, double* g)
     if (E->nsys != 1) return fail(E, RDGPU_ERR_ARG, "normalised RDF is defined for a single system");
     const int S = E->desc.n_types, H = S * S * E->rdf_nbins;
     std::vector<long long> nper(S, 0);
+    int rc = DISPATCH(E, sync_types, E);
+    if (rc) return rc;
     for (int t : E->types_h) nper[t]++;
     double vol = 1.0;
     for (int a = 0; a < 3; ++a)

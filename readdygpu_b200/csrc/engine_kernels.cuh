@@ -1804,9 +1804,13 @@ __device__ __forceinline__ void chunk_entries(const int4& q, int k0, int i, int 
 
 // one BD step of every particle over its pair list; ALLPER: every axis of
 // every system is periodic (the minimum image needs no per-axis test);
-// NARROW: list entries are 16-bit offsets (the handle's list format)
+// NARROW: list entries are 16-bit offsets (the handle's list format).  The
+// FP32 harmonic-repulsion kernel of all-periodic systems runs 9 blocks of 128
+// per SM (56 registers, no spill), measured 4 % faster than 8; 10 spill, and
+// so do the other FP32 variants at 9.
 template <class R, bool HREP, bool ALLPER, int BLOCK, bool NARROW>
-__global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? 1024 : 768) / BLOCK) list_step_kernel(Args<R> a, ListArgs<R> v)
+__global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? (HREP && ALLPER ? 1152 : 1024) : 768) / BLOCK)
+    list_step_kernel(Args<R> a, ListArgs<R> v)
 {
     __shared__ R s_rc2[MAXT * MAXT];
     __shared__ FastTab<R> s_ft;
