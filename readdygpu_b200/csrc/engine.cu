@@ -1836,10 +1836,13 @@ template <class R> int rdf_fine(Engine* E, int nbins, double rmax)
     return RDGPU_OK;
 }
 
-// The RDF frame on a grid of its own (rdf_tile_kernel), from the current
+// The RDF frame on a grid of its own (rdf_rows_kernel), from the current
 // state in any order (no re-sort of the simulation's cells): cells of edge
-// >= rmax.  Returns RDGPU_OK_CONTINUE when some system has fewer than 3 of
-// them along a periodic axis (rdf_fine then takes the frame).
+// >= rmax/2, at least 5 and at most 500 along every axis.  Returns
+// RDGPU_OK_CONTINUE (rdf_fine then takes the frame) when some system has
+// fewer than 5 along a periodic axis (a box shorter than 2.5 rmax), the
+// grid has 2^27 cells or more, or the bin edges do not fit shared memory
+// (more than 4095 bins).
 template <class R> int rdf_tiled(Engine* E, int nbins, double rmax)
 {
     const int S = E->desc.n_types;
@@ -1853,8 +1856,8 @@ template <class R> int rdf_tiled(Engine* E, int nbins, double rmax)
         long long m = 1;
         for (int a = 0; a < 3; ++a) {
             const double Lp = edge(E, s, a);
-            const int n = std::min(cells_along(Lp, rmax), 256);
-            if (E->sys_h[s].per[a] && n < 3) return RDGPU_OK_CONTINUE;
+            const int n = std::min(cells_along(Lp, 0.5 * rmax), 500);
+            if (E->sys_h[s].per[a] && n < 5) return RDGPU_OK_CONTINUE;
             g.n[a] = n;
             g.per[a] = E->sys_h[s].per[a];
             g.L[a] = Lp;
@@ -1866,6 +1869,7 @@ template <class R> int rdf_tiled(Engine* E, int nbins, double rmax)
         nc += m;
     }
     if (nc >= (1LL << 27)) return RDGPU_OK_CONTINUE;
+    if ((size_t)(nbins + 1) * sizeof(float2) > 32 * 1024) return RDGPU_OK_CONTINUE;
     const long long N = E->npart_tot;
     const size_t recsz = sizeof(RdfRec<R>);
     if (E->rdf_grid_n < E->nsys) {
@@ -1902,8 +1906,8 @@ template <class R> int rdf_tiled(Engine* E, int nbins, double rmax)
     const double rpre = rmax + 64.0 * std::ldexp(1.0, -24) * lmax;
     const float r2pre = (float)(rpre * rpre * (1.0 + 1e-5));
     // Bound on |FP32 r^2 - FP64 r^2| of a pair closer than the pre-selection
-    // radius (rdf_bin): each FP32 displacement is within eps of the exact one
-    // (the FP32 conversion of the two coordinates of an FP64 state, the
+    // radius (rdf_rows_kernel): each FP32 displacement is within eps of the
+    // exact one (the FP32 conversion of the two coordinates of an FP64 state, the
     // shifted candidate and the difference, each within 2^-24 of values below
     // 2 lmax + rmax), so r^2 within 2 sqrt(3) rmax eps + 3 eps^2; the FP32
     // squares and sums, the FP32 bin edges and the comparisons round by
@@ -1913,15 +1917,19 @@ template <class R> int rdf_tiled(Engine* E, int nbins, double rmax)
     const float dlt = (float)((2.0 * std::sqrt(3.0) * rr * eps + 3.0 * eps * eps +
                                8.0 * std::ldexp(1.0, -24) * rr * rr + 8.0 * std::ldexp(1.0, -53) * rr * rr) *
                               (1.0 + 1e-3));
-    const size_t edges = (size_t)(nbins + 1) * 8 + (size_t)((nbins + 2) & ~1) * 4;
-    const size_t dyn = edges + (size_t)H * 4;
-    const int use_smem = dyn <= 16 * 1024 ? 1 : 0;
-    const size_t smem = use_smem ? dyn : edges;
-    if (smem > 16 * 1024) return RDGPU_OK_CONTINUE;
-    const int grid = (int)std::min<long long>((nc + RDF_WARPS - 1) / RDF_WARPS, 148LL * 8);
-    rdf_tile_kernel<R><<<grid, RDF_WARPS * 32, smem, E->stream>>>(E->rdf_grid_d, E->nsys, nc, E->rdf_start, rec, S,
-                                                                  nbins, E->rdf_e2, rmax / (double)nbins, r2pre, dlt,
-                                                                  use_smem, E->rdf_tmp);
+    // dynamic shared memory: the edge pairs, then the block's histogram
+    const size_t epairs = (size_t)(nbins + 1) * sizeof(float2);
+    const int use_smem = epairs + (size_t)H * 4 <= 32 * 1024 ? 1 : 0;
+    const size_t smem = epairs + (use_smem ? (size_t)H * 4 : 0);
+    const int grid = (int)std::min<long long>((nc + RDR_WARPS - 1) / RDR_WARPS, 148LL * 8);
+    if (S == 1)
+        rdf_rows_kernel<R, false><<<grid, RDR_WARPS * 32, smem, E->stream>>>(
+            E->rdf_grid_d, E->nsys, nc, E->rdf_start, rec, S, nbins, E->rdf_e2, rmax / (double)nbins, r2pre,
+            dlt, use_smem, E->rdf_tmp);
+    else
+        rdf_rows_kernel<R, true><<<grid, RDR_WARPS * 32, smem, E->stream>>>(
+            E->rdf_grid_d, E->nsys, nc, E->rdf_start, rec, S, nbins, E->rdf_e2, rmax / (double)nbins, r2pre,
+            dlt, use_smem, E->rdf_tmp);
     CK(cudaGetLastError());
     return RDGPU_OK;
 }

@@ -1201,23 +1201,8 @@ __global__ void __launch_bounds__(128, 8) rdf_kernel(const SysDev* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// RDF on a coarse grid (rdf_tile_kernel and its counting sort).  The grid has
-// cells of edge >= rmax and at least 3 cells along every periodic axis, so
-// every pair closer than rmax sits in one cell or in two neighbouring ones,
-// and each unordered pair of neighbouring cells appears once among a cell's
-// 13 forward neighbours.  A warp takes one cell: its particles (up to 96 at
-// a time) go to per-warp shared memory, and the candidates of the cell and
-// its forward neighbours (partners of higher index only in the cell itself),
-// moved to their periodic image next to the cell, are taken one per lane, 32
-// at a time, each tested against all own particles with an FP32 distance
-// that over-accepts (r2pre covers its rounding).  Each lane collects its
-// accepted tests of a window as bits, and one warp scan compacts them into a
-// queue.  Queued pairs are binned 32 at a time, one per lane (rdf_bin): by
-// the FP32 distance when it is farther than a stated bound from every bin
-// edge, else by the exact FP64 predicate and bin rule of rdf_kernel: dx =
-// (xi - xj) - sx, sx the periodic shift of the neighbour cell, which is the
-// symmetric minimum image (mimg_sym) for every pair closer than rmax < L/2.
-// Each pair is counted for both orientations, as in rdf_kernel.
+// RDF on a grid of its own (rdf_rows_kernel below and its counting sort):
+// the particles sorted by the cell of that grid, as RdfRec records.
 struct RdfGrid {
     int n[3];
     int per[3];
@@ -1279,36 +1264,6 @@ __global__ void rdf_scatter_kernel(long long ntot, State<R> cur, const int* __re
     }
 }
 
-constexpr int RDF_WARPS = 4;
-constexpr int RDF_OWN = 96;       // own particles per pass of a cell
-constexpr int RDF_WIN = 8;        // own particles tested per lane between two compactions
-constexpr int RDF_QUEUE = 32 * RDF_WIN + 32;
-constexpr int RDF_NB = 14;        // the cell and its 13 forward neighbours
-
-// per-warp shared memory of rdf_tile_kernel
-struct RdfWarp {
-    float4 own[RDF_OWN];          // own particles as floats, bits(type) in w
-    double ox[3 * RDF_OWN];       // own particles as stored (widened FP32 or FP64)
-    int nbase[RDF_NB];            // first candidate of each neighbour cell
-    int npre[RDF_NB + 1];         // exclusive prefix of the neighbour cells' counts
-    int ncode[RDF_NB];            // periodic shift code of each neighbour cell (2 bits per axis)
-    int2 queue[RDF_QUEUE];        // accepted pairs: (candidate index, own | shift code << 8)
-    float qr2[RDF_QUEUE];         // their FP32 squared distance
-};
-
-// offset q of the half-shell: the cell itself, then the 13 offsets (dx, dy,
-// dz) with dz > 0, or dz == 0 and dy > 0, or dz == dy == 0 and dx > 0
-__device__ __forceinline__ void rdf_offset(int q, int d[3])
-{
-    if (q == 0) { d[0] = d[1] = d[2] = 0; return; }
-    if (q == 1) { d[0] = 1; d[1] = 0; d[2] = 0; return; }
-    if (q < 5) { d[2] = 0; d[1] = 1; d[0] = q - 3; return; }
-    const int k = q - 5;
-    d[2] = 1;
-    d[1] = k / 3 - 1;
-    d[0] = k % 3 - 1;
-}
-
 template <class R>
 __device__ __forceinline__ void rdf_count(int ti, int tj, int k, int S, int nbins, int use_smem,
                                           unsigned* __restrict__ sh, unsigned long long* __restrict__ hist)
@@ -1323,232 +1278,265 @@ __device__ __forceinline__ void rdf_count(int ti, int tj, int k, int S, int nbin
     }
 }
 
-// Bins one queued pair.  The FP64 squared distance r2 of rdf_kernel's rule
-// lies within dlt of the FP32 one (dlt covers the FP32 rounding of the
-// coordinates, the periodic shift, the distance and the FP32 bin edges
-// e2f): when r2f +- dlt falls inside one bin, that is r2's bin; otherwise
-// the FP64 predicate decides from the stored coordinates.
-template <class R>
-__device__ __forceinline__ void rdf_bin(const RdfWarp& w, const RdfRec<R>* __restrict__ rec, int2 e, float r2f,
-                                        float dlt, const RdfGrid& g, int S, int nbins, double rmax2, float inv_wf,
-                                        const double* __restrict__ e2s, const float* __restrict__ e2f,
-                                        int use_smem, unsigned* __restrict__ sh, unsigned long long* __restrict__ hist)
+// ---------------------------------------------------------------------------
+// RDF on a grid of cells of edge >= rmax/2 (rdf_rows_kernel).  Every
+// periodic axis has at least 5 of them, so a pair closer than rmax sits in
+// two cells at most 2 apart along every axis, and each unordered pair of
+// such cells is met exactly once among a cell's 62 forward offsets (dz > 0;
+// dz == 0, dy > 0; dz == dy == 0, dx > 0): two offsets in [-2, 2] never
+// reach the same cell, and d, -d never both.  A warp takes one cell (the own
+// cell): its particles, up to RDR_OWN at a time, go to per-warp shared memory
+// as packed FP32 pairs.  The candidates are the 13 forward rows of the
+// stencil (a row: the cells x-2 .. x+2 at one (dy, dz); the row dy = dz = 0
+// holds x+1 and x+2 only) and the own cell itself (partners of higher index),
+// as up to 27 contiguous ranges of sorted particles (a row splits in two
+// where it wraps around a periodic x bound).  They are taken 32 at a time,
+// one per lane, and moved to their periodic image next to the own cell.
+// Each lane tests its candidate against two own particles per step with
+// packed f32x2 arithmetic: dx = own - candidate image, r^2 = fma(dz, dz,
+// fma(dy, dy, dx dx)), over-accepting through r2pre (the bound and dlt are
+// derived with rdf_tiled on the host).  An accepted pair is binned at once:
+// by the FP32 distance when r^2 is farther than dlt from both edges of its
+// bin, else by the exact FP64 rule of rdf_kernel (rdr_exact).  Each pair is
+// counted for both orientations.
+// ---------------------------------------------------------------------------
+constexpr int RDR_WARPS = 8;
+constexpr int RDR_OWN = 64;        // own particles per pass of a cell (32 packed pairs)
+constexpr int RDR_SELF = 26;       // range slot of the own cell (slots 2q, 2q+1: row q, parts A and B)
+
+struct RdrWarp {
+    ulonglong2 oxy[RDR_OWN / 2];            // packed (x0, x1), (y0, y1) of own pair p
+    unsigned long long oz[RDR_OWN / 2];     // packed (z0, z1)
+    int2 ot[RDR_OWN / 2];                   // their types
+    int rbase[32];                          // first sorted index of range slot r
+    int rlen[32];                           // its length
+    int rpre[32];                           // exclusive prefix of the lengths; INT_MAX past slot 27
+    float4 rsh[32];                         // FP32 image shift of its candidates; w: bits(shift code)
+};
+
+// row q of the forward half of the stencil: offsets (dy, dz) and the x range
+__device__ __forceinline__ void rdr_row(int q, int& dy, int& dz, int& dxlo, int& dxhi)
 {
-    const int o = e.y & 0xff, code = e.y >> 8;
-    if (r2f - dlt >= e2f[nbins]) return;                  // beyond rmax
-    int k = r2f > 0.0f ? (int)(r2f * rsqrtf(r2f) * inv_wf) : 0;
-    k = min(max(k, 0), nbins - 1);
-    const int ti = __float_as_int(w.own[o].w);
-    int tj;
-    if constexpr (sizeof(R) == 4) tj = __float_as_int(__ldg(&rec[e.x].p.w));
-    else tj = __ldg(&rec[e.x].t);
-    if (r2f - dlt >= e2f[k] && r2f + dlt < e2f[k + 1]) {
-        rdf_count<R>(ti, tj, k, S, nbins, use_smem, sh, hist);
-        return;
-    }
-    double xj[3];
-    if constexpr (sizeof(R) == 4) {
-        const float4 p = __ldg(&rec[e.x].p);
-        xj[0] = p.x; xj[1] = p.y; xj[2] = p.z;
+    if (q < 10) { dz = 1 + q / 5; dy = q % 5 - 2; dxlo = -2; dxhi = 2; }
+    else if (q < 12) { dz = 0; dy = q - 9; dxlo = -2; dxhi = 2; }
+    else if (q == 12) { dz = 0; dy = 0; dxlo = 1; dxhi = 2; }
+    else { dz = 0; dy = 0; dxlo = 0; dxhi = 0; }      // q == 13: the own cell
+}
+
+template <bool MULTI>
+__device__ __forceinline__ void rdr_count(int ti, int tj, int k, int S, int nbins, int use_smem,
+                                          unsigned* __restrict__ sh, unsigned long long* __restrict__ hist)
+{
+    if (!MULTI) {
+        if (use_smem) atomicAdd(sh + k, 2u);
+        else atomicAdd(hist + k, 2ull);
     } else {
-        const RdfRec<double> q = rec[e.x];
-        xj[0] = q.x; xj[1] = q.y; xj[2] = q.z;
+        rdf_count<float>(ti, tj, k, S, nbins, use_smem, sh, hist);
+    }
+}
+
+// The exact rule for a pair the FP32 distance cannot bin: own particle i,
+// candidate j of a range with shift code `code`; dx = (xi - xj) - sx with
+// sx the candidate's image shift, r^2 and the bin as in rdf_kernel.
+template <class R, bool MULTI>
+__device__ __noinline__ void rdr_exact(const RdfRec<R>* __restrict__ rec, int i, int j, int code, int ti, int tj,
+                                       const RdfGrid* __restrict__ g, int S, int nbins, double rmax2, double w,
+                                       const double* __restrict__ e2, int use_smem, unsigned* sh,
+                                       unsigned long long* __restrict__ hist)
+{
+    double xi[3], xj[3];
+    if constexpr (sizeof(R) == 4) {
+        const float4 a = __ldg(&rec[i].p), b = __ldg(&rec[j].p);
+        xi[0] = a.x; xi[1] = a.y; xi[2] = a.z;
+        xj[0] = b.x; xj[1] = b.y; xj[2] = b.z;
+    } else {
+        const RdfRec<double> a = rec[i], b = rec[j];
+        xi[0] = a.x; xi[1] = a.y; xi[2] = a.z;
+        xj[0] = b.x; xj[1] = b.y; xj[2] = b.z;
     }
     double d[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const int sc = (code >> (2 * a)) & 3;
-        const double sx = sc == 1 ? g.L[a] : (sc == 2 ? -g.L[a] : 0.0);
-        d[a] = sub_rn(sub_rn(w.ox[3 * o + a], xj[a]), sx);
+        const double sx = sc == 1 ? g->L[a] : (sc == 2 ? -g->L[a] : 0.0);
+        d[a] = sub_rn(sub_rn(xi[a], xj[a]), sx);
     }
     const double r2 = dist2(d[0], d[1], d[2]);
     if (!(r2 < rmax2)) return;
-    while (k > 0 && e2s[k] > r2) --k;
-    while (k < nbins - 1 && e2s[k + 1] <= r2) ++k;
-    rdf_count<R>(ti, tj, k, S, nbins, use_smem, sh, hist);
+    int k = (int)(sqrt(r2) / w);
+    k = min(max(k, 0), nbins - 1);
+    while (k > 0 && __ldg(e2 + k) > r2) --k;
+    while (k < nbins - 1 && __ldg(e2 + k + 1) <= r2) ++k;
+    rdr_count<MULTI>(ti, tj, k, S, nbins, use_smem, sh, hist);
 }
 
-template <class R>
-__global__ void __launch_bounds__(RDF_WARPS * 32) rdf_tile_kernel(const RdfGrid* __restrict__ grids, int nsys,
+template <class R, bool MULTI>
+__global__ void __launch_bounds__(RDR_WARPS * 32, 4) rdf_rows_kernel(const RdfGrid* __restrict__ grids, int nsys,
         long long ncells, const int* __restrict__ start, const RdfRec<R>* __restrict__ rec, int S, int nbins,
         const double* __restrict__ e2, double w, float r2pre, float dlt, int use_smem,
         unsigned long long* __restrict__ hist)
 {
-    // shared memory: the warps' RdfWarp, then the squared bin edges (FP64,
-    // then FP32) and, with use_smem, the block's histogram
-    __shared__ RdfWarp s_w[RDF_WARPS];
-    extern __shared__ double s_dyn[];
-    double* e2s = s_dyn;
-    float* e2f = reinterpret_cast<float*>(s_dyn + nbins + 1);
-    unsigned* sh = reinterpret_cast<unsigned*>(e2f + ((nbins + 2) & ~1));
+    // shared memory: the warps' RdrWarp; dynamic: the FP32 bin edge pairs
+    // (e2f[k], e2f[k+1]), k <= nbins (k == nbins: never inside), then, with
+    // use_smem, the block's histogram
+    __shared__ RdrWarp s_w[RDR_WARPS];
+    extern __shared__ float2 s_e2p[];
+    unsigned* sh = reinterpret_cast<unsigned*>(s_e2p + nbins + 1);
     const int H = S * S * nbins;
-    for (int k = threadIdx.x; k <= nbins; k += blockDim.x) {
-        e2s[k] = e2[k];
-        e2f[k] = (float)e2[k];
-    }
+    for (int k = threadIdx.x; k <= nbins; k += blockDim.x)
+        s_e2p[k] = k < nbins ? make_float2((float)e2[k], (float)e2[k + 1]) : make_float2(INFINITY, INFINITY);
     if (use_smem)
         for (int k = threadIdx.x; k < H; k += blockDim.x) sh[k] = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
-    RdfWarp& W = s_w[wp];
+    RdrWarp& W = s_w[wp];
     const double rmax2 = e2[nbins];
     const float inv_wf = (float)(1.0 / w);
-    for (long long c = (long long)blockIdx.x * RDF_WARPS + wp; c < ncells; c += (long long)gridDim.x * RDF_WARPS) {
+    // stand-ins for a missing own particle or candidate: their squared
+    // distance to anything (each other included) overflows, never accepted
+    const float FAR_OWN = 3e30f, FAR_CAND = -3e30f;
+    for (long long c = (long long)blockIdx.x * RDR_WARPS + wp; c < ncells; c += (long long)gridDim.x * RDR_WARPS) {
         const int a0 = start[c], a1 = start[c + 1];
         if (a0 == a1) continue;
-        // the system of cell c: the last grid whose base is <= c
         int lo = 0, hi = nsys - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
             if (grids[mid].base <= c) lo = mid; else hi = mid - 1;
         }
-        const RdfGrid& g = grids[lo];
-        const long long lc = c - g.base;
-        const int cc[3] = {(int)(lc % g.n[0]), (int)((lc / g.n[0]) % g.n[1]), (int)(lc / ((long long)g.n[0] * g.n[1]))};
-        // the neighbour cells: first candidate, count (0 beyond an open
-        // bound) and periodic shift code; exclusive prefix of the counts
+        const RdfGrid* g = grids + lo;
+        const long long lc = c - g->base;
+        const int n0 = g->n[0], n1 = g->n[1], n2 = g->n[2];
+        const int cx = (int)(lc % n0), cy = (int)((lc / n0) % n1), cz = (int)(lc / ((long long)n0 * n1));
+        // the ranges of the 13 rows and the own cell (lane q: slots 2q, 2q+1)
         __syncwarp();
-        int cnt = 0;
-        if (lane < RDF_NB) {
-            int d[3], z[3];
-            int code = 0, base = 0;
+        if (lane < 14) {
+            int dy, dz, dxlo, dxhi;
+            rdr_row(lane, dy, dz, dxlo, dxhi);
+            int yy = cy + dy, zz = cz + dz, code = 0;
             bool skip = false;
-            rdf_offset(lane, d);
+            if (yy < 0) { skip |= !g->per[1]; yy += n1; code |= 2 << 2; }
+            else if (yy >= n1) { skip |= !g->per[1]; yy -= n1; code |= 1 << 2; }
+            if (zz < 0) { skip |= !g->per[2]; zz += n2; code |= 2 << 4; }
+            else if (zz >= n2) { skip |= !g->per[2]; zz -= n2; code |= 1 << 4; }
+            const int xa = cx + dxlo, xb = cx + dxhi;
+            int alo = xa, ahi = xb, acode = code, blo = 0, bhi = -1, bcode = code;
+            if (g->per[0]) {
+                if (xa < 0) { alo = xa + n0; ahi = n0 - 1; acode = code | 2; blo = 0; bhi = xb; }
+                else if (xb >= n0) { ahi = n0 - 1; blo = 0; bhi = xb - n0; bcode = code | 1; }
+            } else {
+                alo = max(xa, 0);
+                ahi = min(xb, n0 - 1);
+            }
+            const long long row = g->base + ((long long)zz * n1 + yy) * n0;
+            int ab = 0, al = 0, bb = 0, bl = 0;
+            if (!skip && alo <= ahi) { ab = start[row + alo]; al = start[row + ahi + 1] - ab; }
+            if (!skip && blo <= bhi) { bb = start[row + blo]; bl = start[row + bhi + 1] - bb; }
+            W.rbase[2 * lane] = ab; W.rlen[2 * lane] = al;
+            W.rbase[2 * lane + 1] = bb; W.rlen[2 * lane + 1] = bl;
 #pragma unroll
-            for (int ax = 0; ax < 3; ++ax) {
-                z[ax] = cc[ax] + d[ax];
-                if (z[ax] < 0) {
-                    if (!g.per[ax]) skip = true;
-                    z[ax] += g.n[ax];
-                    code |= 2 << (2 * ax);
-                } else if (z[ax] >= g.n[ax]) {
-                    if (!g.per[ax]) skip = true;
-                    z[ax] -= g.n[ax];
-                    code |= 1 << (2 * ax);
-                }
-            }
-            if (!skip) {
-                const long long nc = g.base + ((long long)z[2] * g.n[1] + z[1]) * g.n[0] + z[0];
-                base = start[nc];
-                cnt = start[nc + 1] - base;
-            }
-            W.nbase[lane] = base;
-            W.ncode[lane] = code;
-        }
-        int incl = cnt;
+            for (int part = 0; part < 2; ++part) {
+                const int cd = part ? bcode : acode;
+                float s[3];
 #pragma unroll
-        for (int sft = 1; sft < 32; sft <<= 1) {
-            const int t = __shfl_up_sync(FULL, incl, sft);
-            if (lane >= sft) incl += t;
-        }
-        if (lane < RDF_NB) W.npre[lane] = incl - cnt;
-        const int C = __shfl_sync(FULL, incl, RDF_NB - 1);     // candidates of all neighbour cells
-        if (lane == 0) W.npre[RDF_NB] = C;
-        for (int ob = a0; ob < a1; ob += RDF_OWN) {
-            const int m = min(RDF_OWN, a1 - ob);
-            __syncwarp();
-            for (int t = lane; t < m; t += 32) {
-                double xd[3];
-                int ty;
-                if constexpr (sizeof(R) == 4) {
-                    const float4 p = __ldg(&rec[ob + t].p);
-                    xd[0] = p.x; xd[1] = p.y; xd[2] = p.z;
-                    ty = __float_as_int(p.w);
-                } else {
-                    const RdfRec<double> q = rec[ob + t];
-                    xd[0] = q.x; xd[1] = q.y; xd[2] = q.z;
-                    ty = q.t;
+                for (int a = 0; a < 3; ++a) {
+                    const int sc = (cd >> (2 * a)) & 3;
+                    s[a] = sc == 1 ? (float)g->L[a] : (sc == 2 ? -(float)g->L[a] : 0.f);
                 }
-                W.own[t] = make_float4((float)xd[0], (float)xd[1], (float)xd[2], __int_as_float(ty));
-                W.ox[3 * t] = xd[0]; W.ox[3 * t + 1] = xd[1]; W.ox[3 * t + 2] = xd[2];
+                W.rsh[2 * lane + part] = make_float4(s[0], s[1], s[2], __int_as_float(cd));
+            }
+        }
+        __syncwarp();
+        {
+            const int len = lane < 28 ? W.rlen[lane] : 0;
+            int incl = len;
+#pragma unroll
+            for (int sft = 1; sft < 32; sft <<= 1) {
+                const int t = __shfl_up_sync(FULL, incl, sft);
+                if (lane >= sft) incl += t;
+            }
+            W.rpre[lane] = lane < 28 ? incl - len : INT_MAX;
+        }
+        __syncwarp();
+        const int C = W.rpre[27] + W.rlen[27];        // all candidates
+        for (int ob = a0; ob < a1; ob += RDR_OWN) {
+            const int m = min(RDR_OWN, a1 - ob), np = (m + 1) >> 1;
+            __syncwarp();
+            if (lane < np) {
+                float p[2][4];
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int i = ob + 2 * lane + h;
+                    if (2 * lane + h < m) {
+                        if constexpr (sizeof(R) == 4) {
+                            const float4 q = __ldg(&rec[i].p);
+                            p[h][0] = q.x; p[h][1] = q.y; p[h][2] = q.z; p[h][3] = q.w;
+                        } else {
+                            const RdfRec<double> q = rec[i];
+                            p[h][0] = (float)q.x; p[h][1] = (float)q.y; p[h][2] = (float)q.z;
+                            p[h][3] = __int_as_float(q.t);
+                        }
+                    } else {
+                        p[h][0] = p[h][1] = p[h][2] = FAR_OWN; p[h][3] = 0.f;
+                    }
+                }
+                W.oxy[lane] = make_ulonglong2(f2_pack(p[0][0], p[1][0]), f2_pack(p[0][1], p[1][1]));
+                W.oz[lane] = f2_pack(p[0][2], p[1][2]);
+                W.ot[lane] = make_int2(__float_as_int(p[0][3]), __float_as_int(p[1][3]));
             }
             __syncwarp();
-            int qn = 0;
-            // one candidate per lane, 32 at a time over all neighbour cells
             for (int cb = 0; cb < C; cb += 32) {
                 const int t = cb + lane;
-                // its neighbour cell: the last q with npre[q] <= t
-                int ql = 0;
+                int r = 0;
 #pragma unroll
-                for (int step = 8; step > 0; step >>= 1)
-                    if (ql + step < RDF_NB && W.npre[ql + step] <= t) ql += step;
-                const int j = W.nbase[ql] + (t - W.npre[ql]);
-                const int code = W.ncode[ql];
-                float cx = 3e30f, cy = 3e30f, cz = 3e30f;     // no candidate: never accepted
+                for (int st = 16; st > 0; st >>= 1)
+                    if (W.rpre[r + st] <= t) r += st;
+                int j = 0, tj = 0, omax = RDR_OWN, code = 0;
+                float qx = FAR_CAND, qy = FAR_CAND, qz = FAR_CAND;
                 if (t < C) {
+                    j = W.rbase[r] + (t - W.rpre[r]);
+                    const float4 s4 = W.rsh[r];
                     float4 p;
                     if constexpr (sizeof(R) == 4) {
                         p = __ldg(&rec[j].p);
+                        tj = __float_as_int(p.w);
                     } else {
-                        const RdfRec<double> r = rec[j];
-                        p = make_float4((float)r.x, (float)r.y, (float)r.z, 0.f);
+                        const RdfRec<double> q = rec[j];
+                        p = make_float4((float)q.x, (float)q.y, (float)q.z, 0.f);
+                        tj = q.t;
                     }
-                    // the candidate's image next to the own cell
-                    const int s0 = code & 3, s1 = (code >> 2) & 3, s2 = (code >> 4) & 3;
-                    cx = p.x + (s0 == 1 ? (float)g.L[0] : (s0 == 2 ? -(float)g.L[0] : 0.f));
-                    cy = p.y + (s1 == 1 ? (float)g.L[1] : (s1 == 2 ? -(float)g.L[1] : 0.f));
-                    cz = p.z + (s2 == 1 ? (float)g.L[2] : (s2 == 2 ? -(float)g.L[2] : 0.f));
+                    qx = p.x + s4.x; qy = p.y + s4.y; qz = p.z + s4.z;
+                    code = __float_as_int(s4.w);
+                    if (r == RDR_SELF) omax = j - ob;     // own o pairs with j only when ob + o < j
                 }
-                // partners in the own cell itself (ql == 0) count from a higher index only
-                const int jmin = ql == 0 ? j - ob : RDF_OWN;   // own o tests j only when o < j - ob
-                for (int o0 = 0; o0 < m; o0 += RDF_WIN) {
-                    unsigned bits = 0;
-                    float r2k[RDF_WIN];
-                    const int nw = min(RDF_WIN, m - o0);
+                const f32x2 X = f2_pack(qx, qx), Y = f2_pack(qy, qy), Z = f2_pack(qz, qz);
+                for (int pp = 0; pp < np; ++pp) {
+                    const ulonglong2 a = W.oxy[pp];
+                    const f32x2 dX = f2_sub(a.x, X), dY = f2_sub(a.y, Y), dZ = f2_sub(W.oz[pp], Z);
+                    const f32x2 q2 = f2_fma(dZ, dZ, f2_fma(dY, dY, f2_mul(dX, dX)));
+                    float r2h[2];
+                    f2_unpack(q2, r2h[0], r2h[1]);
 #pragma unroll
-                    for (int it = 0; it < RDF_WIN; ++it) {
-                        r2k[it] = 0.f;
-                        if (it < nw) {
-                            const int o = o0 + it;
-                            const float4 a = W.own[o];
-                            const float dx = a.x - cx, dy = a.y - cy, dz = a.z - cz;
-                            const float r2f = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                            r2k[it] = r2f;
-                            const bool acc = r2f < r2pre && o < jmin;
-                            bits |= (unsigned)acc << it;
+                    for (int h = 0; h < 2; ++h) {
+                        const float r2 = r2h[h];
+                        const int o = 2 * pp + h;
+                        if (r2 < r2pre && o < omax) {
+                            int ti = 0;
+                            if (MULTI) ti = h ? W.ot[pp].y : W.ot[pp].x;
+                            // the bin of the FP32 distance (rsqrt, then floor by a round-down add of
+                            // 2^23), kept when r2 is farther than dlt from both of its edges
+                            const float rr = r2 * rsqrtf(r2);
+                            unsigned k = (unsigned)(__float_as_int(__fadd_rd(rr * inv_wf, 8388608.0f)) - 0x4B000000);
+                            k = min(k, (unsigned)nbins);
+                            const float2 ed = s_e2p[k];
+                            if (r2 - dlt >= ed.x && r2 + dlt < ed.y)
+                                rdr_count<MULTI>(ti, tj, (int)k, S, nbins, use_smem, sh, hist);
+                            else
+                                rdr_exact<R, MULTI>(rec, ob + o, j, code, ti, tj, g, S, nbins, rmax2, w, e2,
+                                                    use_smem, sh, hist);
                         }
-                    }
-                    const int cntl = __popc(bits);
-                    int inc2 = cntl;
-#pragma unroll
-                    for (int sft = 1; sft < 32; sft <<= 1) {
-                        const int tt = __shfl_up_sync(FULL, inc2, sft);
-                        if (lane >= sft) inc2 += tt;
-                    }
-                    const int tot = __shfl_sync(FULL, inc2, 31);
-                    if (tot == 0) continue;
-                    int slot = qn + inc2 - cntl;
-#pragma unroll
-                    for (int it = 0; it < RDF_WIN; ++it) {
-                        if ((bits >> it) & 1u) {
-                            W.queue[slot] = make_int2(j, (o0 + it) | (code << 8));
-                            W.qr2[slot] = r2k[it];
-                            ++slot;
-                        }
-                    }
-                    qn += tot;
-                    __syncwarp();
-                    // bin full batches of 32
-                    int done = 0;
-                    for (; done + 32 <= qn; done += 32)
-                        rdf_bin<R>(W, rec, W.queue[done + lane], W.qr2[done + lane], dlt, g, S, nbins, rmax2, inv_wf,
-                                   e2s, e2f, use_smem, sh, hist);
-                    __syncwarp();
-                    if (done > 0) {
-                        if (lane < qn - done) {
-                            W.queue[lane] = W.queue[done + lane];
-                            W.qr2[lane] = W.qr2[done + lane];
-                        }
-                        qn -= done;
-                        __syncwarp();
                     }
                 }
             }
-            // what is left in the queue
-            __syncwarp();
-            if (lane < qn)
-                rdf_bin<R>(W, rec, W.queue[lane], W.qr2[lane], dlt, g, S, nbins, rmax2, inv_wf, e2s, e2f, use_smem, sh,
-                           hist);
         }
     }
     if (use_smem) {
