@@ -1922,14 +1922,16 @@ template <class R> int rdf_tiled(Engine* E, int nbins, double rmax)
     const int use_smem = epairs + (size_t)H * 4 <= 32 * 1024 ? 1 : 0;
     const size_t smem = epairs + (use_smem ? (size_t)H * 4 : 0);
     const int grid = (int)std::min<long long>((nc + RDR_WARPS - 1) / RDR_WARPS, 148LL * 8);
-    if (S == 1)
-        rdf_rows_kernel<R, false><<<grid, RDR_WARPS * 32, smem, E->stream>>>(
-            E->rdf_grid_d, E->nsys, nc, E->rdf_start, rec, S, nbins, E->rdf_e2, rmax / (double)nbins, r2pre,
-            dlt, use_smem, E->rdf_tmp);
-    else
-        rdf_rows_kernel<R, true><<<grid, RDR_WARPS * 32, smem, E->stream>>>(
-            E->rdf_grid_d, E->nsys, nc, E->rdf_start, rec, S, nbins, E->rdf_e2, rmax / (double)nbins, r2pre,
-            dlt, use_smem, E->rdf_tmp);
+    const double w = rmax / (double)nbins;
+    auto go = [&](auto kernel) {
+        kernel<<<grid, RDR_WARPS * 32, smem, E->stream>>>(E->rdf_grid_d, E->nsys, nc, E->rdf_start, rec, S, nbins,
+                                                         E->rdf_e2, w, r2pre, dlt, E->rdf_tmp);
+    };
+    if (S == 1) {
+        if (use_smem) go(rdf_rows_kernel<R, false, true>); else go(rdf_rows_kernel<R, false, false>);
+    } else {
+        if (use_smem) go(rdf_rows_kernel<R, true, true>); else go(rdf_rows_kernel<R, true, false>);
+    }
     CK(cudaGetLastError());
     return RDGPU_OK;
 }

@@ -1339,7 +1339,7 @@ __device__ __forceinline__ void rdr_count(int ti, int tj, int k, int S, int nbin
 // candidate j of a range with shift code `code`; dx = (xi - xj) - sx with
 // sx the candidate's image shift, r^2 and the bin as in rdf_kernel.
 template <class R, bool MULTI>
-__device__ __noinline__ void rdr_exact(const RdfRec<R>* __restrict__ rec, int i, int j, int code, int ti, int tj,
+__device__ __forceinline__ void rdr_exact(const RdfRec<R>* __restrict__ rec, int i, int j, int code, int ti, int tj,
                                        const RdfGrid* __restrict__ g, int S, int nbins, double rmax2, double w,
                                        const double* __restrict__ e2, int use_smem, unsigned* sh,
                                        unsigned long long* __restrict__ hist)
@@ -1370,31 +1370,70 @@ __device__ __noinline__ void rdr_exact(const RdfRec<R>* __restrict__ rec, int i,
     rdr_count<MULTI>(ti, tj, k, S, nbins, use_smem, sh, hist);
 }
 
-template <class R, bool MULTI>
+// stand-ins for a missing own particle or candidate: their squared distance
+// to anything (each other included) overflows, never accepted
+constexpr float RDR_FAR_OWN = 3e30f, RDR_FAR_CAND = -3e30f;
+constexpr int RDR_CPL = 2;         // candidates per lane and chunk
+
+// candidate t of the cell's ranges (t >= C: none), at its image next to the
+// own cell, as packed pairs against two own particles
+struct RdrCand {
+    f32x2 X, Y, Z;
+    int j, tj, omax, code;
+};
+template <class R>
+__device__ __forceinline__ RdrCand rdr_candidate(const RdrWarp& W, const RdfRec<R>* __restrict__ rec, int t, int C,
+                                                 int ob)
+{
+    // its range slot: the last with rpre <= t (empty slots are passed over)
+    int r = 0;
+#pragma unroll
+    for (int st = 16; st > 0; st >>= 1)
+        if (W.rpre[r + st] <= t) r += st;
+    RdrCand q;
+    q.j = 0; q.tj = 0; q.omax = RDR_OWN; q.code = 0;
+    float qx = RDR_FAR_CAND, qy = RDR_FAR_CAND, qz = RDR_FAR_CAND;
+    if (t < C) {
+        q.j = W.rbase[r] + (t - W.rpre[r]);
+        const float4 s4 = W.rsh[r];
+        float4 p;
+        if constexpr (sizeof(R) == 4) {
+            p = __ldg(&rec[q.j].p);
+            q.tj = __float_as_int(p.w);
+        } else {
+            const RdfRec<double> d = rec[q.j];
+            p = make_float4((float)d.x, (float)d.y, (float)d.z, 0.f);
+            q.tj = d.t;
+        }
+        qx = p.x + s4.x; qy = p.y + s4.y; qz = p.z + s4.z;
+        q.code = __float_as_int(s4.w);
+        if (r == RDR_SELF) q.omax = q.j - ob;     // own o pairs with j only when ob + o < j
+    }
+    q.X = f2_pack(qx, qx); q.Y = f2_pack(qy, qy); q.Z = f2_pack(qz, qz);
+    return q;
+}
+
+template <class R, bool MULTI, bool SMEM>
 __global__ void __launch_bounds__(RDR_WARPS * 32, 4) rdf_rows_kernel(const RdfGrid* __restrict__ grids, int nsys,
         long long ncells, const int* __restrict__ start, const RdfRec<R>* __restrict__ rec, int S, int nbins,
-        const double* __restrict__ e2, double w, float r2pre, float dlt, int use_smem,
-        unsigned long long* __restrict__ hist)
+        const double* __restrict__ e2, double w, float r2pre, float dlt, unsigned long long* __restrict__ hist)
 {
     // shared memory: the warps' RdrWarp; dynamic: the FP32 bin edge pairs
     // (e2f[k], e2f[k+1]), k <= nbins (k == nbins: never inside), then, with
-    // use_smem, the block's histogram
+    // SMEM, the block's histogram
     __shared__ RdrWarp s_w[RDR_WARPS];
     extern __shared__ float2 s_e2p[];
     unsigned* sh = reinterpret_cast<unsigned*>(s_e2p + nbins + 1);
     const int H = S * S * nbins;
     for (int k = threadIdx.x; k <= nbins; k += blockDim.x)
         s_e2p[k] = k < nbins ? make_float2((float)e2[k], (float)e2[k + 1]) : make_float2(INFINITY, INFINITY);
-    if (use_smem)
+    if (SMEM)
         for (int k = threadIdx.x; k < H; k += blockDim.x) sh[k] = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
     RdrWarp& W = s_w[wp];
     const double rmax2 = e2[nbins];
     const float inv_wf = (float)(1.0 / w);
-    // stand-ins for a missing own particle or candidate: their squared
-    // distance to anything (each other included) overflows, never accepted
-    const float FAR_OWN = 3e30f, FAR_CAND = -3e30f;
     for (long long c = (long long)blockIdx.x * RDR_WARPS + wp; c < ncells; c += (long long)gridDim.x * RDR_WARPS) {
         const int a0 = start[c], a1 = start[c + 1];
         if (a0 == a1) continue;
@@ -1476,7 +1515,7 @@ __global__ void __launch_bounds__(RDR_WARPS * 32, 4) rdf_rows_kernel(const RdfGr
                             p[h][3] = __int_as_float(q.t);
                         }
                     } else {
-                        p[h][0] = p[h][1] = p[h][2] = FAR_OWN; p[h][3] = 0.f;
+                        p[h][0] = p[h][1] = p[h][2] = RDR_FAR_OWN; p[h][3] = 0.f;
                     }
                 }
                 W.oxy[lane] = make_ulonglong2(f2_pack(p[0][0], p[1][0]), f2_pack(p[0][1], p[1][1]));
@@ -1484,62 +1523,57 @@ __global__ void __launch_bounds__(RDR_WARPS * 32, 4) rdf_rows_kernel(const RdfGr
                 W.ot[lane] = make_int2(__float_as_int(p[0][3]), __float_as_int(p[1][3]));
             }
             __syncwarp();
-            for (int cb = 0; cb < C; cb += 32) {
-                const int t = cb + lane;
-                int r = 0;
+            for (int cb = 0; cb < C; cb += 32 * RDR_CPL) {
+                RdrCand q[RDR_CPL];
 #pragma unroll
-                for (int st = 16; st > 0; st >>= 1)
-                    if (W.rpre[r + st] <= t) r += st;
-                int j = 0, tj = 0, omax = RDR_OWN, code = 0;
-                float qx = FAR_CAND, qy = FAR_CAND, qz = FAR_CAND;
-                if (t < C) {
-                    j = W.rbase[r] + (t - W.rpre[r]);
-                    const float4 s4 = W.rsh[r];
-                    float4 p;
-                    if constexpr (sizeof(R) == 4) {
-                        p = __ldg(&rec[j].p);
-                        tj = __float_as_int(p.w);
-                    } else {
-                        const RdfRec<double> q = rec[j];
-                        p = make_float4((float)q.x, (float)q.y, (float)q.z, 0.f);
-                        tj = q.t;
-                    }
-                    qx = p.x + s4.x; qy = p.y + s4.y; qz = p.z + s4.z;
-                    code = __float_as_int(s4.w);
-                    if (r == RDR_SELF) omax = j - ob;     // own o pairs with j only when ob + o < j
-                }
-                const f32x2 X = f2_pack(qx, qx), Y = f2_pack(qy, qy), Z = f2_pack(qz, qz);
+                for (int u = 0; u < RDR_CPL; ++u) q[u] = rdr_candidate<R>(W, rec, cb + 32 * u + lane, C, ob);
                 for (int pp = 0; pp < np; ++pp) {
                     const ulonglong2 a = W.oxy[pp];
-                    const f32x2 dX = f2_sub(a.x, X), dY = f2_sub(a.y, Y), dZ = f2_sub(W.oz[pp], Z);
-                    const f32x2 q2 = f2_fma(dZ, dZ, f2_fma(dY, dY, f2_mul(dX, dX)));
-                    float r2h[2];
-                    f2_unpack(q2, r2h[0], r2h[1]);
+                    const f32x2 oz = W.oz[pp];
+                    unsigned ex = 0;      // tests (2u + h) left to the exact rule
 #pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const float r2 = r2h[h];
-                        const int o = 2 * pp + h;
-                        if (r2 < r2pre && o < omax) {
-                            int ti = 0;
-                            if (MULTI) ti = h ? W.ot[pp].y : W.ot[pp].x;
+                    for (int u = 0; u < RDR_CPL; ++u) {
+                        const f32x2 dX = f2_sub(a.x, q[u].X), dY = f2_sub(a.y, q[u].Y), dZ = f2_sub(oz, q[u].Z);
+                        const f32x2 q2 = f2_fma(dZ, dZ, f2_fma(dY, dY, f2_mul(dX, dX)));
+                        float r2h[2];
+                        f2_unpack(q2, r2h[0], r2h[1]);
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
                             // the bin of the FP32 distance (rsqrt, then floor by a round-down add of
-                            // 2^23), kept when r2 is farther than dlt from both of its edges
+                            // 2^23), kept when r2 is farther than dlt from both of its edges; computed
+                            // for every lane without a branch (a rejected or coincident pair, r2 = 0 or
+                            // overflowed, gives a NaN distance: bin nbins, whose edges are infinite)
+                            const float r2 = r2h[h];
+                            const bool acc = (r2 < r2pre) & (2 * pp + h < q[u].omax);
                             const float rr = r2 * rsqrtf(r2);
                             unsigned k = (unsigned)(__float_as_int(__fadd_rd(rr * inv_wf, 8388608.0f)) - 0x4B000000);
                             k = min(k, (unsigned)nbins);
                             const float2 ed = s_e2p[k];
-                            if (r2 - dlt >= ed.x && r2 + dlt < ed.y)
-                                rdr_count<MULTI>(ti, tj, (int)k, S, nbins, use_smem, sh, hist);
-                            else
-                                rdr_exact<R, MULTI>(rec, ob + o, j, code, ti, tj, g, S, nbins, rmax2, w, e2,
-                                                    use_smem, sh, hist);
+                            const bool fast = acc & (r2 - dlt >= ed.x) & (r2 + dlt < ed.y);
+                            if (fast) {
+                                const int ti = MULTI ? (h ? W.ot[pp].y : W.ot[pp].x) : 0;
+                                rdr_count<MULTI>(ti, q[u].tj, (int)k, S, nbins, SMEM, sh, hist);
+                            }
+                            ex |= (unsigned)(acc & !fast) << (2 * u + h);
                         }
+                    }
+                    // the rare pairs near a bin edge (or beyond rmax within the FP32 margin)
+                    if (__any_sync(FULL, ex != 0u)) {
+#pragma unroll
+                        for (int u = 0; u < RDR_CPL; ++u)
+#pragma unroll
+                            for (int h = 0; h < 2; ++h)
+                                if ((ex >> (2 * u + h)) & 1u) {
+                                    const int ti = MULTI ? (h ? W.ot[pp].y : W.ot[pp].x) : 0;
+                                    rdr_exact<R, MULTI>(rec, ob + 2 * pp + h, q[u].j, q[u].code, ti, q[u].tj, g, S,
+                                                        nbins, rmax2, w, e2, SMEM, sh, hist);
+                                }
                     }
                 }
             }
         }
     }
-    if (use_smem) {
+    if (SMEM) {
         __syncthreads();
         for (int k = threadIdx.x; k < H; k += blockDim.x)
             if (sh[k]) atomicAdd(hist + k, (unsigned long long)sh[k]);
@@ -1675,6 +1709,7 @@ __global__ void __launch_bounds__(TSUM_BLOCK) typed_final_kernel(const double* _
 // ---------------------------------------------------------------------------
 constexpr int EF_LISTOVF = 16;
 constexpr int EF_LISTWIDE = 32;   // a partner's offset needs the 32-bit list entries
+constexpr int LIST_CHUNK = 4;     // listed partners whose positions the list step requests together
 
 // List head of particle i (8 bytes): its position at the build on a lattice
 // of 2^16 bins per box edge, wrapping (x: bits 0-15 of .x, y: bits 16-31, z:
@@ -1772,11 +1807,12 @@ __device__ __forceinline__ void store_state(const State<double>& st, long long i
     st.rec[i] = r;
 }
 
-// The partners of list entries k0 .. k0 + 3 (k0 a multiple of 4) of sorted
-// particle i, from the group q that holds them: NARROW, two 32-bit words of
-// 16-bit offsets j - i; wide, the 4 indices.
+// The partners of list entries k0 .. k0 + 3 of sorted particle i (k0 a
+// multiple of 4) from the group q that holds them: NARROW, two 32-bit words
+// of 16-bit offsets j - i (the low or high half of the group); wide, the 4
+// indices of the group.
 template <bool NARROW>
-__device__ __forceinline__ void chunk_entries(const int4& q, int k0, int i, int jj[4])
+__device__ __forceinline__ void quad_entries(const int4& q, int k0, int i, int* jj)
 {
     if constexpr (NARROW) {
         const bool hi = (k0 & 4) != 0;
@@ -1802,7 +1838,41 @@ __global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? (HREP && ALLPER ? 115
 {
     __shared__ R s_rc2[MAXT * MAXT];
     __shared__ FastTab<R> s_ft;
-    if (*((volatile int*)a.err)) return;   // an earlier step failed: keep its input intact
+    // the error flag, the step counter and the buffer parity, then the
+    // particle's inputs, all requested before the pair tables: the block
+    // waits on one round of loads, not three
+    const int err0 = *((volatile int*)a.err);
+    const long long t = *((volatile const long long*)a.step_ptr) + a.step_off;
+    const int nreb = *((volatile const int*)&v.ctl->nreb);
+    const int sel = (int)((t + (long long)nreb) & 1LL);
+    const State<R> cur = sel ? v.b1 : v.b0;
+    const State<R> nxt = sel ? v.b0 : v.b1;
+    if (err0) return;   // an earlier step failed: keep its input intact
+    const int i = blockIdx.x * BLOCK + threadIdx.x;
+    const bool live = i < a.ntot;
+    int si = 0;
+    R xi[3] = {R(0), R(0), R(0)};
+    int wi = 0;
+    R c[3] = {R(0), R(0), R(0)};
+    int id = 0;
+    uint2 hd = make_uint2(0, 0);
+    int4 q0 = make_int4(0, 0, 0, 0), q1 = q0;
+    if (live) {
+        si = a.sys_of[i];
+        load_pos(cur, i, xi, wi);
+        if constexpr (sizeof(R) == 4) {
+            const float4 q = __ldg(cur.aux + i);
+            c[0] = q.x; c[1] = q.y; c[2] = q.z;
+            id = __float_as_int(q.w);
+        } else {
+            id = __ldg(&cur.rec[i].id);
+        }
+        hd = __ldg(v.head + i);
+        // the first 8 list entries (one narrow group, two wide ones; capacity
+        // >= 8), before the list length is known; entries past it are unused
+        q0 = __ldg(v.nbr + i);
+        q1 = NARROW ? q0 : __ldg(v.nbr + i + v.stride);
+    }
     // rows of the S types in use (entries (ti, tj) with ti >= S are never read)
     for (int k = threadIdx.x; k < MAXT * a.tab->S; k += BLOCK) {
         s_rc2[k] = a.tab->rc2[k];
@@ -1812,31 +1882,7 @@ __global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? (HREP && ALLPER ? 115
         }
     }
     __syncthreads();
-    const long long t = *((volatile const long long*)a.step_ptr) + a.step_off;
-    const int sel = list_sel(a, v, a.step_off);
-    const State<R> cur = sel ? v.b1 : v.b0;
-    const State<R> nxt = sel ? v.b0 : v.b1;
-    const int i = blockIdx.x * BLOCK + threadIdx.x;
-    if (i >= a.ntot) return;
-    const int si = a.sys_of[i];
-    R xi[3];
-    int wi;
-    R c[3] = {R(0), R(0), R(0)};
-    int id;
-    load_pos(cur, i, xi, wi);
-    if constexpr (sizeof(R) == 4) {
-        const float4 q = __ldg(cur.aux + i);
-        c[0] = q.x; c[1] = q.y; c[2] = q.z;
-        id = __float_as_int(q.w);
-    } else {
-        id = __ldg(&cur.rec[i].id);
-    }
-    const uint2 hd = __ldg(v.head + i);
-    // the first 8 list entries (one narrow group, two wide ones; capacity
-    // >= 8) are requested together with the particle's own state, before its
-    // list length is known; entries past the length are never used
-    const int4 q0 = __ldg(v.nbr + i);
-    const int4 q1 = NARROW ? q0 : __ldg(v.nbr + i + v.stride);
+    if (!live) return;
     const SysDev& s = a.sys[si];
     const int ti = wi & 0xff;
     Box<R> bx;
@@ -1849,14 +1895,23 @@ __global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? (HREP && ALLPER ? 115
     double il[3] = {0.0, 0.0, 0.0};
     if constexpr (sizeof(R) == 4) pf.load(s, xi);
     else { il[0] = s.il[0]; il[1] = s.il[1]; il[2] = s.il[2]; }
-    // the partners in groups of 4: all their positions are requested before
-    // the first pair is evaluated
-    constexpr int LCHUNK = 4;
+    // the partners in chunks of LCHUNK entries (4 or 8): all their positions
+    // are requested before the first pair is evaluated
+    constexpr int EPG = NARROW ? 8 : 4;      // entries per group
+    constexpr int LCHUNK = LIST_CHUNK;
+    static_assert(LCHUNK % 4 == 0, "whole quads per chunk");
     for (int k0 = 0; k0 < cnt; k0 += LCHUNK) {
-        const int gi = NARROW ? (k0 >> 3) : (k0 >> 2);
-        const int4 q = gi == 0 ? q0 : ((gi == 1 && !NARROW) ? q1 : __ldg(nb4 + (long long)gi * v.stride));
         int jj[LCHUNK];
-        chunk_entries<NARROW>(q, k0, i, jj);
+#pragma unroll
+        for (int h = 0; h < LCHUNK / 4; ++h) {
+            const int kq = k0 + 4 * h;              // the quad's first entry
+            const int gi = kq / EPG;                // and its group
+            int4 q = make_int4(0, 0, 0, 0);
+            if (gi == 0) q = q0;
+            else if (gi == 1 && !NARROW) q = q1;
+            else if (kq < cnt) q = __ldg(nb4 + (long long)gi * v.stride);
+            quad_entries<NARROW>(q, kq, i, jj + 4 * h);
+        }
 #pragma unroll
         for (int u = 0; u < LCHUNK; ++u) jj[u] = (k0 + u < cnt) ? jj[u] : -1;
         R xj[LCHUNK][3];
