@@ -103,3 +103,33 @@ def test_rdf_histogram_larger_than_shared_memory(oracle, prec):
     co = oracle.rdf_counts(d, stored, types, nbins, rmax, f32=(prec == "f32c"))
     assert co.sum() > 0
     assert np.array_equal(c.ravel(), co)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("species", [1, 2])
+def test_rdf_lattice_pairs_on_bin_edges(oracle, prec, species):
+    """A simple cubic lattice of spacing 1 nm with bins of 0.1 nm: every pair
+    distance is sqrt(n) nm, and those with n a perfect square lie exactly on
+    a bin edge in real arithmetic (the FP64 edge table rounds them to one side
+    or the other); with two species, the second, shifted by a quarter
+    spacing, adds distances off the lattice.  Counts bit-exact."""
+    n = 18
+    g = np.arange(n, dtype=np.float64)
+    X, Y, Z = np.meshgrid(g, g, g, indexing="ij")
+    lat = np.column_stack([X.ravel(), Y.ravel(), Z.ravel()])
+    if species == 1:
+        xyz, types = lat, np.zeros(len(lat), np.int32)
+    else:
+        xyz = np.concatenate([lat, lat[::3] + 0.25])
+        types = np.concatenate([np.zeros(len(lat), np.int32), np.ones(len(lat[::3]), np.int32)])
+    t = [ParticleType("A", 1e6, 0.3), ParticleType("B", 1e6, 0.3)][:species]
+    sys_ = System(t, pair=[PairPotential(A.P2_HARMONIC, [(0, 0)], 10.0, "repulsive")],
+                  kT=2.437, dt=1e-9, lo=(0, 0, 0), hi=(float(n), float(n), float(n)), periodic=(1, 1, 1))
+    rmax, nbins = 7.0, 70
+    d, stored, _ = oracle_state(oracle, sys_, xyz, prec)
+    with Engine(sys_, precision=prec, neighbour_mode="cells") as e:
+        e.set_particles(xyz, types)
+        c, _ = e.rdf(nbins, rmax, accumulate=False)
+    co = oracle.rdf_counts(d, stored, types, nbins, rmax, f32=(prec == "f32c"))
+    assert co.sum() > 0
+    assert np.array_equal(c.ravel(), co)
