@@ -204,7 +204,7 @@ def rdf_frames(eng, nbins=200, rmax=20.0, frames=5, every=100):
     ms = (time.perf_counter() - t0) * 1e3 / frames
     return {"bins": nbins, "rmax_nm": rmax, "every_steps": every, "ms_per_frame": ms,
             "ms_per_step_amortized": ms / every,
-            "note": "rdgpu_rdf: particles sorted into the RDF grid, rdf_tile_kernel, uint64 counts to the host"}
+            "note": "rdgpu_rdf: particles sorted into the RDF grid, rdf_rows_kernel, uint64 counts to the host"}
 
 
 def host_cpu_model():
