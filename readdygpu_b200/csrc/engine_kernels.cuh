@@ -26,6 +26,7 @@
 // (lib/ReaDDyGPU_Cpp/CudaKernels/CudaSimulation.cu:1034-1236, 1402-1782,
 // 1838-1919).
 #pragma once
+#include <type_traits>
 #include "engine_device.cuh"
 
 namespace rdgpu {
@@ -1381,15 +1382,14 @@ struct RdrCand {
     f32x2 X, Y, Z;
     int j, tj, omax, code;
 };
+// r: the lane's range slot for its previous candidate (0 at the start),
+// advanced to the last slot with rpre <= t (empty slots are passed over;
+// the candidates of a lane only move forward)
 template <class R>
 __device__ __forceinline__ RdrCand rdr_candidate(const RdrWarp& W, const RdfRec<R>* __restrict__ rec, int t, int C,
-                                                 int ob)
+                                                 int ob, int& r)
 {
-    // its range slot: the last with rpre <= t (empty slots are passed over)
-    int r = 0;
-#pragma unroll
-    for (int st = 16; st > 0; st >>= 1)
-        if (W.rpre[r + st] <= t) r += st;
+    while (W.rpre[r + 1] <= t) ++r;
     RdrCand q;
     q.j = 0; q.tj = 0; q.omax = RDR_OWN; q.code = 0;
     float qx = RDR_FAR_CAND, qy = RDR_FAR_CAND, qz = RDR_FAR_CAND;
@@ -1523,53 +1523,65 @@ __global__ void __launch_bounds__(RDR_WARPS * 32, 4) rdf_rows_kernel(const RdfGr
                 W.ot[lane] = make_int2(__float_as_int(p[0][3]), __float_as_int(p[1][3]));
             }
             __syncwarp();
+            const int self0 = W.rpre[RDR_SELF];      // the first candidate of the own cell
+            int slot[RDR_CPL];
+#pragma unroll
+            for (int u = 0; u < RDR_CPL; ++u) slot[u] = 0;
             for (int cb = 0; cb < C; cb += 32 * RDR_CPL) {
                 RdrCand q[RDR_CPL];
 #pragma unroll
-                for (int u = 0; u < RDR_CPL; ++u) q[u] = rdr_candidate<R>(W, rec, cb + 32 * u + lane, C, ob);
-                for (int pp = 0; pp < np; ++pp) {
-                    const ulonglong2 a = W.oxy[pp];
-                    const f32x2 oz = W.oz[pp];
-                    unsigned ex = 0;      // tests (2u + h) left to the exact rule
+                for (int u = 0; u < RDR_CPL; ++u) q[u] = rdr_candidate<R>(W, rec, cb + 32 * u + lane, C, ob, slot[u]);
+                // the own pairs against this chunk; SELF: the chunk holds candidates
+                // of the own cell, which pair with own particles of lower index only
+                auto own_pairs = [&](auto self_tag) {
+                    constexpr bool SELF = decltype(self_tag)::value;
+                    for (int pp = 0; pp < np; ++pp) {
+                        const ulonglong2 a = W.oxy[pp];
+                        const f32x2 oz = W.oz[pp];
+                        unsigned ex = 0;      // tests (2u + h) left to the exact rule
 #pragma unroll
-                    for (int u = 0; u < RDR_CPL; ++u) {
-                        const f32x2 dX = f2_sub(a.x, q[u].X), dY = f2_sub(a.y, q[u].Y), dZ = f2_sub(oz, q[u].Z);
-                        const f32x2 q2 = f2_fma(dZ, dZ, f2_fma(dY, dY, f2_mul(dX, dX)));
-                        float r2h[2];
-                        f2_unpack(q2, r2h[0], r2h[1]);
+                        for (int u = 0; u < RDR_CPL; ++u) {
+                            const f32x2 dX = f2_sub(a.x, q[u].X), dY = f2_sub(a.y, q[u].Y), dZ = f2_sub(oz, q[u].Z);
+                            const f32x2 q2 = f2_fma(dZ, dZ, f2_fma(dY, dY, f2_mul(dX, dX)));
+                            float r2h[2];
+                            f2_unpack(q2, r2h[0], r2h[1]);
 #pragma unroll
-                        for (int h = 0; h < 2; ++h) {
-                            // the bin of the FP32 distance (rsqrt, then floor by a round-down add of
-                            // 2^23), kept when r2 is farther than dlt from both of its edges; computed
-                            // for every lane without a branch (a rejected or coincident pair, r2 = 0 or
-                            // overflowed, gives a NaN distance: bin nbins, whose edges are infinite)
-                            const float r2 = r2h[h];
-                            const bool acc = (r2 < r2pre) & (2 * pp + h < q[u].omax);
-                            const float rr = r2 * rsqrtf(r2);
-                            unsigned k = (unsigned)(__float_as_int(__fadd_rd(rr * inv_wf, 8388608.0f)) - 0x4B000000);
-                            k = min(k, (unsigned)nbins);
-                            const float2 ed = s_e2p[k];
-                            const bool fast = acc & (r2 - dlt >= ed.x) & (r2 + dlt < ed.y);
-                            if (fast) {
-                                const int ti = MULTI ? (h ? W.ot[pp].y : W.ot[pp].x) : 0;
-                                rdr_count<MULTI>(ti, q[u].tj, (int)k, S, nbins, SMEM, sh, hist);
+                            for (int h = 0; h < 2; ++h) {
+                                // the bin of the FP32 distance (rsqrt, then floor by a round-down add of
+                                // 2^23), kept when r2 is farther than dlt from both of its edges; computed
+                                // for every lane without a branch (a rejected or coincident pair, r2 = 0
+                                // or overflowed, gives a NaN distance: bin nbins, whose edges are infinite)
+                                const float r2 = r2h[h];
+                                const bool acc = (r2 < r2pre) & (!SELF || 2 * pp + h < q[u].omax);
+                                const float rr = r2 * rsqrtf(r2);
+                                unsigned k = (unsigned)(__float_as_int(__fadd_rd(rr * inv_wf, 8388608.0f)) -
+                                                        0x4B000000);
+                                k = min(k, (unsigned)nbins);
+                                const float2 ed = s_e2p[k];
+                                const bool fast = acc & (r2 - dlt >= ed.x) & (r2 + dlt < ed.y);
+                                if (fast) {
+                                    const int ti = MULTI ? (h ? W.ot[pp].y : W.ot[pp].x) : 0;
+                                    rdr_count<MULTI>(ti, q[u].tj, (int)k, S, nbins, SMEM, sh, hist);
+                                }
+                                ex |= (unsigned)(acc & !fast) << (2 * u + h);
                             }
-                            ex |= (unsigned)(acc & !fast) << (2 * u + h);
+                        }
+                        // the rare pairs near a bin edge (or beyond rmax within the FP32 margin)
+                        if (__any_sync(FULL, ex != 0u)) {
+#pragma unroll
+                            for (int u = 0; u < RDR_CPL; ++u)
+#pragma unroll
+                                for (int h = 0; h < 2; ++h)
+                                    if ((ex >> (2 * u + h)) & 1u) {
+                                        const int ti = MULTI ? (h ? W.ot[pp].y : W.ot[pp].x) : 0;
+                                        rdr_exact<R, MULTI>(rec, ob + 2 * pp + h, q[u].j, q[u].code, ti, q[u].tj, g,
+                                                            S, nbins, rmax2, w, e2, SMEM, sh, hist);
+                                    }
                         }
                     }
-                    // the rare pairs near a bin edge (or beyond rmax within the FP32 margin)
-                    if (__any_sync(FULL, ex != 0u)) {
-#pragma unroll
-                        for (int u = 0; u < RDR_CPL; ++u)
-#pragma unroll
-                            for (int h = 0; h < 2; ++h)
-                                if ((ex >> (2 * u + h)) & 1u) {
-                                    const int ti = MULTI ? (h ? W.ot[pp].y : W.ot[pp].x) : 0;
-                                    rdr_exact<R, MULTI>(rec, ob + 2 * pp + h, q[u].j, q[u].code, ti, q[u].tj, g, S,
-                                                        nbins, rmax2, w, e2, SMEM, sh, hist);
-                                }
-                    }
-                }
+                };
+                if (cb + 32 * RDR_CPL > self0) own_pairs(std::true_type{});
+                else own_pairs(std::false_type{});
             }
         }
     }
@@ -1709,7 +1721,8 @@ __global__ void __launch_bounds__(TSUM_BLOCK) typed_final_kernel(const double* _
 // ---------------------------------------------------------------------------
 constexpr int EF_LISTOVF = 16;
 constexpr int EF_LISTWIDE = 32;   // a partner's offset needs the 32-bit list entries
-constexpr int LIST_CHUNK = 4;     // listed partners whose positions the list step requests together
+constexpr int LIST_CHUNK = 4;     // listed partners whose positions the list step requests together (FP32C)
+constexpr int LIST_CHUNK_F64 = 4; // the same for the FP64 step
 
 // List head of particle i (8 bytes): its position at the build on a lattice
 // of 2^16 bins per box edge, wrapping (x: bits 0-15 of .x, y: bits 16-31, z:
@@ -1898,7 +1911,7 @@ __global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? (HREP && ALLPER ? 115
     // the partners in chunks of LCHUNK entries (4 or 8): all their positions
     // are requested before the first pair is evaluated
     constexpr int EPG = NARROW ? 8 : 4;      // entries per group
-    constexpr int LCHUNK = LIST_CHUNK;
+    constexpr int LCHUNK = sizeof(R) == 4 ? LIST_CHUNK : LIST_CHUNK_F64;
     static_assert(LCHUNK % 4 == 0, "whole quads per chunk");
     for (int k0 = 0; k0 < cnt; k0 += LCHUNK) {
         int jj[LCHUNK];
