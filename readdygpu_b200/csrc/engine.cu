@@ -1923,15 +1923,19 @@ template <class R> int rdf_tiled(Engine* E, int nbins, double rmax)
     const size_t smem = epairs + (use_smem ? (size_t)H * 4 : 0);
     const int grid = (int)std::min<long long>((nc + RDR_WARPS - 1) / RDR_WARPS, 148LL * 8);
     const double w = rmax / (double)nbins;
+    // the warps' queues take about 40 KB of static shared memory, so the
+    // dynamic part (up to 32 KB) needs the opt-in above 48 KB per block
     auto go = [&](auto kernel) {
+        if (smem > 8 * 1024)
+            CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         kernel<<<grid, RDR_WARPS * 32, smem, E->stream>>>(E->rdf_grid_d, E->nsys, nc, E->rdf_start, rec, S, nbins,
                                                          E->rdf_e2, w, r2pre, dlt, E->rdf_tmp);
+        return RDGPU_OK;
     };
-    if (S == 1) {
-        if (use_smem) go(rdf_rows_kernel<R, false, true>); else go(rdf_rows_kernel<R, false, false>);
-    } else {
-        if (use_smem) go(rdf_rows_kernel<R, true, true>); else go(rdf_rows_kernel<R, true, false>);
-    }
+    int lrc;
+    if (S == 1) lrc = use_smem ? go(rdf_rows_kernel<R, false, true>) : go(rdf_rows_kernel<R, false, false>);
+    else lrc = use_smem ? go(rdf_rows_kernel<R, true, true>) : go(rdf_rows_kernel<R, true, false>);
+    if (lrc) return lrc;
     CK(cudaGetLastError());
     return RDGPU_OK;
 }

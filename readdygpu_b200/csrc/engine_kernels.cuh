@@ -1304,6 +1304,8 @@ __device__ __forceinline__ void rdf_count(int ti, int tj, int k, int S, int nbin
 constexpr int RDR_WARPS = 8;
 constexpr int RDR_OWN = 64;        // own particles per pass of a cell (32 packed pairs)
 constexpr int RDR_SELF = 26;       // range slot of the own cell (slots 2q, 2q+1: row q, parts A and B)
+constexpr int RDR_CPL = 2;         // candidates per lane and chunk
+constexpr int RDR_QUEUE = 32 * RDR_CPL + 32;   // candidate queue of a warp: a chunk and one batch more
 
 struct RdrWarp {
     ulonglong2 oxy[RDR_OWN / 2];            // packed (x0, x1), (y0, y1) of own pair p
@@ -1313,6 +1315,9 @@ struct RdrWarp {
     int rlen[32];                           // its length
     int rpre[32];                           // exclusive prefix of the lengths; INT_MAX past slot 27
     float4 rsh[32];                         // FP32 image shift of its candidates; w: bits(shift code)
+    float4 cq[RDR_QUEUE];                   // queued candidates: image x, y, z; w: bits(type)
+    int4 ci[RDR_QUEUE];                     // their sorted index, own bound (RDR_OWN: none), shift code
+    float box[6];                           // bounding box of the own particles: low x, y, z, high x, y, z
 };
 
 // row q of the forward half of the stencil: offsets (dy, dz) and the x range
@@ -1374,42 +1379,46 @@ __device__ __forceinline__ void rdr_exact(const RdfRec<R>* __restrict__ rec, int
 // stand-ins for a missing own particle or candidate: their squared distance
 // to anything (each other included) overflows, never accepted
 constexpr float RDR_FAR_OWN = 3e30f, RDR_FAR_CAND = -3e30f;
-constexpr int RDR_CPL = 2;         // candidates per lane and chunk
 
-// candidate t of the cell's ranges (t >= C: none), at its image next to the
-// own cell, as packed pairs against two own particles
+// a candidate as packed pairs against two own particles
 struct RdrCand {
     f32x2 X, Y, Z;
     int j, tj, omax, code;
 };
-// r: the lane's range slot for its previous candidate (0 at the start),
-// advanced to the last slot with rpre <= t (empty slots are passed over;
-// the candidates of a lane only move forward)
+
+// Candidate t of the cell's ranges (t >= C: none) at its image next to the
+// own cell: x, y, z and bits(type) in c, (sorted index, own bound, shift
+// code) in m.  r: the lane's range slot for its previous candidate (0 at
+// the start), advanced to the last slot with rpre <= t (empty slots are
+// passed over; a lane's candidates only move forward).
 template <class R>
-__device__ __forceinline__ RdrCand rdr_candidate(const RdrWarp& W, const RdfRec<R>* __restrict__ rec, int t, int C,
-                                                 int ob, int& r)
+__device__ __forceinline__ void rdr_fetch(const RdrWarp& W, const RdfRec<R>* __restrict__ rec, int t, int C, int ob,
+                                          int& r, float4& c, int4& m)
 {
     while (W.rpre[r + 1] <= t) ++r;
-    RdrCand q;
-    q.j = 0; q.tj = 0; q.omax = RDR_OWN; q.code = 0;
-    float qx = RDR_FAR_CAND, qy = RDR_FAR_CAND, qz = RDR_FAR_CAND;
+    c = make_float4(RDR_FAR_CAND, RDR_FAR_CAND, RDR_FAR_CAND, 0.f);
+    m = make_int4(0, RDR_OWN, 0, 0);
     if (t < C) {
-        q.j = W.rbase[r] + (t - W.rpre[r]);
+        const int j = W.rbase[r] + (t - W.rpre[r]);
         const float4 s4 = W.rsh[r];
         float4 p;
         if constexpr (sizeof(R) == 4) {
-            p = __ldg(&rec[q.j].p);
-            q.tj = __float_as_int(p.w);
+            p = __ldg(&rec[j].p);
         } else {
-            const RdfRec<double> d = rec[q.j];
-            p = make_float4((float)d.x, (float)d.y, (float)d.z, 0.f);
-            q.tj = d.t;
+            const RdfRec<double> d = rec[j];
+            p = make_float4((float)d.x, (float)d.y, (float)d.z, __int_as_float(d.t));
         }
-        qx = p.x + s4.x; qy = p.y + s4.y; qz = p.z + s4.z;
-        q.code = __float_as_int(s4.w);
-        if (r == RDR_SELF) q.omax = q.j - ob;     // own o pairs with j only when ob + o < j
+        c = make_float4(p.x + s4.x, p.y + s4.y, p.z + s4.z, p.w);
+        // own o pairs with a candidate of the own cell only when ob + o < j
+        m = make_int4(j, r == RDR_SELF ? j - ob : RDR_OWN, __float_as_int(s4.w), 0);
     }
-    q.X = f2_pack(qx, qx); q.Y = f2_pack(qy, qy); q.Z = f2_pack(qz, qz);
+}
+
+__device__ __forceinline__ RdrCand rdr_cand(const float4& c, const int4& m)
+{
+    RdrCand q;
+    q.X = f2_pack(c.x, c.x); q.Y = f2_pack(c.y, c.y); q.Z = f2_pack(c.z, c.z);
+    q.j = m.x; q.tj = __float_as_int(c.w); q.omax = m.y; q.code = m.z;
     return q;
 }
 
@@ -1434,6 +1443,10 @@ __global__ void __launch_bounds__(RDR_WARPS * 32, 4) rdf_rows_kernel(const RdfGr
     RdrWarp& W = s_w[wp];
     const double rmax2 = e2[nbins];
     const float inv_wf = (float)(1.0 / w);
+    // a candidate at squared FP32 distance >= r2box from the own particles'
+    // bounding box passes the FP32 test with none of them (the margin covers
+    // the roundings of both distances)
+    const float r2box = r2pre * 1.00001f;
     for (long long c = (long long)blockIdx.x * RDR_WARPS + wp; c < ncells; c += (long long)gridDim.x * RDR_WARPS) {
         const int a0 = start[c], a1 = start[c + 1];
         if (a0 == a1) continue;
@@ -1499,40 +1512,59 @@ __global__ void __launch_bounds__(RDR_WARPS * 32, 4) rdf_rows_kernel(const RdfGr
         const int C = W.rpre[27] + W.rlen[27];        // all candidates
         for (int ob = a0; ob < a1; ob += RDR_OWN) {
             const int m = min(RDR_OWN, a1 - ob), np = (m + 1) >> 1;
-            __syncwarp();
-            if (lane < np) {
-                float p[2][4];
+            // the own particles as packed pairs, and their bounding box
+            float p[2][4];
+            float bl[3] = {INFINITY, INFINITY, INFINITY}, bh[3] = {-INFINITY, -INFINITY, -INFINITY};
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int i = ob + 2 * lane + h;
-                    if (2 * lane + h < m) {
-                        if constexpr (sizeof(R) == 4) {
-                            const float4 q = __ldg(&rec[i].p);
-                            p[h][0] = q.x; p[h][1] = q.y; p[h][2] = q.z; p[h][3] = q.w;
-                        } else {
-                            const RdfRec<double> q = rec[i];
-                            p[h][0] = (float)q.x; p[h][1] = (float)q.y; p[h][2] = (float)q.z;
-                            p[h][3] = __int_as_float(q.t);
-                        }
+            for (int h = 0; h < 2; ++h) {
+                const int o = 2 * lane + h;
+                if (o < m) {
+                    if constexpr (sizeof(R) == 4) {
+                        const float4 q = __ldg(&rec[ob + o].p);
+                        p[h][0] = q.x; p[h][1] = q.y; p[h][2] = q.z; p[h][3] = q.w;
                     } else {
-                        p[h][0] = p[h][1] = p[h][2] = RDR_FAR_OWN; p[h][3] = 0.f;
+                        const RdfRec<double> q = rec[ob + o];
+                        p[h][0] = (float)q.x; p[h][1] = (float)q.y; p[h][2] = (float)q.z;
+                        p[h][3] = __int_as_float(q.t);
                     }
+#pragma unroll
+                    for (int ax = 0; ax < 3; ++ax) { bl[ax] = fminf(bl[ax], p[h][ax]); bh[ax] = fmaxf(bh[ax], p[h][ax]); }
+                } else {
+                    p[h][0] = p[h][1] = p[h][2] = RDR_FAR_OWN; p[h][3] = 0.f;
                 }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+                for (int ax = 0; ax < 3; ++ax) {
+                    bl[ax] = fminf(bl[ax], __shfl_xor_sync(FULL, bl[ax], o));
+                    bh[ax] = fmaxf(bh[ax], __shfl_xor_sync(FULL, bh[ax], o));
+                }
+            __syncwarp();
+            if (lane < 3) {
+                W.box[lane] = lane == 0 ? bl[0] : (lane == 1 ? bl[1] : bl[2]);
+                W.box[3 + lane] = lane == 0 ? bh[0] : (lane == 1 ? bh[1] : bh[2]);
+            }
+            if (lane < np) {
                 W.oxy[lane] = make_ulonglong2(f2_pack(p[0][0], p[1][0]), f2_pack(p[0][1], p[1][1]));
                 W.oz[lane] = f2_pack(p[0][2], p[1][2]);
                 W.ot[lane] = make_int2(__float_as_int(p[0][3]), __float_as_int(p[1][3]));
             }
             __syncwarp();
-            const int self0 = W.rpre[RDR_SELF];      // the first candidate of the own cell
-            int slot[RDR_CPL];
-#pragma unroll
-            for (int u = 0; u < RDR_CPL; ++u) slot[u] = 0;
-            for (int cb = 0; cb < C; cb += 32 * RDR_CPL) {
+            // The own pairs against the queued candidates qb .. qb + 32 RDR_CPL
+            // (those past qn: none).  SELF: some of them are in the own cell and
+            // pair with own particles of lower index only.
+            auto chunk = [&](int qb, int qn) {
                 RdrCand q[RDR_CPL];
+                bool any_self = false;
 #pragma unroll
-                for (int u = 0; u < RDR_CPL; ++u) q[u] = rdr_candidate<R>(W, rec, cb + 32 * u + lane, C, ob, slot[u]);
-                // the own pairs against this chunk; SELF: the chunk holds candidates
-                // of the own cell, which pair with own particles of lower index only
+                for (int u = 0; u < RDR_CPL; ++u) {
+                    const int e = qb + 32 * u + lane;
+                    q[u] = e < qn ? rdr_cand(W.cq[e], W.ci[e])
+                                  : rdr_cand(make_float4(RDR_FAR_CAND, RDR_FAR_CAND, RDR_FAR_CAND, 0.f),
+                                             make_int4(0, RDR_OWN, 0, 0));
+                    any_self |= q[u].omax < RDR_OWN;
+                }
                 auto own_pairs = [&](auto self_tag) {
                     constexpr bool SELF = decltype(self_tag)::value;
                     for (int pp = 0; pp < np; ++pp) {
@@ -1580,9 +1612,42 @@ __global__ void __launch_bounds__(RDR_WARPS * 32, 4) rdf_rows_kernel(const RdfGr
                         }
                     }
                 };
-                if (cb + 32 * RDR_CPL > self0) own_pairs(std::true_type{});
+                if (__any_sync(FULL, any_self)) own_pairs(std::true_type{});
                 else own_pairs(std::false_type{});
+            };
+            // Candidates 32 at a time, one per lane; those whose squared FP32
+            // distance to the own particles' bounding box reaches r2box (no
+            // own particle can then pass the FP32 test) are dropped, the others
+            // queued in order, and the queue is worked off a chunk at a time.
+            int qn = 0, slot = 0;
+            for (int tb = 0; tb < C; tb += 32) {
+                float4 c;
+                int4 mi;
+                rdr_fetch<R>(W, rec, tb + lane, C, ob, slot, c, mi);
+                const float ex = fmaxf(fmaxf(W.box[0] - c.x, c.x - W.box[3]), 0.f);
+                const float ey = fmaxf(fmaxf(W.box[1] - c.y, c.y - W.box[4]), 0.f);
+                const float ez = fmaxf(fmaxf(W.box[2] - c.z, c.z - W.box[5]), 0.f);
+                const bool keep = (tb + lane < C) & (fmaf(ez, ez, fmaf(ey, ey, ex * ex)) < r2box);
+                const unsigned mk = __ballot_sync(FULL, keep);
+                if (keep) {
+                    const int e = qn + __popc(mk & ((1u << lane) - 1u));
+                    W.cq[e] = c;
+                    W.ci[e] = mi;
+                }
+                qn += __popc(mk);
+                __syncwarp();
+                if (qn >= 32 * RDR_CPL) {
+                    chunk(0, 32 * RDR_CPL);
+                    __syncwarp();
+                    qn -= 32 * RDR_CPL;
+                    if (lane < qn) {
+                        W.cq[lane] = W.cq[32 * RDR_CPL + lane];
+                        W.ci[lane] = W.ci[32 * RDR_CPL + lane];
+                    }
+                    __syncwarp();
+                }
             }
+            if (qn > 0) chunk(0, qn);
         }
     }
     if (SMEM) {
