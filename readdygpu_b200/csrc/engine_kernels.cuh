@@ -1291,15 +1291,18 @@ __device__ __forceinline__ void rdf_count(int ti, int tj, int k, int S, int nbin
 // stencil (a row: the cells x-2 .. x+2 at one (dy, dz); the row dy = dz = 0
 // holds x+1 and x+2 only) and the own cell itself (partners of higher index),
 // as up to 27 contiguous ranges of sorted particles (a row splits in two
-// where it wraps around a periodic x bound).  They are taken 32 at a time,
-// one per lane, and moved to their periodic image next to the own cell.
-// Each lane tests its candidate against two own particles per step with
-// packed f32x2 arithmetic: dx = own - candidate image, r^2 = fma(dz, dz,
-// fma(dy, dy, dx dx)), over-accepting through r2pre (the bound and dlt are
-// derived with rdf_tiled on the host).  An accepted pair is binned at once:
-// by the FP32 distance when r^2 is farther than dlt from both edges of its
-// bin, else by the exact FP64 rule of rdf_kernel (rdr_exact).  Each pair is
-// counted for both orientations.
+// where it wraps around a periodic x bound).  They are fetched 32 at a time,
+// one per lane, and moved to their periodic image next to the own cell; a
+// candidate farther from the own particles' bounding box than the FP32 test
+// radius is dropped (about a third of them: the stencil's corners), the
+// others are queued per warp in order.  The queue is worked off in chunks of
+// 64, two candidates per lane, each tested against two own particles per
+// step with packed f32x2 arithmetic: dx = own - candidate image, r^2 =
+// fma(dz, dz, fma(dy, dy, dx dx)), over-accepting through r2pre (the bound
+// and dlt are derived with rdf_tiled on the host).  An accepted pair is
+// binned at once: by the FP32 distance when r^2 is farther than dlt from
+// both edges of its bin, else by the exact FP64 rule of rdf_kernel
+// (rdr_exact).  Each pair is counted for both orientations.
 // ---------------------------------------------------------------------------
 constexpr int RDR_WARPS = 8;
 constexpr int RDR_OWN = 64;        // own particles per pass of a cell (32 packed pairs)
