@@ -1790,7 +1790,7 @@ __global__ void __launch_bounds__(TSUM_BLOCK) typed_final_kernel(const double* _
 constexpr int EF_LISTOVF = 16;
 constexpr int EF_LISTWIDE = 32;   // a partner's offset needs the 32-bit list entries
 constexpr int LIST_CHUNK = 4;     // listed partners whose positions the list step requests together (FP32C)
-constexpr int LIST_CHUNK_F64 = 4; // the same for the FP64 step
+constexpr int LIST_CHUNK_F64 = 2; // the same for the FP64 step (2 or a multiple of 4)
 
 // List head of particle i (8 bytes): its position at the build on a lattice
 // of 2^16 bins per box edge, wrapping (x: bits 0-15 of .x, y: bits 16-31, z:
@@ -1980,12 +1980,12 @@ __global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? (HREP && ALLPER ? 115
     // are requested before the first pair is evaluated
     constexpr int EPG = NARROW ? 8 : 4;      // entries per group
     constexpr int LCHUNK = sizeof(R) == 4 ? LIST_CHUNK : LIST_CHUNK_F64;
-    static_assert(LCHUNK % 4 == 0, "whole quads per chunk");
+    static_assert(LCHUNK == 2 || LCHUNK % 4 == 0, "pairs or whole quads per chunk");
     for (int k0 = 0; k0 < cnt; k0 += LCHUNK) {
-        int jj[LCHUNK];
+        int jj[LCHUNK < 4 ? 4 : LCHUNK];
 #pragma unroll
-        for (int h = 0; h < LCHUNK / 4; ++h) {
-            const int kq = k0 + 4 * h;              // the quad's first entry
+        for (int h = 0; h < (LCHUNK + 3) / 4; ++h) {
+            const int kq = (k0 & ~3) + 4 * h;       // the quad's first entry
             const int gi = kq / EPG;                // and its group
             int4 q = make_int4(0, 0, 0, 0);
             if (gi == 0) q = q0;
@@ -1993,6 +1993,7 @@ __global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? (HREP && ALLPER ? 115
             else if (kq < cnt) q = __ldg(nb4 + (long long)gi * v.stride);
             quad_entries<NARROW>(q, kq, i, jj + 4 * h);
         }
+        if (LCHUNK == 2 && (k0 & 2)) { jj[0] = jj[2]; jj[1] = jj[3]; }   // the quad's upper pair
 #pragma unroll
         for (int u = 0; u < LCHUNK; ++u) jj[u] = (k0 + u < cnt) ? jj[u] : -1;
         R xj[LCHUNK][3];
