@@ -133,3 +133,28 @@ def test_rdf_lattice_pairs_on_bin_edges(oracle, prec, species):
     co = oracle.rdf_counts(d, stored, types, nbins, rmax, f32=(prec == "f32c"))
     assert co.sum() > 0
     assert np.array_equal(c.ravel(), co)
+
+
+@pytest.mark.parametrize("prec", PRECS)
+def test_rdf_dense_cluster_many_passes(oracle, prec):
+    """600 particles packed into one RDF cell (3 nm cube) among 1,000 spread
+    over the box: the cluster's cell holds ten passes of own particles, its
+    candidate queue fills and drains many times, and the own cell's pairs
+    span passes.  Three species; counts bit-exact."""
+    rng = np.random.default_rng(21)
+    L = 40.0
+    types_ = [ParticleType(f"T{i}", 1e6, 0.5) for i in range(3)]
+    sys_ = System(types_, pair=[PairPotential(A.P2_HARMONIC, [(0, 0)], 10.0, "repulsive")],
+                  kT=2.437, dt=1e-9, lo=(0, 0, 0), hi=(L, L, L), periodic=(1, 1, 1))
+    cluster = rng.uniform(13.6, 16.6, size=(600, 3))     # inside RDF cell 3 of edge 40/9 nm per axis
+    spread = rng.uniform(0, L, size=(1000, 3))
+    xyz = np.concatenate([cluster, spread])
+    types = rng.integers(0, 3, len(xyz)).astype(np.int32)
+    rmax, nbins = 8.0, 64
+    d, stored, _ = oracle_state(oracle, sys_, xyz, prec)
+    with Engine(sys_, precision=prec, neighbour_mode="cells") as e:
+        e.set_particles(xyz, types)
+        c, _ = e.rdf(nbins, rmax, accumulate=False)
+    co = oracle.rdf_counts(d, stored, types, nbins, rmax, f32=(prec == "f32c"))
+    assert co.sum() > 600 * 599
+    assert np.array_equal(c.ravel(), co)
