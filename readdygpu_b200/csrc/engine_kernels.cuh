@@ -1995,17 +1995,20 @@ __global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? (HREP && ALLPER ? 115
         }
         if (LCHUNK == 2 && (k0 & 2)) { jj[0] = jj[2]; jj[1] = jj[3]; }   // the quad's upper pair
 #pragma unroll
-        for (int u = 0; u < LCHUNK; ++u) jj[u] = (k0 + u < cnt) ? jj[u] : -1;
+        // entries past the list's end: HREP, the particle itself (r^2 = 0,
+        // no force, and its position is in L1), which spares the chunk's
+        // per-entry branches; otherwise -1 (skipped)
+        for (int u = 0; u < LCHUNK; ++u) jj[u] = (k0 + u < cnt) ? jj[u] : (HREP ? i : -1);
         R xj[LCHUNK][3];
         int wj[LCHUNK];
 #pragma unroll
         for (int u = 0; u < LCHUNK; ++u) {
-            if (jj[u] >= 0) load_pos(cur, jj[u], xj[u], wj[u]);
+            if (HREP || jj[u] >= 0) load_pos(cur, jj[u], xj[u], wj[u]);
             else { xj[u][0] = xj[u][1] = xj[u][2] = R(0); wj[u] = 0; }
         }
 #pragma unroll
         for (int u = 0; u < LCHUNK; ++u) {
-            if (jj[u] < 0) continue;
+            if (!HREP && jj[u] < 0) continue;
             R dx, dy, dz, r2;
             if constexpr (sizeof(R) == 4) {
                 pair_disp_x2(pf, xj[u][0], xj[u][1], xj[u][2], dx, dy, dz, r2);
