@@ -1981,7 +1981,11 @@ __global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? (HREP && ALLPER ? 115
     constexpr int EPG = NARROW ? 8 : 4;      // entries per group
     constexpr int LCHUNK = sizeof(R) == 4 ? LIST_CHUNK : LIST_CHUNK_F64;
     static_assert(LCHUNK == 2 || LCHUNK % 4 == 0, "pairs or whole quads per chunk");
-    for (int k0 = 0; k0 < cnt; k0 += LCHUNK) {
+    // FP32 HREP: every lane runs the warp's longest list (its chunks past its
+    // own list hold only itself), so the loop needs no per-lane exit (1 %
+    // faster on config 4; the FP64 step measured 2 % slower with it)
+    const int kend = (HREP && sizeof(R) == 4) ? __reduce_max_sync(__activemask(), cnt) : cnt;
+    for (int k0 = 0; k0 < kend; k0 += LCHUNK) {
         int jj[LCHUNK < 4 ? 4 : LCHUNK];
 #pragma unroll
         for (int h = 0; h < (LCHUNK + 3) / 4; ++h) {
