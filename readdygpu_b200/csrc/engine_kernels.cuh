@@ -1912,9 +1912,11 @@ __device__ __forceinline__ void quad_entries(const int4& q, int k0, int i, int* 
 // NARROW: list entries are 16-bit offsets (the handle's list format).  The
 // FP32 harmonic-repulsion kernel of all-periodic systems runs 9 blocks of 128
 // per SM (56 registers, no spill), measured 4 % faster than 8; 10 spill, and
-// so do the other FP32 variants at 9.
+// so do the other FP32 variants at 9.  Its FP64 twin runs 7 (72 registers,
+// 3 % faster than 6 despite a few spilled registers; 8 is slower).
 template <class R, bool HREP, bool ALLPER, int BLOCK, bool NARROW>
-__global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? (HREP && ALLPER ? 1152 : 1024) : 768) / BLOCK)
+__global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? (HREP && ALLPER ? 1152 : 1024) : (HREP && ALLPER ? 896 : 768)) /
+                                             BLOCK)
     list_step_kernel(Args<R> a, ListArgs<R> v)
 {
     __shared__ R s_rc2[MAXT * MAXT];
