@@ -64,9 +64,9 @@ def test_rdf_five_cells_open_axis_planted_pairs(oracle, prec, mode):
 
 @pytest.mark.parametrize("prec", PRECS)
 def test_rdf_batch_of_boxes_equals_sum_over_systems(oracle, prec):
-    """A batch of periodic cubes of different sizes: the batch's counts are the
-    sum of the oracle's counts of every box (cells of edge rmax/2 in the large
-    boxes, fewer than 5 of them in the small ones)."""
+    """A batch of periodic cubes of different sizes (10 to 27 RDF cells per
+    edge): the batch's counts are the sum of the oracle's counts of every
+    box."""
     from readdygpu_b200 import configs
     w = configs.config4(n_systems=12, nmin=300, nmax=6000)
     rmax, nbins = 7.0, 70
