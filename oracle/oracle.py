@@ -208,6 +208,17 @@ def bd_normals(seed, step, index):
     return list(o)
 
 
+def bd_normals_many(seed, step, n):
+    """bd_normals of indices 0 .. n-1 as an (n, 3) array."""
+    out = np.empty((n, 3))
+    o = (C.c_double * 3)()
+    f = lib().orc_bd_normals
+    for i in range(n):
+        f(seed, step, i, o)
+        out[i] = o
+    return out
+
+
 def splitmix64(x):
     return lib().orc_splitmix64(x)
 

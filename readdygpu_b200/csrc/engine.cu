@@ -28,9 +28,13 @@ constexpr int RDGPU_OK_CONTINUE = 1;
 // hot particles (moved more than about skin/2 since the build) the list check
 // looks at after a step, at most (fewer for small handles); with more, the
 // step rebuilds the list instead
-constexpr int kHotMax = 2048;
-// blocks of 32 warps of the list check (one warp per hot particle at a time)
-constexpr int kCheckBlocks = 16;
+constexpr int kHotMax = 8192;
+// hot_max = npart / kHotDiv (at least 8, at most kHotMax)
+constexpr long long kHotDiv = 300;
+// the list check: blocks of 8 warps, one warp per hot particle at a time, at
+// most 8 blocks per SM of 148
+constexpr int kCheckBlock = 256;
+constexpr int kCheckBlocks = 148 * 8;
 }  // namespace
 
 std::string& rdgpu_global_error() { return g_create_error; }
@@ -671,9 +675,10 @@ template <class R> ListArgs<R> make_list_args(Engine* E, bool with_list)
     const double dq = list_lattice_error(E);
     v.thr2 = (float)(th - dq > 0 ? (th - dq) * (th - dq) : 0.0);
     v.cap2 = (float)(th - dq > 0 ? (2.0 * th - dq) * (2.0 * th - dq) : 0.0);
-    // checking a hot particle's neighbourhood costs about what rebuilding
-    // the lists of a thousand particles does
-    v.hot_max = (int)std::min<long long>(kHotMax, std::max<long long>(8, E->npart_tot / 1000));
+    // a larger cap stretches the intervals between rebuilds, but the check
+    // costs more per step and the sorted order decays for longer (on config
+    // 4, caps of 2048 to 32768 measured best at 8192)
+    v.hot_max = (int)std::min<long long>(kHotMax, std::max<long long>(8, E->npart_tot / kHotDiv));
     return v;
 }
 
@@ -761,15 +766,15 @@ template <class R> void launch_chain(Engine* E, const Args<R>& a, const ListArgs
     list_finish_kernel<<<1, 32, 0, st>>>(E->ctl, E->err);
 }
 
-// the list check after a step (list_check_kernel): kCheckBlocks blocks of 32
-// warps, one hot particle per warp at a time
+// the list check after a step (list_check_kernel): a warp per hot particle
+// up to hot_max (kCheckBlocks blocks at most); the blocks that the step's hot
+// particles do not fill exit at once
 template <class R> void launch_check(Engine* E, const Args<R>& a, const ListArgs<R>& v, long long off,
                                      cudaGraphConditionalHandle h, int set_cond, cudaStream_t st)
 {
-    // at most 4 hot particles per warp (32 warps a block): fewer blocks for
-    // small handles, whose cap is lower
-    const int grid = std::max(1, std::min(kCheckBlocks, (v.hot_max + 127) / 128));
-    list_check_kernel<R, 1024><<<grid, 1024, 0, st>>>(a, v, off, h, set_cond);
+    constexpr int wpb = kCheckBlock / 32;
+    const int grid = std::max(1, std::min(kCheckBlocks, (v.hot_max + wpb - 1) / wpb));
+    list_check_kernel<R, kCheckBlock><<<grid, kCheckBlock, 0, st>>>(a, v, off, h, set_cond);
 }
 
 // Inside a stream capture: the re-sort of a step becomes a conditional graph

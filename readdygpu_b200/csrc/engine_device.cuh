@@ -115,20 +115,43 @@ __device__ __forceinline__ uint4 bd_words(unsigned long long seed, long long ste
     return philox4x32_10(c, make_uint2((unsigned)seed, (unsigned)(seed >> 32)));
 }
 
+// -2 ln u of the uniform u = (w + 1/2) 2^-32 of Philox word w, in FP32.
+// Near u = 1 the logarithm is small and an absolute error in it becomes a
+// large relative error in sqrt(-2 ln u), so for v = 1 - u < 1/16 it is the
+// Taylor series -ln(1 - v) = v + v^2/2 + ... + v^6/6 (truncation below
+// v^6/7 relative, 9e-9), with v = (~w + 1/2) 2^-32 taken from the
+// complement of the word (exact where it matters; u itself, rounded to 24
+// bits, would be off by up to 2^-25).  Elsewhere, |ln u| >= ln(16/15), the
+// hardware log2 (__log2f) times ln 2.  Both values are computed and one is
+// selected, so the warp does not diverge.
+__device__ __forceinline__ float bm_minus2ln(unsigned w)
+{
+    const float s = 2.3283064365386963e-10f;    // 2^-32
+    const float u = ((float)w + 0.5f) * s;
+    const float v = ((float)(~w) + 0.5f) * s;
+    float p = 1.0f / 6.0f;
+    p = fmaf(p, v, 0.2f);
+    p = fmaf(p, v, 0.25f);
+    p = fmaf(p, v, 1.0f / 3.0f);
+    p = fmaf(p, v, 0.5f);
+    p = fmaf(p, v, 1.0f);
+    const float series = 2.0f * v * p;
+    const float hw = -1.3862943611198906f * __log2f(u);    // -2 ln 2 log2(u)
+    return v < 0.0625f ? series : hw;
+}
+
 // Box-Muller on the uniforms (w + 1/2) 2^-32 of the four Philox words.  The
 // FP32 transform takes the angle from the hardware sin/cos approximation on
 // the argument 2 pi u - pi in [-pi, pi], where its absolute error is about
-// 4e-7, and flips the sign back; the radius uses the accurate logf, since
-// sqrt(-2 ln u) amplifies log errors for u near 1.
+// 4e-7, and flips the sign back; the radius is sqrt(bm_minus2ln(w)).
 __device__ __forceinline__ void bd_normals(unsigned long long seed, long long step, long long index,
                                            float out[3])
 {
     uint4 w = bd_words(seed, step, index);
     const float s = 2.3283064365386963e-10f;
     const float two_pi = 6.283185307179586f, pi = 3.141592653589793f;
-    const float u0 = ((float)w.x + 0.5f) * s, u1 = ((float)w.y + 0.5f) * s;
-    const float u2 = ((float)w.z + 0.5f) * s, u3 = ((float)w.w + 0.5f) * s;
-    const float ra = sqrtf(-2.0f * logf(u0)), rb = sqrtf(-2.0f * logf(u2));
+    const float u1 = ((float)w.y + 0.5f) * s, u3 = ((float)w.w + 0.5f) * s;
+    const float ra = sqrtf(bm_minus2ln(w.x)), rb = sqrtf(bm_minus2ln(w.z));
     float sa, ca, sb, cb;
     __sincosf(fmaf(u1, two_pi, -pi), &sa, &ca);
     __sincosf(fmaf(u3, two_pi, -pi), &sb, &cb);

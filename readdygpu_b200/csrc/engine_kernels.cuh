@@ -2320,17 +2320,24 @@ __device__ __forceinline__ bool hot_pairs_listed(const Args<R>& a, const ListArg
         bx.load(s);
         ListCell<R> g;
         g.locate(s, xh);
+        // candidates 4 at a time: their positions are requested together
+        // (past the range's end, its last candidate again, not tested)
         list_row_ranges<R>(a, s, g, v.rl2max * R(1.0001), lane / 3 - 1, lane % 3 - 1, [&](int j0, int j1, R, R, R) {
-            for (int j = j0; j < j1 && ok; ++j) {
-                if (j == h) continue;
-                R xj[3];
-                int wj;
-                load_pos(st, j, xj, wj);
-                const R dx = mimg_sel(xh[0], xj[0], bx.L[0], bx.half[0], s.per[0]);
-                const R dy = mimg_sel(xh[1], xj[1], bx.L[1], bx.half[1], s.per[1]);
-                const R dz = mimg_sel(xh[2], xj[2], bx.L[2], bx.half[2], s.per[2]);
-                if (dist2(dx, dy, dz) < rc2[wj & 0xff] * R(1.0001) && !(listed(v, h, j) && listed(v, j, h)))
-                    ok = false;
+            for (int j = j0; j < j1 && ok; j += 4) {
+                R xj[4][3];
+                int wj[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) load_pos(st, min(j + u, j1 - 1), xj[u], wj[u]);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int jj = j + u;
+                    if (jj >= j1 || jj == h) continue;
+                    const R dx = mimg_sel(xh[0], xj[u][0], bx.L[0], bx.half[0], s.per[0]);
+                    const R dy = mimg_sel(xh[1], xj[u][1], bx.L[1], bx.half[1], s.per[1]);
+                    const R dz = mimg_sel(xh[2], xj[u][2], bx.L[2], bx.half[2], s.per[2]);
+                    if (dist2(dx, dy, dz) < rc2[wj[u] & 0xff] * R(1.0001) && !(listed(v, h, jj) && listed(v, jj, h)))
+                        ok = false;
+                }
             }
         });
     }
@@ -2347,21 +2354,30 @@ __device__ __forceinline__ bool hot_pairs_listed(const Args<R>& a, const ListArg
 // every such particle while no particle has moved more than sqrt(cap2) ~
 // skin since the build (the step kernel raises the rebuild flag itself
 // beyond that).  A missing pair, or more than hot_max hot particles, raise
-// the flag.  One warp per hot particle at a time, over all blocks; the last
-// block to finish clears the counts and sets the condition of the graph node
-// that holds the re-sort (set_cond).
+// the flag.  One warp per hot particle at a time.  The grid is sized for
+// hot_max; only the first nb blocks, as many as the step's hot particles
+// fill (one when there are none or too many), take part, and the others
+// exit at once, so that a step with few hot particles costs a few blocks.
+// The last of the nb blocks to finish clears the counts and sets the
+// condition of the graph node that holds the re-sort (set_cond).  Every
+// block that takes part reads nhot before the last one clears it (the
+// clearing waits for the nb blocks' counts); a later block that reads 0
+// computes nb = 1 and exits.
 template <class R, int BLOCK>
 __global__ void __launch_bounds__(BLOCK) list_check_kernel(Args<R> a, ListArgs<R> v, long long off,
                                                            cudaGraphConditionalHandle hc, int set_cond)
 {
+    constexpr int WPB = BLOCK / 32;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int n = *((volatile const int*)&v.ctl->nhot);
+    const int nb = (n <= 0 || n > v.hot_max) ? 1 : min((int)gridDim.x, (n + WPB - 1) / WPB);
+    if ((int)blockIdx.x >= nb) return;
     if (*((volatile const int*)a.err) == 0 && *((volatile const int*)&v.ctl->need) == 0) {
-        const int n = *((volatile const int*)&v.ctl->nhot);
         if (n > v.hot_max) {
-            if (threadIdx.x == 0 && blockIdx.x == 0) *((volatile int*)&v.ctl->need) = 1;
+            if (threadIdx.x == 0) *((volatile int*)&v.ctl->need) = 1;
         } else if (n > 0) {
             const State<R> st = list_sel(a, v, off) ? v.b1 : v.b0;
-            for (int k = blockIdx.x * (BLOCK / 32) + warp; k < n; k += gridDim.x * (BLOCK / 32)) {
+            for (int k = blockIdx.x * WPB + warp; k < n; k += nb * WPB) {
                 if (!hot_pairs_listed<R>(a, v, st, __ldg(v.hot + k), lane)) {
                     if (lane == 0) *((volatile int*)&v.ctl->need) = 1;
                     break;
@@ -2373,7 +2389,7 @@ __global__ void __launch_bounds__(BLOCK) list_check_kernel(Args<R> a, ListArgs<R
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
-        if (atomicAdd(&v.ctl->done, 1) == (int)gridDim.x - 1) {
+        if (atomicAdd(&v.ctl->done, 1) == nb - 1) {
             __threadfence();
             v.ctl->done = 0;
             v.ctl->nhot = 0;

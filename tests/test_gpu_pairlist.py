@@ -260,7 +260,7 @@ def test_list_long_run_equals_cells(prec):
 def test_list_check_overflow_of_hot_particles_rebuilds(prec):
     """Every particle of 2000 moves 0.6 nm (more than skin/2, less than the
     skin) in a random direction: far more hot particles than the check takes
-    (N/1000, at least 8), so the step rebuilds the list outright; then forces
+    (N/300, at least 8), so the step rebuilds the list outright; then forces
     act on the rebuilt list.  The trajectory is the cell walk's."""
     sys_, xyz, types = cfg1(2000)
     b = np.array([np.sqrt(2.0 * t.D * sys_.dt) for t in sys_.types])[types]
@@ -280,6 +280,42 @@ def test_list_check_overflow_of_hot_particles_rebuilds(prec):
         out[mode] = (x, m)
     assert out["list"][1]["neighbour_mode"] == "list"
     assert out["list"][1]["list_builds"] >= 2
+    same(prec, out["cells"][0], out["list"][0])
+
+
+@pytest.mark.parametrize("prec", ["f32c", "f64"])
+def test_list_check_hot_particles_over_many_blocks(prec):
+    """150 of 60,000 particles (config 1's species at config 4's density, a
+    periodic 200 nm cube) move 0.6 nm (more than skin/2, less than the skin)
+    in a random direction: within the check's cap (N/300 = 200), so the
+    check looks at all of them, one warp each over 19 blocks of 8 warps, and
+    keeps the list (no pair can have closed the skin).  The trajectory is the
+    cell walk's."""
+    n, L = 60_000, 200.0
+    sys_ = System([ParticleType("A", 1e6, 1.5), ParticleType("B", 5e5, 2.0)],
+                  pair=[PairPotential(A.P2_HARMONIC, [(0, 0), (0, 1), (1, 1)], 10.0, "repulsive")],
+                  kT=2.437, dt=1e-9, lo=(0, 0, 0), hi=(L, L, L), periodic=(1, 1, 1))
+    rng = np.random.default_rng(13)
+    xyz = rng.uniform(0, L, (n, 3))
+    types = (np.arange(n) % 2).astype(np.int32)
+    b = np.array([np.sqrt(2.0 * t.D * sys_.dt) for t in sys_.types])[types]
+    u = rng.standard_normal((n, 3))
+    u *= 0.6 / np.linalg.norm(u, axis=1, keepdims=True)
+    kick = np.zeros((n, 3))
+    sel = rng.choice(n, 150, replace=False)
+    kick[sel] = u[sel] / b[sel, None]
+    out = {}
+    for mode in ("cells", "list"):
+        with Engine(sys_, precision=prec, neighbour_mode=mode, skin=1.0) as e:
+            e.set_particles(xyz, types)
+            e.step_with_noise(kick)
+            for _ in range(3):
+                e.step_with_noise(np.zeros((n, 3)))
+            x, _ = e.get_particles()
+            m = e.metrics()
+        out[mode] = (x, m)
+    assert out["list"][1]["neighbour_mode"] == "list"
+    assert out["list"][1]["list_builds"] == 1
     same(prec, out["cells"][0], out["list"][0])
 
 

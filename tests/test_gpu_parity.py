@@ -133,6 +133,27 @@ def test_philox_noise_matches_oracle(oracle, prec):
     assert np.abs(z - zo).max() <= tol
 
 
+def test_fp32_normals_over_many_words(oracle):
+    """The FP32 Box-Muller transform over 1.2 M Philox words (200,000
+    particles, 2 steps): every normal within 2e-5 of the oracle's FP64 one,
+    the words near u = 1 (where the radius is sqrt(-2 ln u) of a small
+    logarithm) and near u = 0 included."""
+    n = 200_000
+    sys_ = System([ParticleType("A", 1e6, 1.0)], pair=[PairPotential(A.P2_HARMONIC, [(0, 0)], 10.0, "repulsive")],
+                  kT=2.437, dt=1e-9, lo=(0, 0, 0), hi=(300.0, 300.0, 300.0), periodic=(1, 1, 1))
+    xyz = np.random.default_rng(8).uniform(0, 300.0, (n, 3))
+    seed = 1357911
+    with Engine(sys_, precision="f32c", seed=seed, neighbour_mode="cells") as e:
+        e.set_particles(xyz, np.zeros(n, np.int32))
+        zs = [e.debug_noise(t) for t in (3, 4)]
+    for t, z in zip((3, 4), zs):
+        zo = oracle.bd_normals_many(seed, t, n)
+        err = np.abs(z - zo)
+        assert err.max() <= 2e-5, (t, err.max(), zo.ravel()[err.argmax()])
+        r2 = zo[:, 0] ** 2 + zo[:, 1] ** 2
+        assert r2.min() < 1e-4 and r2.max() > 20.0      # both ends of the radius were drawn
+
+
 @pytest.mark.parametrize("prec", PRECS)
 @pytest.mark.parametrize("nbins,rmax", [(50, 12.0), (64, 30.0)])
 def test_rdf_counts_bit_exact(oracle, prec, nbins, rmax):
