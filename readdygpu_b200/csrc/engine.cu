@@ -32,9 +32,10 @@ constexpr int kHotMax = 8192;
 // hot_max = npart / kHotDiv (at least 8, at most kHotMax)
 constexpr long long kHotDiv = 300;
 // the list check: blocks of 8 warps, one warp per hot particle at a time, at
-// most 8 blocks per SM of 148
+// most 512 blocks (two hot particles per warp at the cap of 8192; grids of
+// 128, 256 and 1019 blocks measured slower per step on config 4)
 constexpr int kCheckBlock = 256;
-constexpr int kCheckBlocks = 148 * 8;
+constexpr int kCheckBlocks = 512;
 }  // namespace
 
 std::string& rdgpu_global_error() { return g_create_error; }
