@@ -2000,11 +2000,16 @@ __global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? (HREP && ALLPER ? 115
             quad_entries<NARROW>(q, kq, i, jj + 4 * h);
         }
         if (LCHUNK == 2 && (k0 & 2)) { jj[0] = jj[2]; jj[1] = jj[3]; }   // the quad's upper pair
-#pragma unroll
         // entries past the list's end: HREP, the particle itself (r^2 = 0,
         // no force, and its position is in L1), which spares the chunk's
-        // per-entry branches; otherwise -1 (skipped)
-        for (int u = 0; u < LCHUNK; ++u) jj[u] = (k0 + u < cnt) ? jj[u] : (HREP ? i : -1);
+        // per-entry branches; otherwise -1 (skipped).  Narrow lists hold
+        // offset 0 (the particle itself) in the rest of their last group, and
+        // a group past the list's end is not loaded (zeros, offset 0 again),
+        // so HREP needs no test there
+        if constexpr (!(HREP && NARROW)) {
+#pragma unroll
+            for (int u = 0; u < LCHUNK; ++u) jj[u] = (k0 + u < cnt) ? jj[u] : (HREP ? i : -1);
+        }
         R xj[LCHUNK][3];
         int wj[LCHUNK];
 #pragma unroll
@@ -2260,6 +2265,13 @@ __device__ __forceinline__ void list_build_one(const Args<R>& a, const ListArgs<
             list_row_ranges<R>(a, s, g, lim, dz, dy, [&](int j0, int j1, R sx, R sy, R sz) {
                 list_range<R>(st, j0, j1, i, xi, sx, sy, sz, rl2, lw, cnt);
             });
+    // narrow lists: the rest of the last group (all of group 0 for an empty
+    // list: the list step always loads it) holds offset 0, the particle
+    // itself, which the list step reads past the list's end (zero force)
+    if (lw.narrow && cnt <= v.cap) {
+        const int kfill = cnt == 0 ? 8 : (cnt + 7) & ~7;     // capacity >= 8, a multiple of 8
+        for (int k = cnt; k < kfill; ++k) lw.put(k, i);
+    }
     v.head[i] = make_head(xi, s, min(cnt, v.cap));
     if (cnt > v.cap || lw.wide_need) {
         if (cnt > v.cap) atomicMax(&v.ctl->maxcnt, cnt);
