@@ -476,7 +476,9 @@ __device__ __forceinline__ int img_add(int w, int axis, int delta)
     return (w & ~(0xff << sh)) | (v << sh);
 }
 
-// FP32 with Kahan compensation: true position = x - c
+// FP32 with Kahan compensation: true position = x - c.  ALLPER: every axis
+// of the system is periodic (known to the caller; spares the per-axis test)
+template <bool ALLPER = false>
 __device__ __forceinline__ int em_update(float x[3], float c[3], int& w, const float F[3], const float xi[3], float A,
                                          float B, const SysDev& s)
 {
@@ -488,7 +490,7 @@ __device__ __forceinline__ int em_update(float x[3], float c[3], int& w, const f
         float t = x[a] + y;
         c[a] = (t - x[a]) - y;
         x[a] = t;
-        if (s.per[a]) {
+        if (ALLPER || s.per[a]) {
             const float L = s.Lf[a];
             if (x[a] >= L) {
                 x[a] = x[a] - L;                // exact (Sterbenz)
@@ -508,6 +510,7 @@ __device__ __forceinline__ int em_update(float x[3], float c[3], int& w, const f
     return ef;
 }
 
+template <bool ALLPER = false>
 __device__ __forceinline__ int em_update(double x[3], double* /*c*/, int& w, const double F[3], const double xi[3],
                                          double A, double B, const SysDev& s)
 {
@@ -515,7 +518,7 @@ __device__ __forceinline__ int em_update(double x[3], double* /*c*/, int& w, con
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         double v = x[a] + (A * F[a] + B * xi[a]);
-        if (s.per[a]) {
+        if (ALLPER || s.per[a]) {
             const double L = s.L[a];
             if (v >= L) { v -= L; w = img_add(w, a, 1); }
             else if (v < 0.0) { v += L; w = img_add(w, a, -1); }
@@ -2067,7 +2070,7 @@ __global__ void __launch_bounds__(BLOCK, (sizeof(R) == 4 ? (HREP && ALLPER ? 115
     } else {
         bd_normals(s.seed, t, (long long)id, xn);
     }
-    const int ef = em_update(xi, c, wi, F, xn, a.tab->a[ti], a.tab->b[ti], s);
+    const int ef = em_update<ALLPER>(xi, c, wi, F, xn, a.tab->a[ti], a.tab->b[ti], s);
     // displacement since the build (lattice estimate; the thresholds
     // allow for its error)
     const float dd = head_disp2(hd, xi, s);
